@@ -1,0 +1,298 @@
+/*
+ * cryosph_b200.h -- C ABI of the B200-native per-step particle hot path of the
+ * CryoSPH multiphase SPH solver (weakly-compressible liquid/vapour SPH with
+ * CSF surface tension, heat conduction and Lee phase change).
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (CRYO_OK == 0) and never throws.  cryo_last_error() gives the message of the
+ * last failure on a context.  Host arrays are copied; device memory is owned by
+ * the context.  All work of a context is ordered on one CUDA stream.
+ *
+ * Reference interfaces replaced (paths inside the CryoSPH-CUDA project):
+ *   include/cryosph/solvers/sph_solver.hpp:20-91    SolverConfig      -> cryo_config_t
+ *   include/cryosph/physics/fluid_properties.hpp:11  FluidProperties   -> cryo_fluid_t
+ *   include/cryosph/solvers/sph_solver.hpp:108-132  Diagnostics       -> cryo_diagnostics_t
+ *   include/cryosph/solvers/sph_solver.hpp:134-232  Solver            -> cryo_ctx + cryo_* below
+ *   include/cryosph/core/spatial_hash.hpp:62-92     SpatialHash/reorder -> cryo_grid_build
+ *   include/cryosph/physics/SPH_kernels.cuh:95-113  density passes    -> cryo_pass(...)
+ *   include/cryosph/physics/navier_stokes.cuh:13-23 momentum passes   -> cryo_pass(...)
+ *   include/cryosph/physics/surface_tension.cuh:14-25 ST passes       -> cryo_pass(...)
+ *   include/cryosph/physics/phase_change.cuh:15-46  thermal/PC passes -> cryo_pass(...)
+ */
+#ifndef CRYOSPH_B200_H
+#define CRYOSPH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CRYO_ABI_VERSION 1
+
+/* ---------------------------------------------------------------- status */
+enum {
+  CRYO_OK = 0,
+  CRYO_EINVAL = 1,   /* maps to std::invalid_argument / ValueError           */
+  CRYO_ERANGE = 2,   /* maps to std::out_of_range                            */
+  CRYO_ERUNTIME = 3, /* maps to std::runtime_error                           */
+  CRYO_ECUDA = 4,    /* CUDA runtime failure (also std::runtime_error)       */
+  CRYO_EDEVICE = 5   /* a device-side guard tripped (status word non-zero)   */
+};
+
+/* Device-side guard bits reported through cryo_device_status(). */
+enum {
+  CRYO_DEV_NBR_OVERFLOW = 1u << 0, /* neighbour list capacity exceeded (scan fallback used) */
+  CRYO_DEV_SPLIT_DROPPED = 1u << 1,/* split halves dropped: capacity exhausted */
+  CRYO_DEV_NONFINITE = 1u << 2,    /* NaN/Inf seen in a dt maximum */
+  CRYO_DEV_BAD_CELL = 1u << 3      /* a cell index fell outside the grid table */
+};
+
+/* ------------------------------------------------------------- enums */
+/* Values equal the reference enums (sim_params.cuh:12-18, SPH_kernels.cuh:12,
+ * geometry.hpp:160-164, particle_system.hpp:13-18). */
+enum { CRYO_KERNEL_CUBIC = 0, CRYO_KERNEL_WENDLAND_C2 = 1 };
+enum { CRYO_DENSITY_SUMMATION = 0, CRYO_DENSITY_CONTINUITY = 1 };
+enum { CRYO_ST_NONE = 0, CRYO_ST_CSF = 1, CRYO_ST_AKINCI = 2 };
+enum { CRYO_WALL_ADIABATIC = 0, CRYO_WALL_ISOTHERMAL = 1 };
+enum { CRYO_THERMO_VENTED = 0, CRYO_THERMO_CLOSED = 1 };
+enum { CRYO_WET_NORMAL_ROTATION = 0, CRYO_WET_CONTACT_LINE_FORCE = 1, CRYO_WET_BOTH = 2 };
+enum { CRYO_LIQUID = 0, CRYO_VAPOR = 1, CRYO_WALL = 2, CRYO_DEAD = 3 };
+enum { CRYO_FLAG_HEATED = 1, CRYO_FLAG_SOURCE = 2, CRYO_FLAG_TARGET_VAPOR = 4, CRYO_FLAG_DYING = 8 };
+enum { CRYO_FLUID_CUSTOM = 0, CRYO_FLUID_LH2 = 1, CRYO_FLUID_LN2 = 2, CRYO_FLUID_LOX = 3,
+       CRYO_FLUID_LCH4 = 4, CRYO_FLUID_H2O = 5 };
+
+/* ------------------------------------------------------------ structs */
+/* FluidProperties (fluid_properties.hpp:11-38), SI units. */
+typedef struct cryo_fluid {
+  float rho_liquid, rho_vapor, mu_liquid, mu_vapor, k_liquid, k_vapor;
+  float cp_liquid, cp_vapor, sigma, h_fg, T_sat, p_sat, R_gas;
+} cryo_fluid_t;
+
+/* SolverConfig (sph_solver.hpp:20-91), field for field; booleans are int. */
+typedef struct cryo_config {
+  float dx, h_factor;
+  int kernel, density_mode, normalize_initial_masses;
+  float gravity[3];
+  float velocity_scale, sound_speed, tait_gamma, background_pressure, vapor_stiffness;
+  int clamp_negative_pressure;
+  int transport_velocity;
+  float transport_background_factor;
+  int transport_stress, transport_interface_only;
+  int particle_shifting;
+  float shifting_strength;
+  float artificial_viscosity, artificial_viscosity_vapor, delta_sph;
+  int no_slip, sps_turbulence;
+  float smagorinsky_cs;
+  int surface_tension;
+  float contact_angle_deg, contact_angle_wall_weight;
+  int wall_colour, wetting_model, csf_smooth_normals, csf_balanced;
+  float akinci_gamma, akinci_beta;
+  int thermal, phase_change, wall_thermal_bc;
+  float heater_power, conductivity_scale, lee_evaporation, lee_condensation;
+  int thermo_mode;
+  float vent_relaxation, merge_ratio, split_ratio, max_transfer_fraction;
+  float phase_change_density_limit, vapor_mass_rebalance;
+  float cfl, viscous_number, force_number, capillary_number, thermal_number;
+  float dt_max, dt_min, fixed_dt;
+} cryo_config_t;
+
+/* Diagnostics (sph_solver.hpp:108-132). */
+typedef struct cryo_diagnostics {
+  double time;
+  long long step;
+  double dt;
+  int n_total, n_liquid, n_vapor, n_wall;
+  double mass_liquid, mass_vapor, mass_total;
+  double kinetic_energy, enthalpy, heat_input;
+  double evaporated_mass, condensed_mass, vented_mass, vented_enthalpy;
+  double T_sat, p_ullage, max_speed;
+  double T_liquid_mean, T_liquid_max, T_vapor_mean;
+  float liquid_com[3], liquid_momentum[3];
+  int splits, merges;
+  float slosh_force[3], slosh_moment[3];
+  float frame_acceleration[3], frame_angular_velocity[3];
+} cryo_diagnostics_t;
+
+/* Host particle arrays (HostParticles, particle_system.hpp:76-90).  Vectors are
+ * packed xyz float triples (n*3 floats).  NULL v / nrm / flags / id mean zero
+ * (ids default to 0..n-1). */
+typedef struct cryo_host_particles {
+  int n;
+  const float* x;
+  const float* v;
+  const float* nrm;
+  const float* m;
+  const float* rho;
+  const float* T;
+  const uint8_t* phase;
+  const uint8_t* flags;
+  const uint32_t* id;
+} cryo_host_particles_t;
+
+/* Writable variant for downloads (caller allocates n entries per array). */
+typedef struct cryo_host_particles_out {
+  int n;
+  float* x;
+  float* v;
+  float* nrm;
+  float* m;
+  float* rho;
+  float* T;
+  uint8_t* phase;
+  uint8_t* flags;
+  uint32_t* id;
+} cryo_host_particles_out_t;
+
+/* Per-particle fields that can be read back (ParticleView members,
+ * particle_system.hpp:37-73).  Vector fields have 3 floats per particle. */
+enum {
+  CRYO_F_X = 0, CRYO_F_V, CRYO_F_VT, CRYO_F_NRM, CRYO_F_M, CRYO_F_M0, CRYO_F_RHO, CRYO_F_T,
+  CRYO_F_PHASE, CRYO_F_FLAGS, CRYO_F_ID,
+  CRYO_F_A, CRYO_F_AB, CRYO_F_FW, CRYO_F_MW, CRYO_F_NS, CRYO_F_VW,
+  CRYO_F_P, CRYO_F_DRHO, CRYO_F_DTDT, CRYO_F_SIGMA, CRYO_F_KAPPA, CRYO_F_NU_T, CRYO_F_ALPHA,
+  CRYO_F_WALL_W, CRYO_F_HEAT_W, CRYO_F_OUT_M, CRYO_F_OUT_H, CRYO_F_W_NORM, CRYO_F_RMIN,
+  CRYO_F_P_WV,
+  CRYO_F_COUNT
+};
+
+/* Individual operator passes (the reference's physics free functions). */
+enum {
+  CRYO_PASS_KICK_DRIFT = 0,      /* sph_solver.cu:20-34             */
+  CRYO_PASS_GRID_BUILD,          /* spatial_hash.cu:48-114          */
+  CRYO_PASS_DENSITY,             /* SPH_kernels.cu:6-34             */
+  CRYO_PASS_NORMALIZE_MASSES,    /* SPH_kernels.cu:36-54            */
+  CRYO_PASS_EOS,                 /* navier_stokes.cu:5-14           */
+  CRYO_PASS_WALL_BOUNDARY,       /* navier_stokes.cu:16-69          */
+  CRYO_PASS_INTERFACE,           /* surface_tension.cu:5-85         */
+  CRYO_PASS_TRANSPORT,           /* SPH_kernels.cu:56-104           */
+  CRYO_PASS_SPS,                 /* navier_stokes.cu:71-119         */
+  CRYO_PASS_MOMENTUM,            /* navier_stokes.cu:121-245        */
+  CRYO_PASS_SMOOTH_NORMALS,      /* surface_tension.cu:87-118       */
+  CRYO_PASS_CSF,                 /* surface_tension.cu:120-177      */
+  CRYO_PASS_AKINCI,              /* surface_tension.cu:179-213      */
+  CRYO_PASS_DENSITY_RATE,        /* SPH_kernels.cu:162-203          */
+  CRYO_PASS_THERMAL,             /* phase_change.cu:31-75 (+ heat-weight sum, sph_solver.cu:466-473) */
+  CRYO_PASS_MAXIMA,              /* sph_solver.cu:475-479           */
+  CRYO_PASS_KICK,                /* sph_solver.cu:36-46             */
+  CRYO_PASS_SHIFTING,            /* SPH_kernels.cu:106-160          */
+  CRYO_PASS_PC_SOURCES,          /* phase_change.cu:77-137          */
+  CRYO_PASS_PC_NORMALIZE,        /* phase_change.cu:139-172 (+ sums, sph_solver.cu:550-552) */
+  CRYO_PASS_PC_APPLY,            /* phase_change.cu:174-215         */
+  CRYO_PASS_REBALANCE,           /* phase_change.cu:217-268         */
+  CRYO_PASS_SPLIT,               /* phase_change.cu:270-335, sph_solver.cu:556-576 */
+  CRYO_PASS_VENTING,             /* phase_change.cu:337-358, sph_solver.cu:578-583 */
+  CRYO_PASS_SATURATION,          /* sph_solver.cu:586-607           */
+  CRYO_PASS_COUNT
+};
+
+typedef struct cryo_ctx cryo_ctx;
+
+/* ----------------------------------------------------------- defaults */
+/* Default SolverConfig values (sph_solver.hpp:20-91). */
+void cryo_config_default(cryo_config_t* cfg);
+/* Fluid presets (fluid_properties.cpp:16-79); which = CRYO_FLUID_*. */
+int cryo_fluid_preset(int which, cryo_fluid_t* out);
+/* Clausius-Clapeyron (fluid_properties.cpp:7-14). */
+float cryo_saturation_temperature(const cryo_fluid_t* f, float p);
+float cryo_saturation_pressure(const cryo_fluid_t* f, float T);
+int cryo_abi_version(void);
+
+/* ------------------------------------------------------------ context */
+/* Solver::Solver (sph_solver.cu:273-279): validates dx > 0 and the contact
+ * angle in [0,180]; creates the blocking stream on `device`. */
+int cryo_create(const cryo_config_t* cfg, const cryo_fluid_t* fluid, int device, cryo_ctx** out);
+void cryo_destroy(cryo_ctx* ctx);
+const char* cryo_last_error(const cryo_ctx* ctx);
+/* Device name string, "NAME (sm_XY)" (cuda_utils.cpp:70-76). */
+int cryo_device_name(int device, char* buf, int buflen);
+int cryo_device_count(void);
+/* The context's CUDA stream (cudaStream_t) as an integer handle. */
+uintptr_t cryo_stream(const cryo_ctx* ctx);
+
+/* Solver::set_particles (sph_solver.cu:407-428).  domain_lo/hi: float[3]. */
+int cryo_set_particles(cryo_ctx* ctx, const cryo_host_particles_t* p, const float* domain_lo,
+                       const float* domain_hi);
+
+/* Solver::step / run_steps / run_until / relax / next_dt (sph_solver.cu:506-543,707-736). */
+int cryo_step(cryo_ctx* ctx);
+int cryo_run_steps(cryo_ctx* ctx, long long n);
+int cryo_run_until(cryo_ctx* ctx, double t_end);
+int cryo_relax(cryo_ctx* ctx, double duration, float damping);
+int cryo_next_dt(cryo_ctx* ctx, double* dt);
+/* Blocks until all submitted work finished; then refreshes the host mirror. */
+int cryo_synchronize(cryo_ctx* ctx);
+
+/* Clock and counters (sph_solver.hpp:155-158). */
+int cryo_time(cryo_ctx* ctx, double* t, long long* step, double* last_dt);
+int cryo_num_particles(cryo_ctx* ctx, int* n);
+int cryo_capacity(cryo_ctx* ctx, int* capacity);
+
+/* Solver::diagnostics (sph_solver.cu:609-653). */
+int cryo_diagnostics(cryo_ctx* ctx, cryo_diagnostics_t* out);
+
+/* Solver::particles (persistent arrays).  out->n must be >= the particle count;
+ * on return out->n holds the count. */
+int cryo_download(cryo_ctx* ctx, cryo_host_particles_out_t* out);
+/* One per-particle field (CRYO_F_*) into a host buffer of `cap` bytes. */
+int cryo_get_field(cryo_ctx* ctx, int field, void* host_out, size_t cap);
+
+/* Run-time controls (sph_solver.cu:655-705). */
+int cryo_set_gravity(cryo_ctx* ctx, const float* g3);
+int cryo_set_frame_motion(cryo_ctx* ctx, const float* acc3, const float* omega3, const float* omega_dot3,
+                          const float* origin3);
+/* ManeuverProfile (sph_solver.hpp:96-105): n knots, times strictly increasing,
+ * acc n*3, omega n*3 or NULL. */
+int cryo_set_maneuver(cryo_ctx* ctx, int n, const double* time, const float* acc, const float* omega,
+                      const float* origin3);
+int cryo_clear_frame_motion(cryo_ctx* ctx);
+int cryo_set_heater_power(cryo_ctx* ctx, float watts);
+int cryo_set_contact_angle(cryo_ctx* ctx, float degrees);
+int cryo_damp_velocities(cryo_ctx* ctx, float factor);
+/* ManeuverProfile::evaluate (sph_solver.cu:244-268), host helper. */
+int cryo_maneuver_evaluate(int n, const double* time, const float* acc, const float* omega, double t,
+                           float* a3, float* w3, float* wdot3);
+
+/* Solver::probe_pressure (sph_solver.cu:738-748): np points (np*3 floats). */
+int cryo_probe_pressure(cryo_ctx* ctx, const float* points, int np, float* out);
+
+/* Derived parameters (the SimParams scalars the Python API exposes). */
+int cryo_sound_speed(cryo_ctx* ctx, float* c0);
+int cryo_smoothing_length(cryo_ctx* ctx, float* h);
+
+/* ------------------------------------------------ operator-level access */
+/* Runs one operator pass on the current state, exactly as the reference's
+ * free function of the same name would (see CRYO_PASS_*).  Used to check
+ * parity pass by pass.  Requires set_particles. */
+int cryo_pass(cryo_ctx* ctx, int pass);
+/* Cell-sorted grid tables after the last grid build.  keys/perm: n entries
+ * (sorted key, gather permutation); cell_start/cell_end: num_cells entries. */
+int cryo_grid_info(cryo_ctx* ctx, int* num_cells, int* nx, int* ny, int* nz, float* origin3, float* cell);
+int cryo_grid_tables(cryo_ctx* ctx, uint32_t* keys, uint32_t* perm, int32_t* cell_start, int32_t* cell_end);
+/* Neighbour list of every particle in reference iteration order
+ * (spatial_hash.hpp:37-56 filtered by r^2 < (2h)^2, self included):
+ * counts[n], and the indices concatenated into list (capacity `cap`). */
+int cryo_neighbor_lists(cryo_ctx* ctx, int32_t* counts, int32_t* list, long long cap, long long* total);
+/* Sets the step size used by the next pass calls (SimParams::dt). */
+int cryo_set_pass_dt(cryo_ctx* ctx, float dt);
+/* Device guard word (CRYO_DEV_* bits), cleared on read. */
+int cryo_device_status(cryo_ctx* ctx, unsigned* status);
+
+/* Full-state checkpoint (persistent arrays + scalar block) in a host blob. */
+int cryo_state_size(cryo_ctx* ctx, size_t* bytes);
+int cryo_save_state(cryo_ctx* ctx, void* blob, size_t cap);
+int cryo_load_state(cryo_ctx* ctx, const void* blob, size_t bytes);
+
+/* Execution mode: 1 = capture each step as a CUDA graph and replay it (default),
+ * 0 = launch the kernels one by one. */
+int cryo_set_graph_mode(cryo_ctx* ctx, int enable);
+/* Neighbour iteration: 1 = per-step neighbour lists (default), 0 = scan the
+ * 27 cells in every pass. */
+int cryo_set_neighbor_mode(cryo_ctx* ctx, int use_lists);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CRYOSPH_B200_H */

@@ -1,0 +1,405 @@
+"""ctypes view of the C ABI declared in include/cryosph_b200.h.
+
+`load()` opens libcryosph_b200.so (built in-tree by build.py) and declares the
+argument types of every entry point.  The struct classes mirror the C structs
+field for field; `config_default()`, `fluid_preset()` fill them from the
+library.  Errors come back as CryoError carrying the status code and message.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_NAME = "libcryosph_b200.so"
+
+# status codes
+CRYO_OK, CRYO_EINVAL, CRYO_ERANGE, CRYO_ERUNTIME, CRYO_ECUDA, CRYO_EDEVICE = range(6)
+# phases / flags
+LIQUID, VAPOR, WALL, DEAD = 0, 1, 2, 3
+FLAG_HEATED, FLAG_SOURCE, FLAG_TARGET_VAPOR, FLAG_DYING = 1, 2, 4, 8
+FLUID_CUSTOM, FLUID_LH2, FLUID_LN2, FLUID_LOX, FLUID_LCH4, FLUID_H2O = range(6)
+
+FIELDS = [
+    "x", "v", "vt", "nrm", "m", "m0", "rho", "T", "phase", "flags", "id",
+    "a", "ab", "fw", "mw", "ns", "vw",
+    "p", "drho", "dTdt", "sigma", "kappa", "nu_t", "alpha",
+    "wall_w", "heat_w", "out_m", "out_h", "w_norm", "rmin", "p_wv",
+]
+FIELD_ID = {name: k for k, name in enumerate(FIELDS)}
+VEC_FIELDS = {"x", "v", "vt", "nrm", "a", "ab", "fw", "mw", "ns", "vw"}
+U8_FIELDS = {"phase", "flags"}
+U32_FIELDS = {"id"}
+
+PASSES = [
+    "kick_drift", "grid_build", "density", "normalize_masses", "eos", "wall_boundary", "interface",
+    "transport", "sps", "momentum", "smooth_normals", "csf", "akinci", "density_rate", "thermal",
+    "maxima", "kick", "shifting", "pc_sources", "pc_normalize", "pc_apply", "rebalance", "split",
+    "venting", "saturation",
+]
+PASS_ID = {name: k for k, name in enumerate(PASSES)}
+
+
+class Fluid(C.Structure):
+    _fields_ = [(n, C.c_float) for n in (
+        "rho_liquid", "rho_vapor", "mu_liquid", "mu_vapor", "k_liquid", "k_vapor",
+        "cp_liquid", "cp_vapor", "sigma", "h_fg", "T_sat", "p_sat", "R_gas")]
+
+
+_F, _I = C.c_float, C.c_int
+CONFIG_FIELDS = [
+    ("dx", _F), ("h_factor", _F), ("kernel", _I), ("density_mode", _I), ("normalize_initial_masses", _I),
+    ("gravity", _F * 3), ("velocity_scale", _F), ("sound_speed", _F), ("tait_gamma", _F),
+    ("background_pressure", _F), ("vapor_stiffness", _F), ("clamp_negative_pressure", _I),
+    ("transport_velocity", _I), ("transport_background_factor", _F), ("transport_stress", _I),
+    ("transport_interface_only", _I), ("particle_shifting", _I), ("shifting_strength", _F),
+    ("artificial_viscosity", _F), ("artificial_viscosity_vapor", _F), ("delta_sph", _F),
+    ("no_slip", _I), ("sps_turbulence", _I), ("smagorinsky_cs", _F),
+    ("surface_tension", _I), ("contact_angle_deg", _F), ("contact_angle_wall_weight", _F),
+    ("wall_colour", _I), ("wetting_model", _I), ("csf_smooth_normals", _I), ("csf_balanced", _I),
+    ("akinci_gamma", _F), ("akinci_beta", _F),
+    ("thermal", _I), ("phase_change", _I), ("wall_thermal_bc", _I), ("heater_power", _F),
+    ("conductivity_scale", _F), ("lee_evaporation", _F), ("lee_condensation", _F), ("thermo_mode", _I),
+    ("vent_relaxation", _F), ("merge_ratio", _F), ("split_ratio", _F), ("max_transfer_fraction", _F),
+    ("phase_change_density_limit", _F), ("vapor_mass_rebalance", _F),
+    ("cfl", _F), ("viscous_number", _F), ("force_number", _F), ("capillary_number", _F),
+    ("thermal_number", _F), ("dt_max", _F), ("dt_min", _F), ("fixed_dt", _F),
+]
+
+
+class Config(C.Structure):
+    _fields_ = CONFIG_FIELDS
+
+    def update(self, **kw):
+        for k, v in kw.items():
+            if k == "gravity":
+                self.gravity[:] = [float(a) for a in v]
+            else:
+                if not hasattr(self, k):
+                    raise AttributeError(k)
+                setattr(self, k, int(v) if isinstance(v, bool) else v)
+        return self
+
+
+_D = C.c_double
+DIAG_FIELDS = [
+    ("time", _D), ("step", C.c_longlong), ("dt", _D),
+    ("n_total", _I), ("n_liquid", _I), ("n_vapor", _I), ("n_wall", _I),
+    ("mass_liquid", _D), ("mass_vapor", _D), ("mass_total", _D),
+    ("kinetic_energy", _D), ("enthalpy", _D), ("heat_input", _D),
+    ("evaporated_mass", _D), ("condensed_mass", _D), ("vented_mass", _D), ("vented_enthalpy", _D),
+    ("T_sat", _D), ("p_ullage", _D), ("max_speed", _D),
+    ("T_liquid_mean", _D), ("T_liquid_max", _D), ("T_vapor_mean", _D),
+    ("liquid_com", _F * 3), ("liquid_momentum", _F * 3),
+    ("splits", _I), ("merges", _I),
+    ("slosh_force", _F * 3), ("slosh_moment", _F * 3),
+    ("frame_acceleration", _F * 3), ("frame_angular_velocity", _F * 3),
+]
+
+
+class Diagnostics(C.Structure):
+    _fields_ = DIAG_FIELDS
+
+    def as_dict(self):
+        out = {}
+        for name, typ in DIAG_FIELDS:
+            v = getattr(self, name)
+            out[name] = tuple(float(a) for a in v) if isinstance(v, C.Array) else v
+        return out
+
+
+class HostParticles(C.Structure):
+    _fields_ = [("n", _I), ("x", C.c_void_p), ("v", C.c_void_p), ("nrm", C.c_void_p), ("m", C.c_void_p),
+                ("rho", C.c_void_p), ("T", C.c_void_p), ("phase", C.c_void_p), ("flags", C.c_void_p),
+                ("id", C.c_void_p)]
+
+
+class CryoError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def host_particles(arrays: dict, keep: list):
+    """Packs a dict of numpy arrays into a HostParticles struct.  `keep`
+    receives the converted arrays so they outlive the call."""
+    def conv(name, dtype, shape_last=None):
+        a = arrays.get(name)
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dtype)
+        keep.append(a)
+        return a
+    x = conv("x", np.float32)
+    hp = HostParticles()
+    hp.n = int(x.shape[0])
+    hp.x = _ptr(x)
+    hp.v = _ptr(conv("v", np.float32))
+    hp.nrm = _ptr(conv("nrm", np.float32))
+    hp.m = _ptr(conv("m", np.float32))
+    hp.rho = _ptr(conv("rho", np.float32))
+    hp.T = _ptr(conv("T", np.float32))
+    hp.phase = _ptr(conv("phase", np.uint8))
+    hp.flags = _ptr(conv("flags", np.uint8))
+    hp.id = _ptr(conv("id", np.uint32))
+    return hp
+
+
+def field_dtype(name, real=np.float32):
+    if name in U8_FIELDS:
+        return np.uint8
+    if name in U32_FIELDS:
+        return np.uint32
+    return real
+
+
+def field_shape(name, n):
+    return (n, 3) if name in VEC_FIELDS else (n,)
+
+
+# SolverConfig defaults (sph_solver.hpp:20-91); cryo_config_default() in the
+# library returns the same values (checked by the CPU tests).
+CONFIG_DEFAULTS = dict(
+    dx=0.005, h_factor=1.3, kernel=1, density_mode=0, normalize_initial_masses=1, gravity=(0.0, 0.0, -9.81),
+    velocity_scale=0.0, sound_speed=0.0, tait_gamma=7.0, background_pressure=-1.0, vapor_stiffness=-1.0,
+    clamp_negative_pressure=0, transport_velocity=1, transport_background_factor=2.0, transport_stress=0,
+    transport_interface_only=1, particle_shifting=0, shifting_strength=0.25, artificial_viscosity=0.02,
+    artificial_viscosity_vapor=0.2, delta_sph=0.1, no_slip=1, sps_turbulence=0, smagorinsky_cs=0.12,
+    surface_tension=1, contact_angle_deg=90.0, contact_angle_wall_weight=0.01, wall_colour=1, wetting_model=0,
+    csf_smooth_normals=0, csf_balanced=0, akinci_gamma=-1.0, akinci_beta=-1.0, thermal=1, phase_change=1,
+    wall_thermal_bc=0, heater_power=0.0, conductivity_scale=1.0, lee_evaporation=10.0, lee_condensation=10.0,
+    thermo_mode=0, vent_relaxation=0.02, merge_ratio=0.3, split_ratio=2.0, max_transfer_fraction=0.25,
+    phase_change_density_limit=0.01, vapor_mass_rebalance=1.0, cfl=0.25, viscous_number=0.125,
+    force_number=0.25, capillary_number=0.25, thermal_number=0.1, dt_max=1e-2, dt_min=1e-9, fixed_dt=0.0)
+
+# Fluid presets (fluid_properties.cpp:16-79).
+FLUID_PRESETS = {
+    FLUID_LH2: dict(rho_liquid=70.85, rho_vapor=1.338, mu_liquid=1.33e-5, mu_vapor=1.11e-6, k_liquid=0.1034,
+                    k_vapor=0.0166, cp_liquid=9770.0, cp_vapor=12200.0, sigma=1.93e-3, h_fg=445.6e3, T_sat=20.37,
+                    p_sat=101325.0, R_gas=4124.2),
+    FLUID_LN2: dict(rho_liquid=806.1, rho_vapor=4.61, mu_liquid=1.61e-4, mu_vapor=5.4e-6, k_liquid=0.1446,
+                    k_vapor=0.0074, cp_liquid=2042.0, cp_vapor=1123.0, sigma=8.85e-3, h_fg=199.2e3, T_sat=77.36,
+                    p_sat=101325.0, R_gas=296.8),
+    FLUID_LOX: dict(rho_liquid=1141.0, rho_vapor=4.47, mu_liquid=1.96e-4, mu_vapor=6.9e-6, k_liquid=0.152,
+                    k_vapor=0.0084, cp_liquid=1699.0, cp_vapor=972.0, sigma=13.2e-3, h_fg=213.1e3, T_sat=90.19,
+                    p_sat=101325.0, R_gas=259.8),
+    FLUID_LCH4: dict(rho_liquid=422.4, rho_vapor=1.816, mu_liquid=1.17e-4, mu_vapor=4.4e-6, k_liquid=0.184,
+                     k_vapor=0.0119, cp_liquid=3481.0, cp_vapor=2218.0, sigma=13.4e-3, h_fg=510.8e3, T_sat=111.67,
+                     p_sat=101325.0, R_gas=518.3),
+    FLUID_H2O: dict(rho_liquid=998.2, rho_vapor=0.598, mu_liquid=1.0e-3, mu_vapor=1.23e-5, k_liquid=0.598,
+                    k_vapor=0.0248, cp_liquid=4182.0, cp_vapor=2080.0, sigma=0.0728, h_fg=2.257e6, T_sat=373.15,
+                    p_sat=101325.0, R_gas=461.5),
+    FLUID_CUSTOM: dict(rho_liquid=1000.0, rho_vapor=1.0, mu_liquid=1e-3, mu_vapor=1e-5, k_liquid=0.6,
+                       k_vapor=0.025, cp_liquid=4180.0, cp_vapor=2000.0, sigma=0.072, h_fg=2.26e6, T_sat=373.15,
+                       p_sat=101325.0, R_gas=461.5),
+}
+
+
+def py_config(**kw):
+    """Config filled from CONFIG_DEFAULTS (no library needed)."""
+    c = Config()
+    c.update(**CONFIG_DEFAULTS)
+    return c.update(**kw)
+
+
+def py_fluid(which):
+    f = Fluid()
+    for k, v in FLUID_PRESETS[which].items():
+        setattr(f, k, v)
+    return f
+
+
+_lib = None
+
+
+def lib_path():
+    return os.path.join(HERE, LIB_NAME)
+
+
+def load(path=None):
+    """Loads libcryosph_b200.so and declares the entry points (idempotent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or lib_path()
+    if not os.path.exists(p):
+        raise ImportError(f"{LIB_NAME} is not built (expected at {p}); run build.py")
+    L = C.CDLL(p)
+    vp, ip, i, f, d = C.c_void_p, C.POINTER(C.c_int), C.c_int, C.c_float, C.c_double
+    fp, dp = C.POINTER(C.c_float), C.POINTER(C.c_double)
+    decl = {
+        "cryo_abi_version": (i, []),
+        "cryo_config_default": (None, [C.POINTER(Config)]),
+        "cryo_fluid_preset": (i, [i, C.POINTER(Fluid)]),
+        "cryo_saturation_temperature": (f, [C.POINTER(Fluid), f]),
+        "cryo_saturation_pressure": (f, [C.POINTER(Fluid), f]),
+        "cryo_create": (i, [C.POINTER(Config), C.POINTER(Fluid), i, C.POINTER(vp)]),
+        "cryo_destroy": (None, [vp]),
+        "cryo_last_error": (C.c_char_p, [vp]),
+        "cryo_device_name": (i, [i, C.c_char_p, i]),
+        "cryo_device_count": (i, []),
+        "cryo_stream": (C.c_size_t, [vp]),
+        "cryo_set_particles": (i, [vp, C.POINTER(HostParticles), fp, fp]),
+        "cryo_step": (i, [vp]),
+        "cryo_run_steps": (i, [vp, C.c_longlong]),
+        "cryo_run_until": (i, [vp, d]),
+        "cryo_relax": (i, [vp, d, f]),
+        "cryo_next_dt": (i, [vp, dp]),
+        "cryo_synchronize": (i, [vp]),
+        "cryo_time": (i, [vp, dp, C.POINTER(C.c_longlong), dp]),
+        "cryo_num_particles": (i, [vp, ip]),
+        "cryo_capacity": (i, [vp, ip]),
+        "cryo_diagnostics": (i, [vp, C.POINTER(Diagnostics)]),
+        "cryo_download": (i, [vp, vp]),
+        "cryo_get_field": (i, [vp, i, vp, C.c_size_t]),
+        "cryo_set_gravity": (i, [vp, fp]),
+        "cryo_set_frame_motion": (i, [vp, fp, fp, fp, fp]),
+        "cryo_set_maneuver": (i, [vp, i, dp, fp, fp, fp]),
+        "cryo_clear_frame_motion": (i, [vp]),
+        "cryo_set_heater_power": (i, [vp, f]),
+        "cryo_set_contact_angle": (i, [vp, f]),
+        "cryo_damp_velocities": (i, [vp, f]),
+        "cryo_maneuver_evaluate": (i, [i, dp, fp, fp, d, fp, fp, fp]),
+        "cryo_probe_pressure": (i, [vp, fp, i, fp]),
+        "cryo_sound_speed": (i, [vp, fp]),
+        "cryo_smoothing_length": (i, [vp, fp]),
+        "cryo_pass": (i, [vp, i]),
+        "cryo_grid_info": (i, [vp, ip, ip, ip, ip, fp, fp]),
+        "cryo_grid_tables": (i, [vp, vp, vp, vp, vp]),
+        "cryo_neighbor_lists": (i, [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "cryo_set_pass_dt": (i, [vp, f]),
+        "cryo_device_status": (i, [vp, C.POINTER(C.c_uint)]),
+        "cryo_state_size": (i, [vp, C.POINTER(C.c_size_t)]),
+        "cryo_save_state": (i, [vp, vp, C.c_size_t]),
+        "cryo_load_state": (i, [vp, vp, C.c_size_t]),
+        "cryo_set_graph_mode": (i, [vp, i]),
+        "cryo_set_neighbor_mode": (i, [vp, i]),
+    }
+    for name, (res, args) in decl.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def config_default(lib=None, **kw):
+    L = lib or load()
+    c = Config()
+    L.cryo_config_default(C.byref(c))
+    return c.update(**kw)
+
+
+def fluid_preset(which, lib=None):
+    L = lib or load()
+    f = Fluid()
+    rc = L.cryo_fluid_preset(which, C.byref(f))
+    if rc:
+        raise CryoError(rc, "unknown fluid preset")
+    return f
+
+
+def vec3(v):
+    return (C.c_float * 3)(*[float(a) for a in v])
+
+
+class Context:
+    """Thin RAII wrapper over a cryo_ctx (used by the parity tests)."""
+
+    def __init__(self, cfg: Config, fluid: Fluid, device=0, lib=None):
+        self.L = lib or load()
+        self.h = C.c_void_p()
+        rc = self.L.cryo_create(C.byref(cfg), C.byref(fluid), device, C.byref(self.h))
+        if rc:
+            raise CryoError(rc, "cryo_create failed")
+
+    def close(self):
+        if self.h:
+            self.L.cryo_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != CRYO_OK:
+            msg = self.L.cryo_last_error(self.h)
+            raise CryoError(rc, msg.decode() if msg else "")
+
+    def set_particles(self, arrays, lo, hi):
+        keep = []
+        hp = host_particles(arrays, keep)
+        self.check(self.L.cryo_set_particles(self.h, C.byref(hp), vec3(lo), vec3(hi)))
+
+    def num_particles(self):
+        n = C.c_int()
+        self.check(self.L.cryo_num_particles(self.h, C.byref(n)))
+        return n.value
+
+    def field(self, name):
+        n = self.num_particles()
+        out = np.empty(field_shape(name, n), dtype=field_dtype(name))
+        self.check(self.L.cryo_get_field(self.h, FIELD_ID[name], out.ctypes.data_as(C.c_void_p), out.nbytes))
+        return out
+
+    def run_pass(self, name):
+        self.check(self.L.cryo_pass(self.h, PASS_ID[name]))
+
+    def set_pass_dt(self, dt):
+        self.check(self.L.cryo_set_pass_dt(self.h, float(dt)))
+
+    def step(self, n=1):
+        self.check(self.L.cryo_run_steps(self.h, int(n)))
+
+    def relax(self, duration, damping=0.98):
+        self.check(self.L.cryo_relax(self.h, float(duration), float(damping)))
+
+    def next_dt(self):
+        d = C.c_double()
+        self.check(self.L.cryo_next_dt(self.h, C.byref(d)))
+        return d.value
+
+    def diagnostics(self):
+        d = Diagnostics()
+        self.check(self.L.cryo_diagnostics(self.h, C.byref(d)))
+        return d
+
+    def time(self):
+        t, s, dt = C.c_double(), C.c_longlong(), C.c_double()
+        self.check(self.L.cryo_time(self.h, C.byref(t), C.byref(s), C.byref(dt)))
+        return t.value, s.value, dt.value
+
+    def grid_info(self):
+        nc, nx, ny, nz = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        o, cell = (C.c_float * 3)(), C.c_float()
+        self.check(self.L.cryo_grid_info(self.h, C.byref(nc), C.byref(nx), C.byref(ny), C.byref(nz), o,
+                                         C.byref(cell)))
+        return dict(num_cells=nc.value, nx=nx.value, ny=ny.value, nz=nz.value, origin=tuple(o), cell=cell.value)
+
+    def grid_tables(self):
+        info = self.grid_info()
+        n = self.num_particles()
+        keys = np.empty(n, np.uint32)
+        perm = np.empty(n, np.uint32)
+        cs = np.empty(info["num_cells"], np.int32)
+        ce = np.empty(info["num_cells"], np.int32)
+        self.check(self.L.cryo_grid_tables(self.h, _ptr(keys), _ptr(perm), _ptr(cs), _ptr(ce)))
+        return keys, perm, cs, ce
+
+    def neighbor_lists(self):
+        n = self.num_particles()
+        counts = np.empty(n, np.int32)
+        total = C.c_longlong()
+        self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), None, 0, C.byref(total)))
+        lst = np.empty(max(total.value, 1), np.int32)
+        self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), _ptr(lst), total.value, C.byref(total)))
+        return counts, lst[: total.value]
