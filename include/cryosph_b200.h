@@ -235,8 +235,14 @@ int cryo_diagnostics(cryo_ctx* ctx, cryo_diagnostics_t* out);
 /* Solver::particles (persistent arrays).  out->n must be >= the particle count;
  * on return out->n holds the count. */
 int cryo_download(cryo_ctx* ctx, cryo_host_particles_out_t* out);
-/* One per-particle field (CRYO_F_*) into a host buffer of `cap` bytes. */
+/* One per-particle field (CRYO_F_*) into a host buffer of `cap` bytes.
+ * Vector fields: 3 floats per particle; phase/flags: uint8; id: uint32. */
 int cryo_get_field(cryo_ctx* ctx, int field, void* host_out, size_t cap);
+/* Overwrites one per-particle field of the current particles (same layout as
+ * cryo_get_field, `bytes` must match the particle count).  Test and
+ * checkpoint helper: the DeviceArray::upload of ParticleSystem fields
+ * (cuda_utils.cuh:214-217). */
+int cryo_set_field(cryo_ctx* ctx, int field, const void* host_in, size_t bytes);
 
 /* Run-time controls (sph_solver.cu:655-705). */
 int cryo_set_gravity(cryo_ctx* ctx, const float* g3);

@@ -258,6 +258,7 @@ def load(path=None):
         "cryo_diagnostics": (i, [vp, C.POINTER(Diagnostics)]),
         "cryo_download": (i, [vp, vp]),
         "cryo_get_field": (i, [vp, i, vp, C.c_size_t]),
+        "cryo_set_field": (i, [vp, i, vp, C.c_size_t]),
         "cryo_set_gravity": (i, [vp, fp]),
         "cryo_set_frame_motion": (i, [vp, fp, fp, fp, fp]),
         "cryo_set_maneuver": (i, [vp, i, dp, fp, fp, fp]),
@@ -350,6 +351,17 @@ class Context:
         out = np.empty(field_shape(name, n), dtype=field_dtype(name))
         self.check(self.L.cryo_get_field(self.h, FIELD_ID[name], out.ctypes.data_as(C.c_void_p), out.nbytes))
         return out
+
+    def set_field(self, name, data):
+        n = self.num_particles()
+        a = np.ascontiguousarray(data, dtype=field_dtype(name)).reshape(field_shape(name, n))
+        self.check(self.L.cryo_set_field(self.h, FIELD_ID[name], a.ctypes.data_as(C.c_void_p), a.nbytes))
+
+    def set_graph_mode(self, on):
+        self.check(self.L.cryo_set_graph_mode(self.h, int(bool(on))))
+
+    def run_until(self, t):
+        self.check(self.L.cryo_run_until(self.h, float(t)))
 
     def run_pass(self, name):
         self.check(self.L.cryo_pass(self.h, PASS_ID[name]))

@@ -1,0 +1,1574 @@
+// cryo_abi.cu -- host side of the B200 hot path: the context (device memory,
+// stream, CUDA graphs), the parameter lowering (Solver::init_params), the
+// step orchestration and every extern "C" entry point of cryosph_b200.h.
+//
+// Nothing here throws across the ABI: each entry point runs inside guard(),
+// which maps exceptions to status codes the way the reference's exceptions
+// map to Python (invalid_argument -> CRYO_EINVAL, out_of_range -> CRYO_ERANGE,
+// runtime_error -> CRYO_ERUNTIME, CUDA failures -> CRYO_ECUDA).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cryo_kernels.cuh"
+
+using namespace cryo;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
+};
+
+#define CK(expr)                                                                                 \
+  do {                                                                                           \
+    const cudaError_t e__ = (expr);                                                              \
+    if (e__ != cudaSuccess)                                                                      \
+      throw CudaError(std::string("CUDA error '") + cudaGetErrorString(e__) + "' at " #expr);   \
+  } while (0)
+
+#define LAUNCH_CHECK() CK(cudaGetLastError())
+
+struct Persist {
+  float4 *xp = nullptr, *vT = nullptr, *vt = nullptr, *nrm = nullptr, *mrps = nullptr;
+  uint32_t* id = nullptr;
+};
+
+// One device allocation carved into 256-byte aligned arrays.
+struct Arena {
+  char* base = nullptr;
+  size_t size = 0, used = 0;
+  void release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    size = used = 0;
+  }
+  template <class T>
+  T* take(size_t n) {
+    const size_t bytes = (n * sizeof(T) + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + used);
+    used += bytes;
+    return p;
+  }
+};
+
+size_t particle_bytes(size_t cap) {
+  const size_t a = 256;
+  auto r = [&](size_t b) { return (b + a - 1) / a * a; };
+  size_t t = 0;
+  for (int s = 0; s < 2; ++s) t += 5 * r(cap * 16) + r(cap * 4);    // persistent sets
+  t += 7 * r(cap * 16) + 4 * r(cap * 4);                            // scratch
+  t += 5 * r(cap * 4);                                              // sort keys/vals, split flags
+  const size_t tiles = (cap + RS_TILE - 1) / RS_TILE + 1;
+  t += r(tiles * RS_BINS * 4);                                      // radix histogram
+  const size_t chunks = cap / kChunk + 2;
+  t += r(chunks * 32 * 8);                                          // reduction partials
+  t += r(64 * 8) + r(64);                                           // diagnostics out, tickets
+  return t;
+}
+
+}  // namespace
+
+struct cryo_ctx {
+  cryo_config_t cfg{};
+  cryo_fluid_t fluid{};
+  Params P{};
+  int device = 0;
+  int sm_count = 148;
+  cudaStream_t stream = nullptr;
+  std::string err;
+
+  // particle storage
+  int capacity = 0;
+  Arena arena;
+  Persist set[2];
+  int cur = 0;
+  float4 *a4 = nullptr, *ab4 = nullptr, *fw = nullptr, *mw = nullptr, *vwp = nullptr, *ns4 = nullptr,
+         *pc = nullptr;
+  float *rmin = nullptr, *wall_w = nullptr, *heat_w = nullptr, *nu_t = nullptr;
+  uint32_t *keys_a = nullptr, *keys_b = nullptr, *vals_a = nullptr, *vals_b = nullptr, *split_flag = nullptr;
+  uint32_t* hist = nullptr;
+  double* partials = nullptr;
+  int max_chunks = 0;
+  double* diag_out = nullptr;
+  unsigned* ticket = nullptr;
+  const uint32_t* sorted_keys = nullptr;  // of the last grid build
+  const uint32_t* sorted_perm = nullptr;
+  int last_sort_n = 0;
+
+  // grid
+  int* cell_begin = nullptr;
+  int cell_cap = 0;
+
+  // scalar block
+  DynState* dyn = nullptr;   // device
+  DynState* hdyn = nullptr;  // pinned host mirror
+
+  // maneuver table (device)
+  double* man_t = nullptr;
+  float* man_acc = nullptr;
+  float* man_omega = nullptr;
+  int man_cap = 0;
+  // host copy of the table (for host-side evaluation at set time)
+  std::vector<double> h_man_t;
+  std::vector<float> h_man_acc, h_man_omega;
+
+  // solver state on the host side
+  bool has_particles = false, initialized = false, has_vapor = false;
+  float char_length = 0;
+  float pass_dt = 0;
+
+  // execution
+  bool graph_mode = true;
+  bool graph_valid[2] = {false, false};
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  bool use_lists = true;
+
+  ~cryo_ctx() {
+    for (int k = 0; k < 2; ++k)
+      if (graph[k]) cudaGraphExecDestroy(graph[k]);
+    if (stream) cudaStreamSynchronize(stream);
+    arena.release();
+    if (cell_begin) cudaFree(cell_begin);
+    if (dyn) cudaFree(dyn);
+    if (hdyn) cudaFreeHost(hdyn);
+    if (man_t) cudaFree(man_t);
+    if (man_acc) cudaFree(man_acc);
+    if (man_omega) cudaFree(man_omega);
+    if (stream) cudaStreamDestroy(stream);
+  }
+
+  // ------------------------------------------------------------ helpers
+  View view(int s) const {
+    View V{};
+    V.xp = set[s].xp; V.vT = set[s].vT; V.vt = set[s].vt; V.nrm = set[s].nrm; V.mrps = set[s].mrps;
+    V.id = set[s].id;
+    V.a4 = a4; V.ab4 = ab4; V.fw = fw; V.mw = mw; V.vwp = vwp; V.ns4 = ns4; V.pc = pc;
+    V.rmin = rmin; V.wall_w = wall_w; V.heat_w = heat_w; V.nu_t = nu_t;
+    V.cell_begin = cell_begin;
+    V.dyn = dyn;
+    V.man_t = man_t; V.man_acc = man_acc; V.man_omega = man_omega;
+    V.partials = partials;
+    V.counters = ticket;
+    V.capacity = capacity;
+    return V;
+  }
+  Reduce reduce() const { return Reduce{partials, ticket, max_chunks}; }
+  int grid_blocks() const {
+    const int need = (capacity + kBlock - 1) / kBlock;
+    return std::max(1, std::min(need, sm_count * 8));
+  }
+  void invalidate_graphs() {
+    for (int k = 0; k < 2; ++k) {
+      if (graph[k]) cudaGraphExecDestroy(graph[k]);
+      graph[k] = nullptr;
+      graph_valid[k] = false;
+    }
+  }
+  void sync() { CK(cudaStreamSynchronize(stream)); }
+  void pull() {  // device scalar block -> host mirror
+    CK(cudaMemcpyAsync(hdyn, dyn, sizeof(DynState), cudaMemcpyDeviceToHost, stream));
+    sync();
+  }
+  void push() {  // host mirror -> device scalar block
+    CK(cudaMemcpyAsync(dyn, hdyn, sizeof(DynState), cudaMemcpyHostToDevice, stream));
+    sync();
+  }
+
+  // -------------------------------------------------------- allocation
+  void allocate(int cap) {
+    sync();
+    invalidate_graphs();
+    Arena a;
+    a.size = particle_bytes((size_t)cap);
+    CK(cudaMalloc(&a.base, a.size));
+    CK(cudaMemsetAsync(a.base, 0, a.size, stream));
+    Persist ns[2];
+    for (int s = 0; s < 2; ++s) {
+      ns[s].xp = a.take<float4>(cap); ns[s].vT = a.take<float4>(cap); ns[s].vt = a.take<float4>(cap);
+      ns[s].nrm = a.take<float4>(cap); ns[s].mrps = a.take<float4>(cap); ns[s].id = a.take<uint32_t>(cap);
+    }
+    float4* na4 = a.take<float4>(cap); float4* nab4 = a.take<float4>(cap); float4* nfw = a.take<float4>(cap);
+    float4* nmw = a.take<float4>(cap); float4* nvwp = a.take<float4>(cap); float4* nns4 = a.take<float4>(cap);
+    float4* npc = a.take<float4>(cap);
+    float* nrmin = a.take<float>(cap); float* nwall = a.take<float>(cap); float* nheat = a.take<float>(cap);
+    float* nnut = a.take<float>(cap);
+    uint32_t* nka = a.take<uint32_t>(cap); uint32_t* nkb = a.take<uint32_t>(cap);
+    uint32_t* nva = a.take<uint32_t>(cap); uint32_t* nvb = a.take<uint32_t>(cap);
+    uint32_t* nsf = a.take<uint32_t>(cap);
+    const size_t tiles = (size_t)(cap + RS_TILE - 1) / RS_TILE + 1;
+    uint32_t* nhist = a.take<uint32_t>(tiles * RS_BINS);
+    const int nchunks = cap / kChunk + 2;
+    double* npart = a.take<double>((size_t)nchunks * 32);
+    double* ndiag = a.take<double>(64);
+    unsigned* ntick = a.take<unsigned>(64);
+    if (a.used > a.size) throw std::runtime_error("internal: arena overflow");
+    // keep the first n particles of every array (ParticleSystem::grow,
+    // particle_system.cpp:66-71)
+    if (arena.base && capacity > 0) {
+      pull();
+      const size_t keep = (size_t)std::min(hdyn->n, cap);
+      auto cp = [&](void* dst, const void* src, size_t elem) {
+        if (keep) CK(cudaMemcpyAsync(dst, src, keep * elem, cudaMemcpyDeviceToDevice, stream));
+      };
+      for (int s = 0; s < 2; ++s) {
+        cp(ns[s].xp, set[s].xp, 16); cp(ns[s].vT, set[s].vT, 16); cp(ns[s].vt, set[s].vt, 16);
+        cp(ns[s].nrm, set[s].nrm, 16); cp(ns[s].mrps, set[s].mrps, 16); cp(ns[s].id, set[s].id, 4);
+      }
+      cp(na4, a4, 16); cp(nab4, ab4, 16); cp(nfw, fw, 16); cp(nmw, mw, 16); cp(nvwp, vwp, 16); cp(nns4, ns4, 16);
+      cp(npc, pc, 16); cp(nrmin, rmin, 4); cp(nwall, wall_w, 4); cp(nheat, heat_w, 4); cp(nnut, nu_t, 4);
+      sync();
+    }
+    arena.release();
+    arena = a;
+    set[0] = ns[0]; set[1] = ns[1];
+    a4 = na4; ab4 = nab4; fw = nfw; mw = nmw; vwp = nvwp; ns4 = nns4; pc = npc;
+    rmin = nrmin; wall_w = nwall; heat_w = nheat; nu_t = nnut;
+    keys_a = nka; keys_b = nkb; vals_a = nva; vals_b = nvb; split_flag = nsf;
+    hist = nhist; partials = npart; max_chunks = nchunks; diag_out = ndiag; ticket = ntick;
+    sorted_keys = nullptr;
+    sorted_perm = nullptr;
+    capacity = cap;
+    if (hdyn) {
+      pull();
+      hdyn->capacity = cap;
+      push();
+    }
+  }
+
+  // --------------------------------------------------- parameter lowering
+  void init_params();
+  void configure_grid(const float* lo, const float* hi);
+
+  // ------------------------------------------------------ step pieces
+  void grid_build(int src);               // keys of current positions, sort, cells, gather
+  void sort_and_gather(int src);          // after keys_a holds the keys
+  void evaluate_rates(int s, bool maxima_reset);
+  void enqueue_step(int s);
+  void launch_step();
+  void ensure_initialized();
+  void check_capacity();
+  void run_steps(long long n);
+  void run_until(double t_end);
+};
+
+// -------------------------------------------------------------------------
+// Solver::init_params (sph_solver.cu:292-405), host single precision in the
+// reference's order (the host compiler emits no FMA on x86-64 by default and
+// the build passes -ffp-contract=off).
+void cryo_ctx::init_params() {
+  const cryo_config_t& c = cfg;
+  Params& p = P;
+  const float dx = c.dx;
+  const float h = c.h_factor * dx;
+  p.ktype = c.kernel;
+  p.h = h;
+  p.inv_h = 1.0f / h;
+  p.support = 2.0f * h;
+  {
+    const float h3 = h * h * h;
+    p.knorm = (c.kernel == CRYO_KERNEL_CUBIC) ? 1.0f / (kPi * h3) : 21.0f / (16.0f * kPi * h3);
+  }
+  p.dx = dx;
+  p.support2 = p.support * p.support;
+  {
+    double sigma0 = 0;
+    const int r = (int)std::ceil(p.support / dx);
+    for (int k = -r; k <= r; ++k)
+      for (int j = -r; j <= r; ++j)
+        for (int i = -r; i <= r; ++i) sigma0 += kernel_W(p, dx * std::sqrt((float)(i * i + j * j + k * k)));
+    p.vol0 = (float)(1.0 / sigma0);
+  }
+  p.rho0[0] = fluid.rho_liquid;
+  p.rho0[1] = fluid.rho_vapor;
+  p.mu[0] = fluid.mu_liquid;
+  p.mu[1] = fluid.mu_vapor;
+  p.k[0] = fluid.k_liquid * c.conductivity_scale;
+  p.k[1] = fluid.k_vapor * c.conductivity_scale;
+  p.cp[0] = fluid.cp_liquid;
+  p.cp[1] = fluid.cp_vapor;
+  p.mref[0] = p.rho0[0] * p.vol0;
+  p.mref[1] = p.rho0[1] * p.vol0;
+
+  const bool st_on = c.surface_tension != CRYO_ST_NONE;
+  const V3 cg = v3(c.gravity[0], c.gravity[1], c.gravity[2]);
+  const float g = norm(cg);
+  float vref = c.velocity_scale;
+  auto mx = [](float a, float b) { return (a < b) ? b : a; };
+  if (!(vref > 0)) {
+    vref = std::sqrt(g * char_length);
+    if (st_on) vref = mx(vref, std::sqrt(fluid.sigma / (fluid.rho_liquid * h)));
+    vref = mx(vref, 1e-3f);
+  }
+  p.c0 = c.sound_speed > 0 ? c.sound_speed : 10.0f * vref;
+  p.tait_gamma = c.tait_gamma;
+  p.tait_B = p.rho0[0] * p.c0 * p.c0 / p.tait_gamma;
+  p.p_bg = c.background_pressure >= 0 ? c.background_pressure
+                                      : (has_vapor ? 0.1f * p.rho0[1] * p.c0 * p.c0 : 0.0f);
+  p.vapor_K = c.vapor_stiffness > 0 ? c.vapor_stiffness : (has_vapor ? p.rho0[1] * p.c0 * p.c0 : p.p_bg);
+  p.gas_R = p.vapor_K > 0 ? p.vapor_K / (p.rho0[1] * fluid.T_sat) : fluid.R_gas;
+  p.clamp_neg = c.clamp_negative_pressure ? 1 : 0;
+
+  p.alpha_av = c.artificial_viscosity;
+  p.alpha_av_vap = c.artificial_viscosity_vapor;
+  p.delta_sph = c.delta_sph;
+  p.density_mode = c.density_mode;
+  p.no_slip = c.no_slip ? 1 : 0;
+  p.sps = c.sps_turbulence ? 1 : 0;
+  p.smagorinsky_cs = c.smagorinsky_cs;
+  p.tvf = c.transport_velocity ? 1 : 0;
+  p.tvf_stress = c.transport_stress ? 1 : 0;
+  p.tvf_factor = c.transport_background_factor;
+  p.tvf_interface_only = c.transport_interface_only ? 1 : 0;
+  p.shift_strength = c.particle_shifting ? c.shifting_strength : 0.0f;
+  p.tvf_sigma_min = has_vapor ? 0.0f : 0.95f / p.vol0;
+
+  p.st_model = c.surface_tension;
+  p.sigma = st_on ? fluid.sigma : 0.0f;
+  const float theta = c.contact_angle_deg * kPi / 180.0f;
+  p.cos_theta = std::cos(theta);
+  p.sin_theta = std::sin(theta);
+  p.wall_adhesion_weight = c.contact_angle_wall_weight;
+  p.wall_colour = c.wall_colour ? 1 : 0;
+  p.wetting_model = c.wetting_model;
+  p.csf_smooth = c.csf_smooth_normals ? 1 : 0;
+  p.csf_balanced = c.csf_balanced ? 1 : 0;
+  p.normal_eps = 0.1f / h;
+  {
+    // Akinci strengths (sph_solver.cu:372-386), Simpson rule of
+    // radial_moment4 (sph_solver.cu:181-193)
+    const double sup = p.support;
+    auto moment = [&](bool adh) {
+      const int nn = 2000;
+      const double hs = sup / nn;
+      double acc = 0;
+      for (int k = 0; k <= nn; ++k) {
+        const double r = k * hs;
+        const double w = (k == 0 || k == nn) ? 1.0 : (k % 2 ? 4.0 : 2.0);
+        const double f = adh ? (double)akinci_adhesion((float)r, (float)sup) : (double)akinci_cohesion((float)r, (float)sup);
+        acc += w * r * r * r * r * f;
+      }
+      return acc * hs / 3.0;
+    };
+    const double i_coh = moment(false), i_adh = moment(true);
+    const double rho = fluid.rho_liquid;
+    const double gamma = c.akinci_gamma >= 0
+                             ? (double)c.akinci_gamma
+                             : (i_coh > 0 ? 8.0 * fluid.sigma / ((double)kPi * rho * rho * i_coh) : 0.0);
+    p.akinci_gamma = (float)gamma;
+    p.akinci_beta = c.akinci_beta >= 0
+                        ? c.akinci_beta
+                        : (float)(i_adh > 0 ? gamma * (i_coh / i_adh) * 0.5 * (1.0 + (double)p.cos_theta) : 0.0);
+  }
+  p.thermal = c.thermal ? 1 : 0;
+  p.phase_change = c.phase_change ? 1 : 0;
+  p.wall_bc = c.wall_thermal_bc;
+  p.T_wall = fluid.T_sat;
+  p.T_ref = fluid.T_sat;
+  p.h_fg = fluid.h_fg;
+  p.lee_evap = c.lee_evaporation;
+  p.lee_cond = c.lee_condensation;
+  p.max_transfer_fraction = c.max_transfer_fraction;
+  p.pc_density_limit = c.phase_change_density_limit;
+  p.vapor_rebalance = c.vapor_mass_rebalance;
+  p.merge_ratio = c.merge_ratio;
+  p.split_ratio = c.split_ratio;
+  p.heat_power = c.heater_power;
+
+  p.cfg_phase_change = c.phase_change ? 1 : 0;
+  p.thermo_closed = c.thermo_mode == CRYO_THERMO_CLOSED ? 1 : 0;
+  p.has_vapor = has_vapor ? 1 : 0;
+  p.csf_active = (c.surface_tension == CRYO_ST_CSF && has_vapor) ? 1 : 0;
+  p.vent_relaxation = c.vent_relaxation;
+  p.cfl = c.cfl;
+  p.viscous_number = c.viscous_number;
+  p.force_number = c.force_number;
+  p.capillary_number = c.capillary_number;
+  p.thermal_number = c.thermal_number;
+  p.dt_max = c.dt_max;
+  p.dt_min = c.dt_min;
+  p.fixed_dt = c.fixed_dt;
+  p.f_rho_l = fluid.rho_liquid;
+  p.f_rho_v = fluid.rho_vapor;
+  p.f_T_sat = fluid.T_sat;
+  p.f_p_sat = fluid.p_sat;
+  p.f_R_gas = fluid.R_gas;
+  p.f_h_fg = fluid.h_fg;
+}
+
+// SpatialHash::configure (spatial_hash.cu:15-30) + view() (:36-46)
+void cryo_ctx::configure_grid(const float* lo, const float* hi) {
+  const float cell = P.support;
+  if (!(cell > 0)) throw std::invalid_argument("SpatialHash: cell size must be positive");
+  P.cell = cell;
+  P.ox = lo[0] - cell;
+  P.oy = lo[1] - cell;
+  P.oz = lo[2] - cell;
+  const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+  P.nx = std::max(1, (int)std::ceil(ex / cell) + 2);
+  P.ny = std::max(1, (int)std::ceil(ey / cell) + 2);
+  P.nz = std::max(1, (int)std::ceil(ez / cell) + 2);
+  const long long cells = (long long)P.nx * P.ny * P.nz;
+  if (cells > 400000000LL) throw std::runtime_error("SpatialHash: grid too large; increase the cell size");
+  P.num_cells = (int)cells;
+  P.inv_cell = 1.0f / cell;
+  int bits = 0;
+  while (bits < 32 && ((uint64_t)1 << bits) <= (uint64_t)P.num_cells) ++bits;  // sentinel fits
+  P.key_bits = std::max(bits, 1);
+  if (cell_cap < P.num_cells + 2) {
+    if (cell_begin) CK(cudaFree(cell_begin));
+    CK(cudaMalloc(&cell_begin, (size_t)(P.num_cells + 2) * sizeof(int)));
+    cell_cap = P.num_cells + 2;
+  }
+  CK(cudaMemsetAsync(cell_begin, 0, (size_t)(P.num_cells + 2) * sizeof(int), stream));
+}
+
+// Keys of the current positions in keys_a, then sort, cell table and gather
+// (SpatialHash::build, spatial_hash.cu:48-114).  Flips `cur`.
+void cryo_ctx::grid_build(int src) {
+  const int G = grid_blocks();
+  k_keys<<<G, kBlock, 0, stream>>>(P, view(src), keys_a);
+  LAUNCH_CHECK();
+  sort_and_gather(src);
+}
+
+void cryo_ctx::sort_and_gather(int src) {
+  const int G = grid_blocks();
+  const int tiles = (capacity + RS_TILE - 1) / RS_TILE;
+  const uint32_t* kin = keys_a;
+  const uint32_t* vin = nullptr;
+  uint32_t* kout = keys_b;
+  uint32_t* vout = vals_b;
+  for (int shift = 0; shift < P.key_bits; shift += RS_BITS) {
+    const int bits = std::min(RS_BITS, P.key_bits - shift);
+    k_rs_upsweep<<<tiles, RS_THREADS, 0, stream>>>(kin, shift, bits, dyn, hist);
+    LAUNCH_CHECK();
+    k_rs_scan<<<1, 1024, 0, stream>>>(hist, dyn);
+    LAUNCH_CHECK();
+    k_rs_downsweep<<<tiles, RS_THREADS, 0, stream>>>(kin, vin, kout, vout, shift, bits, dyn, hist);
+    LAUNCH_CHECK();
+    kin = kout;
+    vin = vout;
+    kout = (kout == keys_b) ? keys_a : keys_b;
+    vout = (vout == vals_b) ? vals_a : vals_b;
+  }
+  sorted_keys = kin;
+  sorted_perm = vin;
+  k_cells<<<G, kBlock, 0, stream>>>(P, kin, dyn, cell_begin);
+  LAUNCH_CHECK();
+  k_gather<<<G, kBlock, 0, stream>>>(view(src), view(1 - src), vin);
+  LAUNCH_CHECK();
+}
+
+// Solver::evaluate_rates (sph_solver.cu:449-480) on set s.
+void cryo_ctx::evaluate_rates(int s, bool maxima_reset) {
+  const int G = grid_blocks();
+  const View V = view(s);
+  if (maxima_reset) {
+    k_begin_step<<<1, 1, 0, stream>>>(P, V, BEGIN_RATES);
+    LAUNCH_CHECK();
+  }
+  k_density<<<G, kBlock, 0, stream>>>(P, V, 1);
+  LAUNCH_CHECK();
+  k_wall<<<G, kBlock, 0, stream>>>(P, V);
+  LAUNCH_CHECK();
+  k_interface<<<G, kBlock, 0, stream>>>(P, V, reduce(), P.thermal ? 1 : 0);
+  LAUNCH_CHECK();
+  if (P.sps) {
+    k_sps<<<G, kBlock, 0, stream>>>(P, V);
+    LAUNCH_CHECK();
+  }
+  if (P.csf_active && P.csf_smooth) {
+    k_smooth_normals<<<G, kBlock, 0, stream>>>(P, V);
+    LAUNCH_CHECK();
+  }
+  int what = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
+  if (P.csf_active) what |= FORCE_CSF;
+  if (P.st_model == CRYO_ST_AKINCI) what |= FORCE_AKINCI;
+  if (P.density_mode == CRYO_DENSITY_CONTINUITY) what |= FORCE_DRHO;
+  if (P.thermal) what |= FORCE_THERMAL;
+  k_forces<<<G, kBlock, 0, stream>>>(P, V, what);
+  LAUNCH_CHECK();
+}
+
+// One Solver::step (sph_solver.cu:511-533) starting from set s; all device side.
+void cryo_ctx::enqueue_step(int s) {
+  const int G = grid_blocks();
+  k_begin_step<<<1, 1, 0, stream>>>(P, view(s), BEGIN_STEP);
+  LAUNCH_CHECK();
+  k_kick_drift_keys<<<G, kBlock, 0, stream>>>(P, view(s), keys_a);
+  LAUNCH_CHECK();
+  sort_and_gather(s);
+  const int d = 1 - s;
+  const View V = view(d);
+  evaluate_rates(d, false);
+  k_kick<<<G, kBlock, 0, stream>>>(P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
+  LAUNCH_CHECK();
+  if (P.shift_strength > 0.0f) {
+    k_shift_compute<<<G, kBlock, 0, stream>>>(P, V);
+    LAUNCH_CHECK();
+    k_shift_apply<<<G, kBlock, 0, stream>>>(P, V);
+    LAUNCH_CHECK();
+  }
+  if (P.cfg_phase_change) {
+    const Reduce R = reduce();
+    k_pc_normalize<<<G, kBlock, 0, stream>>>(P, V, R, 1);
+    LAUNCH_CHECK();
+    k_pc_apply<<<G, kBlock, 0, stream>>>(P, V, 1);
+    LAUNCH_CHECK();
+    const bool reb = P.vapor_rebalance > 0.0f && has_vapor;
+    if (reb) {
+      k_rebalance1<<<G, kBlock, 0, stream>>>(P, V, 1);
+      LAUNCH_CHECK();
+    }
+    k_rebalance2_mark<<<G, kBlock, 0, stream>>>(P, V, R, split_flag, reb ? 1 : 0, 1);
+    LAUNCH_CHECK();
+    k_split<<<G, kBlock, 0, stream>>>(P, V, R, split_flag, 1);
+    LAUNCH_CHECK();
+    if (cfg.thermo_mode == CRYO_THERMO_VENTED && has_vapor) {
+      k_venting<<<G, kBlock, 0, stream>>>(P, V, R, cfg.vent_relaxation, 1);
+      LAUNCH_CHECK();
+    }
+  }
+  k_saturation<<<G, kBlock, 0, stream>>>(P, V, reduce(), 1);
+  LAUNCH_CHECK();
+}
+
+void cryo_ctx::launch_step() {
+  const int s = cur;
+  if (graph_mode) {
+    if (!graph_valid[s]) {
+      if (graph[s]) CK(cudaGraphExecDestroy(graph[s]));
+      graph[s] = nullptr;
+      cudaGraph_t g = nullptr;
+      CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue_step(s);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      CK(cudaStreamEndCapture(stream, &g));
+      CK(cudaGraphInstantiate(&graph[s], g, 0));
+      CK(cudaGraphDestroy(g));
+      graph_valid[s] = true;
+    }
+    CK(cudaGraphLaunch(graph[s], stream));
+  } else {
+    enqueue_step(s);
+  }
+  cur = 1 - s;
+}
+
+// Solver::ensure_initialized (sph_solver.cu:439-447)
+void cryo_ctx::ensure_initialized() {
+  if (initialized) return;
+  if (!has_particles) throw std::runtime_error("Solver: no particles loaded");
+  grid_build(cur);
+  cur = 1 - cur;
+  const int G = grid_blocks();
+  if (cfg.normalize_initial_masses) {
+    k_normalize_masses<<<G, kBlock, 0, stream>>>(P, view(cur));
+    LAUNCH_CHECK();
+  }
+  evaluate_rates(cur, true);
+  k_saturation<<<G, kBlock, 0, stream>>>(P, view(cur), reduce(), 0);
+  LAUNCH_CHECK();
+  initialized = true;
+}
+
+// Head-room for splits (sph_solver.cu:556-560), checked between steps.
+void cryo_ctx::check_capacity() {
+  pull();
+  if ((long long)hdyn->n * 4 > (long long)capacity * 3) allocate(capacity * 3 / 2 + 1024);
+}
+
+void cryo_ctx::run_steps(long long n) {
+  ensure_initialized();
+  for (long long k = 0; k < n; ++k) {
+    launch_step();
+    if ((k & 15) == 15) check_capacity();
+  }
+  check_capacity();
+}
+
+// Solver::run_until (sph_solver.cu:540-543): the steps are issued in batches
+// that cannot pass t_end (each step is at most dt_max), then one at a time.
+void cryo_ctx::run_until(double t_end) {
+  ensure_initialized();
+  pull();
+  while (hdyn->time < t_end) {
+    const double bound = cfg.fixed_dt > 0 ? (double)cfg.fixed_dt : (double)cfg.dt_max;
+    long long k = (long long)std::floor((t_end - hdyn->time) / bound);
+    k = std::max(1LL, std::min(k, 64LL));
+    for (long long s = 0; s < k; ++s) launch_step();
+    check_capacity();  // pulls the clock
+  }
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+thread_local std::string g_create_error;
+
+template <class F>
+int guard(cryo_ctx* ctx, F&& f) {
+  try {
+    f();
+    return CRYO_OK;
+  } catch (const std::invalid_argument& e) {
+    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
+    return CRYO_EINVAL;
+  } catch (const std::out_of_range& e) {
+    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
+    return CRYO_ERANGE;
+  } catch (const CudaError& e) {
+    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
+    return CRYO_ECUDA;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
+    return CRYO_ERUNTIME;
+  }
+}
+
+void set3(float* d, const float* s) { d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; }
+
+void fluid_from(int which, cryo_fluid_t* f) {
+  // FluidProperties presets (fluid_properties.cpp:16-79); custom = the
+  // struct defaults (fluid_properties.hpp:12-24).
+  auto put = [&](float rl, float rv, float ml, float mv, float kl, float kv, float cl, float cv, float s, float hfg,
+                 float ts, float ps, float R) {
+    *f = cryo_fluid_t{rl, rv, ml, mv, kl, kv, cl, cv, s, hfg, ts, ps, R};
+  };
+  switch (which) {
+    case CRYO_FLUID_LH2: put(70.85f, 1.338f, 1.33e-5f, 1.11e-6f, 0.1034f, 0.0166f, 9770.f, 12200.f, 1.93e-3f, 445.6e3f, 20.37f, 101325.f, 4124.2f); break;
+    case CRYO_FLUID_LN2: put(806.1f, 4.61f, 1.61e-4f, 5.4e-6f, 0.1446f, 0.0074f, 2042.f, 1123.f, 8.85e-3f, 199.2e3f, 77.36f, 101325.f, 296.8f); break;
+    case CRYO_FLUID_LOX: put(1141.f, 4.47f, 1.96e-4f, 6.9e-6f, 0.152f, 0.0084f, 1699.f, 972.f, 13.2e-3f, 213.1e3f, 90.19f, 101325.f, 259.8f); break;
+    case CRYO_FLUID_LCH4: put(422.4f, 1.816f, 1.17e-4f, 4.4e-6f, 0.184f, 0.0119f, 3481.f, 2218.f, 13.4e-3f, 510.8e3f, 111.67f, 101325.f, 518.3f); break;
+    case CRYO_FLUID_H2O: put(998.2f, 0.598f, 1.0e-3f, 1.23e-5f, 0.598f, 0.0248f, 4182.f, 2080.f, 0.0728f, 2.257e6f, 373.15f, 101325.f, 461.5f); break;
+    case CRYO_FLUID_CUSTOM: put(1000.f, 1.f, 1e-3f, 1e-5f, 0.6f, 0.025f, 4180.f, 2000.f, 0.072f, 2.26e6f, 373.15f, 101325.f, 461.5f); break;
+    default: throw std::invalid_argument("unknown fluid preset");
+  }
+}
+
+// Field access: (array, component offset in floats, components, element stride in bytes).
+struct FieldLoc {
+  void* base;
+  int offset;   // in 4-byte words inside the element
+  int comps;    // 1 or 3
+  int stride;   // element size in bytes
+  int kind;     // 0 float, 1 u8 phase, 2 u8 flags, 3 u32
+};
+
+FieldLoc locate(cryo_ctx* c, int field) {
+  const Persist& s = c->set[c->cur];
+  switch (field) {
+    case CRYO_F_X: return {s.xp, 0, 3, 16, 0};
+    case CRYO_F_V: return {s.vT, 0, 3, 16, 0};
+    case CRYO_F_VT: return {s.vt, 0, 3, 16, 0};
+    case CRYO_F_NRM: return {s.nrm, 0, 3, 16, 0};
+    case CRYO_F_M: return {s.mrps, 0, 1, 16, 0};
+    case CRYO_F_M0: return {s.vt, 3, 1, 16, 0};
+    case CRYO_F_RHO: return {s.mrps, 1, 1, 16, 0};
+    case CRYO_F_T: return {s.vT, 3, 1, 16, 0};
+    case CRYO_F_PHASE: return {s.xp, 3, 1, 16, 1};
+    case CRYO_F_FLAGS: return {s.xp, 3, 1, 16, 2};
+    case CRYO_F_ID: return {s.id, 0, 1, 4, 3};
+    case CRYO_F_A: return {c->a4, 0, 3, 16, 0};
+    case CRYO_F_AB: return {c->ab4, 0, 3, 16, 0};
+    case CRYO_F_FW: return {c->fw, 0, 3, 16, 0};
+    case CRYO_F_MW: return {c->mw, 0, 3, 16, 0};
+    case CRYO_F_NS: return {c->ns4, 0, 3, 16, 0};
+    case CRYO_F_VW: return {c->vwp, 0, 3, 16, 0};
+    case CRYO_F_P: return {s.mrps, 2, 1, 16, 0};
+    case CRYO_F_DRHO: return {c->ab4, 3, 1, 16, 0};
+    case CRYO_F_DTDT: return {c->a4, 3, 1, 16, 0};
+    case CRYO_F_SIGMA: return {s.mrps, 3, 1, 16, 0};
+    case CRYO_F_KAPPA: return {c->ns4, 3, 1, 16, 0};
+    case CRYO_F_NU_T: return {c->nu_t, 0, 1, 4, 0};
+    case CRYO_F_ALPHA: return {s.nrm, 3, 1, 16, 0};
+    case CRYO_F_WALL_W: return {c->wall_w, 0, 1, 4, 0};
+    case CRYO_F_HEAT_W: return {c->heat_w, 0, 1, 4, 0};
+    case CRYO_F_OUT_M: return {c->pc, 0, 1, 16, 0};
+    case CRYO_F_OUT_H: return {c->pc, 1, 1, 16, 0};
+    case CRYO_F_W_NORM: return {c->pc, 2, 1, 16, 0};
+    case CRYO_F_RMIN: return {c->rmin, 0, 1, 4, 0};
+    case CRYO_F_P_WV: return {c->vwp, 3, 1, 16, 0};
+    default: throw std::invalid_argument("unknown field");
+  }
+}
+
+size_t field_bytes(const FieldLoc& f, int n) {
+  if (f.kind == 1 || f.kind == 2) return (size_t)n;
+  return (size_t)n * 4 * f.comps;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int cryo_abi_version(void) { return CRYO_ABI_VERSION; }
+
+// SolverConfig defaults (sph_solver.hpp:20-91)
+void cryo_config_default(cryo_config_t* c) {
+  std::memset(c, 0, sizeof(*c));
+  c->dx = 0.005f; c->h_factor = 1.3f; c->kernel = CRYO_KERNEL_WENDLAND_C2;
+  c->density_mode = CRYO_DENSITY_SUMMATION; c->normalize_initial_masses = 1;
+  c->gravity[0] = 0; c->gravity[1] = 0; c->gravity[2] = -9.81f;
+  c->velocity_scale = 0; c->sound_speed = 0; c->tait_gamma = 7; c->background_pressure = -1;
+  c->vapor_stiffness = -1; c->clamp_negative_pressure = 0;
+  c->transport_velocity = 1; c->transport_background_factor = 2.0f; c->transport_stress = 0;
+  c->transport_interface_only = 1; c->particle_shifting = 0; c->shifting_strength = 0.25f;
+  c->artificial_viscosity = 0.02f; c->artificial_viscosity_vapor = 0.2f; c->delta_sph = 0.1f;
+  c->no_slip = 1; c->sps_turbulence = 0; c->smagorinsky_cs = 0.12f;
+  c->surface_tension = CRYO_ST_CSF; c->contact_angle_deg = 90; c->contact_angle_wall_weight = 0.01f;
+  c->wall_colour = 1; c->wetting_model = CRYO_WET_NORMAL_ROTATION; c->csf_smooth_normals = 0;
+  c->csf_balanced = 0; c->akinci_gamma = -1; c->akinci_beta = -1;
+  c->thermal = 1; c->phase_change = 1; c->wall_thermal_bc = CRYO_WALL_ADIABATIC; c->heater_power = 0;
+  c->conductivity_scale = 1; c->lee_evaporation = 10; c->lee_condensation = 10;
+  c->thermo_mode = CRYO_THERMO_VENTED; c->vent_relaxation = 0.02f; c->merge_ratio = 0.3f; c->split_ratio = 2.0f;
+  c->max_transfer_fraction = 0.25f; c->phase_change_density_limit = 0.01f; c->vapor_mass_rebalance = 1.0f;
+  c->cfl = 0.25f; c->viscous_number = 0.125f; c->force_number = 0.25f; c->capillary_number = 0.25f;
+  c->thermal_number = 0.1f; c->dt_max = 1e-2f; c->dt_min = 1e-9f; c->fixed_dt = 0;
+}
+
+int cryo_fluid_preset(int which, cryo_fluid_t* out) {
+  return guard(nullptr, [&] { fluid_from(which, out); });
+}
+
+// FluidProperties::saturation_temperature / _pressure (fluid_properties.cpp:7-14)
+float cryo_saturation_temperature(const cryo_fluid_t* f, float p) {
+  const double inv_T = 1.0 / f->T_sat - ((double)f->R_gas / f->h_fg) * std::log((double)p / f->p_sat);
+  return (float)(1.0 / inv_T);
+}
+float cryo_saturation_pressure(const cryo_fluid_t* f, float T) {
+  return (float)(f->p_sat * std::exp((double)f->h_fg / f->R_gas * (1.0 / f->T_sat - 1.0 / (double)T)));
+}
+
+int cryo_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+int cryo_device_name(int device, char* buf, int buflen) {
+  return guard(nullptr, [&] {
+    cudaDeviceProp prop{};
+    CK(cudaGetDeviceProperties(&prop, device));
+    const std::string s = std::string(prop.name) + " (sm_" + std::to_string(prop.major) + std::to_string(prop.minor) + ")";
+    if (buf && buflen > 0) {
+      std::strncpy(buf, s.c_str(), (size_t)buflen - 1);
+      buf[buflen - 1] = 0;
+    }
+  });
+}
+
+// Solver::Solver (sph_solver.cu:273-279)
+int cryo_create(const cryo_config_t* cfg, const cryo_fluid_t* fluid, int device, cryo_ctx** out) {
+  *out = nullptr;
+  cryo_ctx* c = nullptr;
+  const int rc = guard(nullptr, [&] {
+    if (!(cfg->dx > 0)) throw std::invalid_argument("SolverConfig.dx must be > 0");
+    if (cfg->contact_angle_deg < 0 || cfg->contact_angle_deg > 180)
+      throw std::invalid_argument("contact angle must be within [0, 180] degrees");
+    c = new cryo_ctx;
+    try {
+      c->cfg = *cfg;
+      c->fluid = *fluid;
+      c->device = device;
+      CK(cudaSetDevice(device));
+      int sms = 0;
+      if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess && sms > 0)
+        c->sm_count = sms;
+      CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault));
+      CK(cudaMalloc(&c->dyn, sizeof(DynState)));
+      CK(cudaMallocHost(&c->hdyn, sizeof(DynState)));
+      std::memset(c->hdyn, 0, sizeof(DynState));
+      c->hdyn->p_ullage = fluid->p_sat;
+      c->hdyn->spacing_ratio = 1.0f;
+      c->hdyn->T_sat = fluid->T_sat;
+      set3(c->hdyn->cfg_gravity, cfg->gravity);
+      set3(c->hdyn->gravity, cfg->gravity);
+      c->push();
+    } catch (...) {
+      delete c;
+      c = nullptr;
+      throw;
+    }
+  });
+  *out = c;
+  return rc;
+}
+
+void cryo_destroy(cryo_ctx* ctx) { delete ctx; }
+
+const char* cryo_last_error(const cryo_ctx* ctx) { return ctx ? ctx->err.c_str() : g_create_error.c_str(); }
+
+uintptr_t cryo_stream(const cryo_ctx* ctx) { return reinterpret_cast<uintptr_t>(ctx->stream); }
+
+// Solver::set_particles (sph_solver.cu:407-428) + ParticleSystem::upload
+// (particle_system.cpp:73-93) + SpatialHash::configure.
+int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float* lo, const float* hi) {
+  return guard(c, [&] {
+    const int n = p->n;
+    if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
+    bool vap = false;
+    for (int i = 0; i < n; ++i) vap |= p->phase[i] == CRYO_VAPOR;
+    if (vap && c->cfg.surface_tension == CRYO_ST_AKINCI)
+      throw std::invalid_argument(
+          "Solver: the Akinci surface-tension model is a free-surface (liquid-only) model; use CSF when vapour "
+          "particles are present (FillSpec.include_vapor = false for Akinci runs)");
+    c->sync();
+    c->has_vapor = vap;
+    const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+    float cl = ex;
+    if (cl < ey) cl = ey;
+    if (cl < ez) cl = ez;
+    c->char_length = cl;
+    c->init_params();
+    {
+      const long long cap2 = (long long)((double)n * 2.0);
+      const long long cap = std::max(cap2, (long long)n + 1024);
+      if (cap > (long long)std::numeric_limits<int>::max() / 2) throw std::out_of_range("particle count too large");
+      if (cap > c->capacity) {
+        c->arena.release();
+        c->capacity = 0;
+        c->allocate((int)cap);
+      }
+    }
+    c->configure_grid(lo, hi);
+    c->invalidate_graphs();
+    // pack the host arrays into the device layout
+    std::vector<float4> xp(n), vT(n), vt(n), nrm(n), mrps(n);
+    std::vector<uint32_t> id(n);
+    uint32_t next_id = 0;
+    for (int i = 0; i < n; ++i) {
+      const float* x = p->x + 3 * i;
+      const float v0 = p->v ? p->v[3 * i] : 0.f, v1 = p->v ? p->v[3 * i + 1] : 0.f, v2 = p->v ? p->v[3 * i + 2] : 0.f;
+      xp[i] = make_float4(x[0], x[1], x[2], pack_pf(p->phase[i], p->flags ? p->flags[i] : 0));
+      vT[i] = make_float4(v0, v1, v2, p->T[i]);
+      vt[i] = make_float4(v0, v1, v2, p->m[i]);
+      nrm[i] = p->nrm ? make_float4(p->nrm[3 * i], p->nrm[3 * i + 1], p->nrm[3 * i + 2], 0.f)
+                      : make_float4(0.f, 0.f, 0.f, 0.f);
+      mrps[i] = make_float4(p->m[i], p->rho[i], 0.f, 0.f);
+      id[i] = p->id ? p->id[i] : (uint32_t)i;
+      next_id = std::max(next_id, id[i] + 1);
+    }
+    c->cur = 0;
+    const Persist& s = c->set[0];
+    CK(cudaMemcpyAsync(s.xp, xp.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s.vT, vT.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s.vt, vt.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s.nrm, nrm.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s.mrps, mrps.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(s.id, id.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
+    // scratch fields start clean (particle_system.cpp:85-88)
+    const size_t cap = (size_t)c->capacity;
+    for (float4* a : {c->a4, c->ab4, c->fw, c->mw, c->vwp, c->ns4, c->pc})
+      CK(cudaMemsetAsync(a, 0, cap * 16, c->stream));
+    for (float* a : {c->wall_w, c->heat_w, c->nu_t}) CK(cudaMemsetAsync(a, 0, cap * 4, c->stream));
+    // scalar block: keep the frame state, reset the rest (sph_solver.cu:419-427)
+    c->pull();
+    DynState& d = *c->hdyn;
+    d.n = n;
+    d.n_alive = n;
+    d.capacity = c->capacity;
+    d.next_id = next_id;
+    d.time = 0;
+    d.last_dt = 0;
+    d.step = 0;
+    d.dt = 0;
+    set3(d.cfg_gravity, c->cfg.gravity);
+    d.gravity[0] = c->cfg.gravity[0] - d.frame_acc[0];
+    d.gravity[1] = c->cfg.gravity[1] - d.frame_acc[1];
+    d.gravity[2] = c->cfg.gravity[2] - d.frame_acc[2];
+    d.T_sat = c->fluid.T_sat;
+    d.heat_inv_norm = 0;
+    d.p_ullage = c->fluid.p_sat;
+    d.fluid_volume0 = 0;
+    d.heat_input = 0;
+    d.v_max = d.a_max = d.Tv_max = d.nu_t_max = 0;
+    d.spacing_ratio = 1.0f;
+    d.evaporated = d.condensed = d.vented = d.vented_h = 0;
+    d.merges = d.splits = 0;
+    d.status = 0;
+    d.split_requested = 0;
+    d.damp_after_step = 0;
+    d.damping = 1.0f;
+    d.thermal_on = c->P.thermal;
+    d.phase_change_on = c->cfg.phase_change ? 1 : 0;
+    c->push();
+    c->has_particles = true;
+    c->initialized = false;
+  });
+}
+
+int cryo_step(cryo_ctx* c) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    c->launch_step();
+  });
+}
+
+int cryo_run_steps(cryo_ctx* c, long long n) {
+  return guard(c, [&] {
+    c->run_steps(n);
+    c->sync();
+  });
+}
+
+int cryo_run_until(cryo_ctx* c, double t_end) {
+  return guard(c, [&] {
+    c->run_until(t_end);
+    c->sync();
+  });
+}
+
+// Solver::relax (sph_solver.cu:707-736)
+int cryo_relax(cryo_ctx* c, double duration, float damping) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    c->pull();
+    const int thermal = c->hdyn->thermal_on;
+    const int pc_on = c->hdyn->phase_change_on;
+    c->hdyn->thermal_on = 0;
+    c->hdyn->phase_change_on = 0;
+    c->hdyn->damp_after_step = 1;
+    c->hdyn->damping = damping;
+    c->push();
+    const double t_end = c->hdyn->time + duration;
+    auto restore = [&] {
+      c->pull();
+      c->hdyn->thermal_on = thermal;
+      c->hdyn->phase_change_on = pc_on;
+      c->hdyn->damp_after_step = 0;
+      c->push();
+    };
+    try {
+      c->run_until(t_end);
+    } catch (...) {
+      restore();
+      throw;
+    }
+    restore();
+    const int G = c->grid_blocks();
+    k_scale_velocities<<<G, kBlock, 0, c->stream>>>(c->view(c->cur), 0.0f, 0);
+    LAUNCH_CHECK();
+    c->pull();
+    DynState& d = *c->hdyn;
+    d.time = 0;
+    d.step = 0;
+    d.last_dt = 0;
+    d.heat_input = d.evaporated = d.condensed = d.vented = d.vented_h = 0;
+    d.splits = d.merges = 0;
+    c->push();
+    c->evaluate_rates(c->cur, true);
+    k_saturation<<<G, kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), 0);
+    LAUNCH_CHECK();
+    c->sync();
+  });
+}
+
+int cryo_next_dt(cryo_ctx* c, double* dt) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    c->pull();
+    *dt = compute_dt(c->P, *c->hdyn);
+  });
+}
+
+int cryo_synchronize(cryo_ctx* c) {
+  return guard(c, [&] { c->pull(); });
+}
+
+int cryo_time(cryo_ctx* c, double* t, long long* step, double* last_dt) {
+  return guard(c, [&] {
+    c->pull();
+    *t = c->hdyn->time;
+    *step = c->hdyn->step;
+    *last_dt = c->hdyn->last_dt;
+  });
+}
+
+int cryo_num_particles(cryo_ctx* c, int* n) {
+  return guard(c, [&] {
+    c->pull();
+    *n = c->has_particles ? c->hdyn->n : 0;
+  });
+}
+
+int cryo_capacity(cryo_ctx* c, int* cap) {
+  return guard(c, [&] { *cap = c->capacity; });
+}
+
+// Solver::diagnostics (sph_solver.cu:609-653)
+int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    const int G = c->grid_blocks();
+    k_diagnostics<<<G, kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), c->diag_out);
+    LAUNCH_CHECK();
+    double v[25];
+    CK(cudaMemcpyAsync(v, c->diag_out, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+    c->pull();
+    const DynState& d = *c->hdyn;
+    std::memset(o, 0, sizeof(*o));
+    o->time = d.time;
+    o->step = d.step;
+    o->dt = d.last_dt;
+    o->n_total = d.n;
+    o->n_liquid = (int)v[0];
+    o->n_vapor = (int)v[1];
+    o->n_wall = (int)v[2];
+    o->mass_liquid = v[3];
+    o->mass_vapor = v[4];
+    o->mass_total = o->mass_liquid + o->mass_vapor;
+    o->kinetic_energy = v[5] + v[6];
+    o->enthalpy = v[7] + v[8];
+    o->heat_input = d.heat_input;
+    o->evaporated_mass = d.evaporated;
+    o->condensed_mass = d.condensed;
+    o->vented_mass = d.vented;
+    o->vented_enthalpy = d.vented_h;
+    o->T_sat = d.T_sat;
+    o->p_ullage = d.p_ullage;
+    o->max_speed = (double)(float)v[23];
+    if (o->mass_liquid > 0) {
+      o->T_liquid_mean = v[9] / o->mass_liquid;
+      o->T_liquid_max = (double)(float)v[24];
+      for (int k = 0; k < 3; ++k) {
+        o->liquid_com[k] = (float)(v[11 + k] / o->mass_liquid);
+        o->liquid_momentum[k] = (float)v[14 + k];
+      }
+    }
+    if (o->mass_vapor > 0) o->T_vapor_mean = v[10] / o->mass_vapor;
+    o->splits = d.splits;
+    o->merges = d.merges;
+    for (int k = 0; k < 3; ++k) {
+      o->slosh_force[k] = -(float)v[17 + k];
+      o->slosh_moment[k] = -(float)v[20 + k];
+      o->frame_acceleration[k] = d.frame_acc[k];
+      o->frame_angular_velocity[k] = d.omega[k];
+    }
+  });
+}
+
+int cryo_get_field(cryo_ctx* c, int field, void* out, size_t cap) {
+  return guard(c, [&] {
+    c->pull();
+    const int n = c->has_particles ? c->hdyn->n : 0;
+    const FieldLoc f = locate(c, field);
+    if (cap < field_bytes(f, n)) throw std::out_of_range("cryo_get_field: buffer too small");
+    if (n == 0) return;
+    std::vector<char> raw((size_t)n * f.stride);
+    CK(cudaMemcpyAsync(raw.data(), f.base, raw.size(), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    for (int i = 0; i < n; ++i) {
+      const char* e = raw.data() + (size_t)i * f.stride;
+      if (f.kind == 0) {
+        std::memcpy(static_cast<float*>(out) + (size_t)i * f.comps, e + 4 * f.offset, 4 * f.comps);
+      } else if (f.kind == 3) {
+        std::memcpy(static_cast<uint32_t*>(out) + i, e, 4);
+      } else {
+        int bits;
+        std::memcpy(&bits, e + 4 * f.offset, 4);
+        static_cast<uint8_t*>(out)[i] = (uint8_t)(f.kind == 1 ? (bits & 0xff) : ((bits >> 8) & 0xff));
+      }
+    }
+  });
+}
+
+int cryo_set_field(cryo_ctx* c, int field, const void* in, size_t bytes) {
+  return guard(c, [&] {
+    c->pull();
+    const int n = c->has_particles ? c->hdyn->n : 0;
+    const FieldLoc f = locate(c, field);
+    if (bytes != field_bytes(f, n)) throw std::invalid_argument("cryo_set_field: size does not match the particle count");
+    if (n == 0) return;
+    std::vector<char> raw((size_t)n * f.stride);
+    CK(cudaMemcpyAsync(raw.data(), f.base, raw.size(), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    for (int i = 0; i < n; ++i) {
+      char* e = raw.data() + (size_t)i * f.stride;
+      if (f.kind == 0) {
+        std::memcpy(e + 4 * f.offset, static_cast<const float*>(in) + (size_t)i * f.comps, 4 * f.comps);
+      } else if (f.kind == 3) {
+        std::memcpy(e, static_cast<const uint32_t*>(in) + i, 4);
+      } else {
+        int bits;
+        std::memcpy(&bits, e + 4 * f.offset, 4);
+        const int v = static_cast<const uint8_t*>(in)[i];
+        bits = f.kind == 1 ? ((bits & ~0xff) | v) : ((bits & ~0xff00) | (v << 8));
+        std::memcpy(e + 4 * f.offset, &bits, 4);
+      }
+    }
+    CK(cudaMemcpyAsync(f.base, raw.data(), raw.size(), cudaMemcpyHostToDevice, c->stream));
+    c->sync();
+  });
+}
+
+// Solver::particles (particle_system.cpp:95-101)
+int cryo_download(cryo_ctx* c, cryo_host_particles_out_t* o) {
+  return guard(c, [&] {
+    c->pull();
+    const int n = c->has_particles ? c->hdyn->n : 0;
+    if (o->n < n) {
+      o->n = n;
+      throw std::out_of_range("cryo_download: arrays too small");
+    }
+    o->n = n;
+    if (n == 0) return;
+    const Persist& s = c->set[c->cur];
+    std::vector<float4> xp(n), vT(n), nrm(n), mrps(n);
+    CK(cudaMemcpyAsync(xp.data(), s.xp, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(vT.data(), s.vT, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(nrm.data(), s.nrm, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(mrps.data(), s.mrps, n * 16, cudaMemcpyDeviceToHost, c->stream));
+    if (o->id) CK(cudaMemcpyAsync(o->id, s.id, n * 4, cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    for (int i = 0; i < n; ++i) {
+      if (o->x) { o->x[3 * i] = xp[i].x; o->x[3 * i + 1] = xp[i].y; o->x[3 * i + 2] = xp[i].z; }
+      if (o->v) { o->v[3 * i] = vT[i].x; o->v[3 * i + 1] = vT[i].y; o->v[3 * i + 2] = vT[i].z; }
+      if (o->nrm) { o->nrm[3 * i] = nrm[i].x; o->nrm[3 * i + 1] = nrm[i].y; o->nrm[3 * i + 2] = nrm[i].z; }
+      if (o->m) o->m[i] = mrps[i].x;
+      if (o->rho) o->rho[i] = mrps[i].y;
+      if (o->T) o->T[i] = vT[i].w;
+      int bits;
+      std::memcpy(&bits, &xp[i].w, 4);
+      if (o->phase) o->phase[i] = (uint8_t)(bits & 0xff);
+      if (o->flags) o->flags[i] = (uint8_t)((bits >> 8) & 0xff);
+    }
+  });
+}
+
+// Solver::set_gravity (sph_solver.cu:655-658)
+int cryo_set_gravity(cryo_ctx* c, const float* g) {
+  return guard(c, [&] {
+    set3(c->cfg.gravity, g);
+    c->pull();
+    set3(c->hdyn->cfg_gravity, g);
+    for (int k = 0; k < 3; ++k) c->hdyn->gravity[k] = g[k] - c->hdyn->frame_acc[k];
+    c->push();
+  });
+}
+
+namespace {
+void host_apply_frame(DynState& d, const float* a, const float* w, const float* wd, const float* o) {
+  set3(d.frame_acc, a);
+  for (int k = 0; k < 3; ++k) d.gravity[k] = d.cfg_gravity[k] - a[k];
+  set3(d.omega, w);
+  set3(d.omega_dot, wd);
+  set3(d.frame_origin, o);
+  const float n1 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
+  const float n2 = wd[0] * wd[0] + wd[1] * wd[1] + wd[2] * wd[2];
+  d.frame_rot = (n1 > 0.0f || n2 > 0.0f) ? 1 : 0;
+}
+
+// ManeuverProfile::evaluate (sph_solver.cu:244-268), host
+void host_maneuver(int n, const double* t, const float* acc, const float* om, double tq, float* a, float* w,
+                   float* wd) {
+  wd[0] = wd[1] = wd[2] = 0;
+  if (tq <= t[0] || n == 1) {
+    set3(a, acc);
+    if (om) set3(w, om); else w[0] = w[1] = w[2] = 0;
+    return;
+  }
+  if (tq >= t[n - 1]) {
+    set3(a, acc + 3 * (n - 1));
+    if (om) set3(w, om + 3 * (n - 1)); else w[0] = w[1] = w[2] = 0;
+    return;
+  }
+  const int k = (int)(std::upper_bound(t, t + n, tq) - t) - 1;
+  const double dt = t[k + 1] - t[k];
+  const float f = (float)((tq - t[k]) / dt);
+  for (int q = 0; q < 3; ++q) a[q] = acc[3 * k + q] * (1.0f - f) + acc[3 * (k + 1) + q] * f;
+  if (om) {
+    for (int q = 0; q < 3; ++q) {
+      w[q] = om[3 * k + q] * (1.0f - f) + om[3 * (k + 1) + q] * f;
+      wd[q] = (om[3 * (k + 1) + q] - om[3 * k + q]) / (float)dt;
+    }
+  } else {
+    w[0] = w[1] = w[2] = 0;
+  }
+}
+}  // namespace
+
+// Solver::set_frame_motion (sph_solver.cu:669-672)
+int cryo_set_frame_motion(cryo_ctx* c, const float* a, const float* w, const float* wd, const float* o) {
+  return guard(c, [&] {
+    c->pull();
+    c->hdyn->has_maneuver = 0;
+    host_apply_frame(*c->hdyn, a, w, wd, o);
+    c->push();
+  });
+}
+
+// ManeuverProfile::validate + Solver::set_maneuver (sph_solver.cu:234-242,674-681)
+int cryo_set_maneuver(cryo_ctx* c, int n, const double* t, const float* acc, const float* omega,
+                      const float* origin) {
+  return guard(c, [&] {
+    if (n <= 0) throw std::invalid_argument("ManeuverProfile: empty time table");
+    for (int k = 1; k < n; ++k)
+      if (!(t[k] > t[k - 1])) throw std::invalid_argument("ManeuverProfile: time must be strictly increasing");
+    c->sync();
+    if (n > c->man_cap) {
+      if (c->man_t) CK(cudaFree(c->man_t));
+      if (c->man_acc) CK(cudaFree(c->man_acc));
+      if (c->man_omega) CK(cudaFree(c->man_omega));
+      CK(cudaMalloc(&c->man_t, n * sizeof(double)));
+      CK(cudaMalloc(&c->man_acc, n * 3 * sizeof(float)));
+      CK(cudaMalloc(&c->man_omega, n * 3 * sizeof(float)));
+      c->man_cap = n;
+      c->invalidate_graphs();
+    }
+    CK(cudaMemcpyAsync(c->man_t, t, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->man_acc, acc, n * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    if (omega) CK(cudaMemcpyAsync(c->man_omega, omega, n * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    c->pull();
+    DynState& d = *c->hdyn;
+    d.has_maneuver = 1;
+    d.man_n = n;
+    d.man_rot = omega ? 1 : 0;
+    const float zero[3] = {0, 0, 0};
+    set3(d.man_origin, origin ? origin : zero);
+    float a[3], w[3], wd[3];
+    host_maneuver(n, t, acc, omega, d.time, a, w, wd);
+    host_apply_frame(d, a, w, wd, d.man_origin);
+    c->push();
+  });
+}
+
+int cryo_maneuver_evaluate(int n, const double* t, const float* acc, const float* omega, double tq, float* a,
+                           float* w, float* wd) {
+  return guard(nullptr, [&] {
+    if (n <= 0) throw std::invalid_argument("ManeuverProfile: empty time table");
+    host_maneuver(n, t, acc, omega, tq, a, w, wd);
+  });
+}
+
+// Solver::clear_frame_motion (sph_solver.cu:683-686)
+int cryo_clear_frame_motion(cryo_ctx* c) {
+  return guard(c, [&] {
+    c->pull();
+    c->hdyn->has_maneuver = 0;
+    const float z[3] = {0, 0, 0};
+    host_apply_frame(*c->hdyn, z, z, z, z);
+    c->push();
+  });
+}
+
+// Solver::set_heater_power (sph_solver.cu:688-691)
+int cryo_set_heater_power(cryo_ctx* c, float watts) {
+  return guard(c, [&] {
+    c->sync();
+    c->cfg.heater_power = watts;
+    c->P.heat_power = watts;
+    c->invalidate_graphs();
+  });
+}
+
+// Solver::set_contact_angle (sph_solver.cu:693-699)
+int cryo_set_contact_angle(cryo_ctx* c, float degrees) {
+  return guard(c, [&] {
+    if (degrees < 0 || degrees > 180) throw std::invalid_argument("contact angle must be within [0, 180] degrees");
+    c->sync();
+    c->cfg.contact_angle_deg = degrees;
+    const float theta = degrees * kPi / 180.0f;
+    c->P.cos_theta = std::cos(theta);
+    c->P.sin_theta = std::sin(theta);
+    c->invalidate_graphs();
+  });
+}
+
+// Solver::damp_velocities (sph_solver.cu:701-705)
+int cryo_damp_velocities(cryo_ctx* c, float factor) {
+  return guard(c, [&] {
+    if (!c->has_particles) return;
+    k_scale_velocities<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->view(c->cur), factor, 1);
+    LAUNCH_CHECK();
+    c->sync();
+  });
+}
+
+// Solver::probe_pressure (sph_solver.cu:738-748)
+int cryo_probe_pressure(cryo_ctx* c, const float* pts, int np, float* out) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    if (np <= 0) return;
+    float* d = nullptr;
+    CK(cudaMallocAsync(&d, (size_t)np * 4 * sizeof(float), c->stream));
+    CK(cudaMemcpyAsync(d, pts, (size_t)np * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    const int blocks = std::max(1, std::min((np + 127) / 128, c->sm_count * 8));
+    k_probe<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(out, d + 3 * (size_t)np, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaFreeAsync(d, c->stream));
+    c->sync();
+  });
+}
+
+int cryo_sound_speed(cryo_ctx* c, float* c0) {
+  return guard(c, [&] { *c0 = c->P.c0; });
+}
+int cryo_smoothing_length(cryo_ctx* c, float* h) {
+  return guard(c, [&] { *h = c->P.h; });
+}
+
+int cryo_set_pass_dt(cryo_ctx* c, float dt) {
+  return guard(c, [&] {
+    c->pass_dt = dt;
+    c->pull();
+    c->hdyn->dt = dt;
+    c->push();
+  });
+}
+
+// Operator-level calls: one reference free function on the current state.
+int cryo_pass(cryo_ctx* c, int pass) {
+  return guard(c, [&] {
+    if (!c->has_particles) throw std::runtime_error("Solver: no particles loaded");
+    const int G = c->grid_blocks();
+    const View V = c->view(c->cur);
+    const Reduce R = c->reduce();
+    cudaStream_t st = c->stream;
+    const Params& P = c->P;
+    switch (pass) {
+      case CRYO_PASS_KICK_DRIFT:
+        k_kick_drift<<<G, kBlock, 0, st>>>(P, V, P.density_mode == CRYO_DENSITY_CONTINUITY, P.tvf);
+        break;
+      case CRYO_PASS_GRID_BUILD:
+        c->grid_build(c->cur);
+        c->cur = 1 - c->cur;
+        break;
+      case CRYO_PASS_DENSITY: k_density<<<G, kBlock, 0, st>>>(P, V, 0); break;
+      case CRYO_PASS_NORMALIZE_MASSES: k_normalize_masses<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_EOS: k_eos<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_WALL_BOUNDARY: k_wall<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_INTERFACE: k_interface<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
+      case CRYO_PASS_TRANSPORT: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_TRANSPORT); break;
+      case CRYO_PASS_SPS: k_sps<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_MOMENTUM: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_MOMENTUM); break;
+      case CRYO_PASS_SMOOTH_NORMALS: k_smooth_normals<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_CSF: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_CSF); break;
+      case CRYO_PASS_AKINCI: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_AKINCI); break;
+      case CRYO_PASS_DENSITY_RATE: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_DRHO); break;
+      case CRYO_PASS_THERMAL:
+        k_heat_norm<<<G, kBlock, 0, st>>>(P, V, R);
+        LAUNCH_CHECK();
+        k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
+        break;
+      case CRYO_PASS_MAXIMA:
+        k_begin_step<<<1, 1, 0, st>>>(P, V, BEGIN_RATES);
+        LAUNCH_CHECK();
+        k_maxima<<<G, kBlock, 0, st>>>(P, V);
+        break;
+      case CRYO_PASS_KICK: k_kick<<<G, kBlock, 0, st>>>(P, V, 0); break;
+      case CRYO_PASS_SHIFTING:
+        k_shift_compute<<<G, kBlock, 0, st>>>(P, V);
+        LAUNCH_CHECK();
+        k_shift_apply<<<G, kBlock, 0, st>>>(P, V);
+        break;
+      case CRYO_PASS_PC_SOURCES: k_pc_sources<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_PC_NORMALIZE: k_pc_normalize<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
+      case CRYO_PASS_PC_APPLY: k_pc_apply<<<G, kBlock, 0, st>>>(P, V, 0); break;
+      case CRYO_PASS_REBALANCE:
+        k_rebalance1<<<G, kBlock, 0, st>>>(P, V, 0);
+        LAUNCH_CHECK();
+        k_rebalance2_mark<<<G, kBlock, 0, st>>>(P, V, R, c->split_flag, 1, 0);
+        break;
+      case CRYO_PASS_SPLIT:
+        k_rebalance2_mark<<<G, kBlock, 0, st>>>(P, V, R, c->split_flag, 0, 0);
+        LAUNCH_CHECK();
+        k_split<<<G, kBlock, 0, st>>>(P, V, R, c->split_flag, 0);
+        break;
+      case CRYO_PASS_VENTING: k_venting<<<G, kBlock, 0, st>>>(P, V, R, c->cfg.vent_relaxation, 0); break;
+      case CRYO_PASS_SATURATION: k_saturation<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
+      default: throw std::invalid_argument("unknown pass");
+    }
+    LAUNCH_CHECK();
+    c->sync();
+  });
+}
+
+int cryo_grid_info(cryo_ctx* c, int* num_cells, int* nx, int* ny, int* nz, float* origin, float* cell) {
+  return guard(c, [&] {
+    *num_cells = c->P.num_cells;
+    *nx = c->P.nx; *ny = c->P.ny; *nz = c->P.nz;
+    origin[0] = c->P.ox; origin[1] = c->P.oy; origin[2] = c->P.oz;
+    *cell = c->P.cell;
+  });
+}
+
+// Tables of the last grid build: the sorted keys and permutation, and the
+// reference's cell_start / cell_end (-1 for empty cells, spatial_hash.cu:79-91)
+// derived from the dense cell table.
+int cryo_grid_tables(cryo_ctx* c, uint32_t* keys, uint32_t* perm, int32_t* cs, int32_t* ce) {
+  return guard(c, [&] {
+    c->pull();
+    const int nc = c->P.num_cells;
+    if (keys || perm) {
+      if (!c->sorted_keys) throw std::runtime_error("no grid build yet");
+      if (keys) CK(cudaMemcpyAsync(keys, c->sorted_keys, (size_t)c->hdyn->n_alive * 4, cudaMemcpyDeviceToHost, c->stream));
+      if (perm) CK(cudaMemcpyAsync(perm, c->sorted_perm, (size_t)c->hdyn->n_alive * 4, cudaMemcpyDeviceToHost, c->stream));
+    }
+    if (cs || ce) {
+      std::vector<int> b(nc + 1);
+      CK(cudaMemcpyAsync(b.data(), c->cell_begin, (size_t)(nc + 1) * 4, cudaMemcpyDeviceToHost, c->stream));
+      c->sync();
+      for (int k = 0; k < nc; ++k) {
+        const bool nonempty = b[k + 1] > b[k];
+        if (cs) cs[k] = nonempty ? b[k] : -1;
+        if (ce) ce[k] = nonempty ? b[k + 1] : -1;
+      }
+    }
+    c->sync();
+  });
+}
+
+int cryo_neighbor_lists(cryo_ctx* c, int32_t* counts, int32_t* list, long long cap, long long* total) {
+  return guard(c, [&] {
+    c->pull();
+    const int n = c->hdyn->n;
+    int* dcount = nullptr;
+    CK(cudaMallocAsync(&dcount, (size_t)std::max(n, 1) * sizeof(int), c->stream));
+    k_nbr_count<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), dcount);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(counts, dcount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    std::vector<long long> off(n);
+    long long t = 0;
+    for (int i = 0; i < n; ++i) {
+      off[i] = t;
+      t += counts[i];
+    }
+    *total = t;
+    if (list && cap >= t && t > 0) {
+      long long* doff = nullptr;
+      int* dlist = nullptr;
+      CK(cudaMallocAsync(&doff, (size_t)n * sizeof(long long), c->stream));
+      CK(cudaMallocAsync(&dlist, (size_t)t * sizeof(int), c->stream));
+      CK(cudaMemcpyAsync(doff, off.data(), (size_t)n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+      k_nbr_fill<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), doff, dlist);
+      LAUNCH_CHECK();
+      CK(cudaMemcpyAsync(list, dlist, (size_t)t * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaFreeAsync(doff, c->stream));
+      CK(cudaFreeAsync(dlist, c->stream));
+    }
+    CK(cudaFreeAsync(dcount, c->stream));
+    c->sync();
+  });
+}
+
+int cryo_device_status(cryo_ctx* c, unsigned* status) {
+  return guard(c, [&] {
+    c->pull();
+    *status = c->hdyn->status;
+    c->hdyn->status = 0;
+    c->push();
+  });
+}
+
+// ------------------------------------------------------------- checkpoints
+namespace {
+struct Blob {
+  uint32_t magic, version;
+  int n, capacity, num_cells;
+  int initialized, has_vapor;
+  DynState dyn;
+};
+const int kCkptArrays16 = 12;  // xp vT vt nrm mrps | a4 ab4 fw mw vwp ns4 pc
+const int kCkptArrays4 = 5;    // id | rmin wall_w heat_w nu_t
+}  // namespace
+
+int cryo_state_size(cryo_ctx* c, size_t* bytes) {
+  return guard(c, [&] {
+    c->pull();
+    const size_t n = (size_t)c->hdyn->n;
+    *bytes = sizeof(Blob) + n * (16 * kCkptArrays16 + 4 * kCkptArrays4) + (size_t)(c->P.num_cells + 1) * 4;
+  });
+}
+
+int cryo_save_state(cryo_ctx* c, void* blob, size_t cap) {
+  return guard(c, [&] {
+    c->pull();
+    const size_t n = (size_t)c->hdyn->n;
+    const size_t cells = (size_t)(c->P.num_cells + 1) * 4;
+    const size_t need = sizeof(Blob) + n * (16 * kCkptArrays16 + 4 * kCkptArrays4) + cells;
+    if (cap < need) throw std::out_of_range("cryo_save_state: buffer too small");
+    Blob h{0x43525953u, 1u, (int)n, c->capacity, c->P.num_cells, c->initialized ? 1 : 0, c->has_vapor ? 1 : 0,
+           *c->hdyn};
+    char* p = static_cast<char*>(blob);
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    const Persist& s = c->set[c->cur];
+    const void* a16[kCkptArrays16] = {s.xp, s.vT, s.vt, s.nrm, s.mrps, c->a4, c->ab4, c->fw, c->mw, c->vwp, c->ns4, c->pc};
+    const void* a4[kCkptArrays4] = {s.id, c->rmin, c->wall_w, c->heat_w, c->nu_t};
+    for (const void* a : a16) {
+      CK(cudaMemcpyAsync(p, a, n * 16, cudaMemcpyDeviceToHost, c->stream));
+      p += n * 16;
+    }
+    for (const void* a : a4) {
+      CK(cudaMemcpyAsync(p, a, n * 4, cudaMemcpyDeviceToHost, c->stream));
+      p += n * 4;
+    }
+    CK(cudaMemcpyAsync(p, c->cell_begin, cells, cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+  });
+}
+
+int cryo_load_state(cryo_ctx* c, const void* blob, size_t bytes) {
+  return guard(c, [&] {
+    if (bytes < sizeof(Blob)) throw std::invalid_argument("cryo_load_state: blob too small");
+    Blob h;
+    std::memcpy(&h, blob, sizeof(h));
+    if (h.magic != 0x43525953u || h.version != 1u) throw std::invalid_argument("cryo_load_state: not a state blob");
+    const size_t n = (size_t)h.n;
+    if (!c->has_particles) throw std::runtime_error("cryo_load_state: call set_particles first (grid and parameters)");
+    if (h.num_cells != c->P.num_cells) throw std::invalid_argument("cryo_load_state: grid does not match");
+    const size_t cells = (size_t)(h.num_cells + 1) * 4;
+    if (bytes != sizeof(Blob) + n * (16 * kCkptArrays16 + 4 * kCkptArrays4) + cells)
+      throw std::invalid_argument("cryo_load_state: blob size mismatch");
+    c->sync();
+    if ((int)n > c->capacity || h.capacity > c->capacity) c->allocate(std::max((int)n, h.capacity));
+    const char* p = static_cast<const char*>(blob) + sizeof(Blob);
+    const Persist& s = c->set[c->cur];
+    void* a16[kCkptArrays16] = {s.xp, s.vT, s.vt, s.nrm, s.mrps, c->a4, c->ab4, c->fw, c->mw, c->vwp, c->ns4, c->pc};
+    void* a4[kCkptArrays4] = {s.id, c->rmin, c->wall_w, c->heat_w, c->nu_t};
+    for (void* a : a16) {
+      CK(cudaMemcpyAsync(a, p, n * 16, cudaMemcpyHostToDevice, c->stream));
+      p += n * 16;
+    }
+    for (void* a : a4) {
+      CK(cudaMemcpyAsync(a, p, n * 4, cudaMemcpyHostToDevice, c->stream));
+      p += n * 4;
+    }
+    *c->hdyn = h.dyn;
+    c->hdyn->capacity = c->capacity;
+    c->push();
+    c->initialized = h.initialized != 0;
+    c->has_vapor = h.has_vapor != 0;
+    CK(cudaMemcpyAsync(c->cell_begin, p, cells, cudaMemcpyHostToDevice, c->stream));
+    c->sync();
+  });
+}
+
+int cryo_set_graph_mode(cryo_ctx* c, int enable) {
+  return guard(c, [&] {
+    c->sync();
+    c->graph_mode = enable != 0;
+    c->invalidate_graphs();
+  });
+}
+
+int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {
+  return guard(c, [&] { c->use_lists = use_lists != 0; });
+}
+
+}  // extern "C"

@@ -1,0 +1,246 @@
+// cryo_control.cu -- device-resident step control: the adaptive time step,
+// the manoeuvre frame, the lumped ullage model and the FP64 diagnostics.
+// These replace host code of the reference (sph_solver.cu:244-268,482-504,
+// 586-653) so that a whole step runs without a host round trip.
+#include "cryo_kernels.cuh"
+
+namespace cryo {
+
+// ManeuverProfile::evaluate (sph_solver.cu:244-268)
+__device__ void maneuver_evaluate(const View& V, int n, int rot, double t, V3& a, V3& w, V3& wd) {
+  const double* tt = V.man_t;
+  const float* acc = V.man_acc;
+  const float* om = V.man_omega;
+  auto A = [&](int k) { return v3(acc[3 * k], acc[3 * k + 1], acc[3 * k + 2]); };
+  auto W = [&](int k) { return v3(om[3 * k], om[3 * k + 1], om[3 * k + 2]); };
+  wd = V3{0, 0, 0};
+  if (t <= tt[0] || n == 1) {
+    a = A(0);
+    w = rot ? W(0) : V3{0, 0, 0};
+    return;
+  }
+  if (t >= tt[n - 1]) {
+    a = A(n - 1);
+    w = rot ? W(n - 1) : V3{0, 0, 0};
+    return;
+  }
+  int lo = 0, hi = n;  // upper_bound
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (t < tt[mid]) hi = mid;
+    else lo = mid + 1;
+  }
+  const int k = lo - 1;
+  const double dt = tt[k + 1] - tt[k];
+  const float f = (float)((t - tt[k]) / dt);
+  a = A(k) * (1.0f - f) + A(k + 1) * f;
+  if (rot) {
+    w = W(k) * (1.0f - f) + W(k + 1) * f;
+    wd = (W(k + 1) - W(k)) / (float)dt;
+  } else {
+    w = V3{0, 0, 0};
+  }
+}
+
+// Solver::apply_frame (sph_solver.cu:660-667)
+__device__ void apply_frame(DynState* d, V3 a, V3 w, V3 wd, const float* origin) {
+  d->frame_acc[0] = a.x; d->frame_acc[1] = a.y; d->frame_acc[2] = a.z;
+  d->gravity[0] = d->cfg_gravity[0] - a.x;
+  d->gravity[1] = d->cfg_gravity[1] - a.y;
+  d->gravity[2] = d->cfg_gravity[2] - a.z;
+  d->omega[0] = w.x; d->omega[1] = w.y; d->omega[2] = w.z;
+  d->omega_dot[0] = wd.x; d->omega_dot[1] = wd.y; d->omega_dot[2] = wd.z;
+  d->frame_origin[0] = origin[0]; d->frame_origin[1] = origin[1]; d->frame_origin[2] = origin[2];
+  d->frame_rot = (norm2(w) > 0.0f || norm2(wd) > 0.0f) ? 1 : 0;
+}
+
+// Start of Solver::step (sph_solver.cu:513-522): the step size from the maxima
+// of the previous rate evaluation, the frame at the new time level, and the
+// maxima reset for this step's evaluation (BEGIN_STEP).  BEGIN_RATES only
+// resets the maxima (a rate evaluation outside a step).
+__global__ void k_begin_step(Params P, View V, int mode) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  DynState* d = V.dyn;
+  if (mode == BEGIN_STEP) {
+    const float dt = compute_dt(P, *d);
+    d->dt = dt;
+    if (d->has_maneuver) {
+      V3 a, w, wd;
+      maneuver_evaluate(V, d->man_n, d->man_rot, d->time + (double)dt, a, w, wd);
+      apply_frame(d, a, w, wd, d->man_origin);
+    }
+  }
+  d->v_max = 0.0f;
+  d->a_max = 0.0f;
+  d->Tv_max = 0.0f;
+  d->nu_t_max = 0.0f;
+  d->spacing_ratio = 1.0f;
+}
+
+// Solver::update_saturation (sph_solver.cu:586-607) with the phase inventory
+// (sph_solver.cu:137-145) as one FP64 reduction; with end_of_step the clock
+// advances (sph_solver.cu:530-532) and the relax damping is applied
+// (scale_velocities, sph_solver.cu:716-717).
+__global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce R, int end_of_step) {
+  __shared__ double sh[3 * kBlock / 32];
+  DynState* d = V.dyn;
+  const int n = d->n;
+  const int nch = num_chunks(n);
+  const bool closed = P.thermo_closed && P.has_vapor;
+  const bool damp = end_of_step && d->damp_after_step;
+  const float damping = d->damping;
+  if (closed || damp) {
+    for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+      const int i = c * kChunk + threadIdx.x;
+      double s[3] = {0.0, 0.0, 0.0};
+      if (i < n) {
+        const int ph = ph_of(V.xp[i]);
+        const float4 vT = V.vT[i];
+        if (closed) {
+          const double m = V.mrps[i].x;
+          if (ph == kLiquid) s[0] = m;
+          if (ph == kVapor) {
+            s[1] = m;
+            s[2] = m * vT.w;
+          }
+        }
+        if (damp && is_fluid(ph)) {
+          V.vT[i] = f4(xyz(vT) * damping, vT.w);
+          const float4 vt = V.vt[i];
+          V.vt[i] = f4(xyz(vt) * damping, vt.w);
+        }
+      }
+      if (closed) publish_chunk<3>(R, c, s, sh);
+    }
+  }
+  const bool last = closed ? last_block(R.ticket) : (blockIdx.x == 0);
+  if (!last || threadIdx.x != 0) return;
+  bool done = false;
+  if (closed) {
+    const double m_liq = sum_partials(R, 0, nch);
+    const double m_vap = sum_partials(R, 1, nch);
+    const double mT_vap = sum_partials(R, 2, nch);
+    if (!(d->fluid_volume0 > 0)) d->fluid_volume0 = m_liq / P.f_rho_l + m_vap / P.f_rho_v;
+    const double v_ullage = d->fluid_volume0 - m_liq / P.f_rho_l;
+    const double ratio = v_ullage > 0 && m_vap > 0 ? (mT_vap / v_ullage) / ((double)P.f_rho_v * P.f_T_sat) : 0.0;
+    if (isfinite(ratio) && ratio > 0) {
+      d->p_ullage = P.f_p_sat * ratio;
+      // FluidProperties::saturation_temperature (fluid_properties.cpp:7-10)
+      const float p = (float)d->p_ullage;
+      const double inv_T = 1.0 / P.f_T_sat - ((double)P.f_R_gas / P.f_h_fg) * log((double)p / P.f_p_sat);
+      d->T_sat = (float)(1.0 / inv_T);
+      done = true;
+    }
+  }
+  if (!done) {
+    d->p_ullage = P.f_p_sat;
+    d->T_sat = P.f_T_sat;
+  }
+  if (end_of_step) {
+    d->time += (double)d->dt;
+    d->step += 1;
+    d->last_dt = (double)d->dt;
+  }
+}
+
+// Heat-weight normalisation on its own (sph_solver.cu:466-472), for
+// operator-level calls.
+__global__ void __launch_bounds__(kBlock) k_heat_norm(Params P, View V, Reduce R) {
+  __shared__ double sh[kBlock / 32];
+  DynState* d = V.dyn;
+  const int n = d->n;
+  const int nch = num_chunks(n);
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int i = c * kChunk + threadIdx.x;
+    double s[1] = {0.0};
+    if (i < n && is_fluid(ph_of(V.xp[i]))) s[0] = (double)V.heat_w[i];
+    publish_chunk<1>(R, c, s, sh);
+  }
+  if (last_block(R.ticket) && threadIdx.x == 0) {
+    if (P.heat_power != 0.0f) {
+      const double S = sum_partials(R, 0, nch);
+      d->heat_inv_norm = S > 0 ? (float)(1.0 / S) : 0.0f;
+    } else {
+      d->heat_inv_norm = 0.0f;
+    }
+  }
+}
+
+// Solver::diagnostics (sph_solver.cu:609-653): every phase sum, count and
+// maximum in one FP64 pass.  out[] layout:
+//   0-2 counts L/V/W, 3-4 mass L/V, 5-6 KE L/V, 7-8 enthalpy L/V, 9-10 mT L/V,
+//   11-13 m x (L), 14-16 m v (L), 17-19 sum fw (fluid), 20-22 sum mw (fluid),
+//   23 max fluid speed, 24 max liquid T
+__global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce R, double* __restrict__ out) {
+  __shared__ double sh[23 * kBlock / 32];
+  __shared__ float shmax[2][kBlock / 32];
+  DynState* d = V.dyn;
+  const int n = d->n;
+  const int nch = num_chunks(n);
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int i = c * kChunk + threadIdx.x;
+    double s[23];
+#pragma unroll
+    for (int k = 0; k < 23; ++k) s[k] = 0.0;
+    float vmax = 0.0f, tmax = 0.0f;
+    if (i < n) {
+      const float4 xp = V.xp[i];
+      const int ph = ph_of(xp);
+      const float4 vT = V.vT[i];
+      const double m = V.mrps[i].x;
+      if (ph == kLiquid || ph == kVapor) {
+        const int k = ph;
+        s[k] = 1.0;
+        s[3 + k] = m;
+        s[5 + k] = 0.5 * m * (double)norm2(xyz(vT));
+        s[7 + k] = m * (double)specific_enthalpy(P, ph, vT.w);
+        s[9 + k] = m * vT.w;
+        const float4 fw = V.fw[i], mw = V.mw[i];
+        s[17] = fw.x; s[18] = fw.y; s[19] = fw.z;
+        s[20] = mw.x; s[21] = mw.y; s[22] = mw.z;
+        vmax = norm(xyz(vT));
+        if (ph == kLiquid) {
+          s[11] = m * xp.x; s[12] = m * xp.y; s[13] = m * xp.z;
+          s[14] = m * vT.x; s[15] = m * vT.y; s[16] = m * vT.z;
+          tmax = vT.w;
+        }
+      } else if (ph == kWall) {
+        s[2] = 1.0;
+      }
+    }
+    publish_chunk<23>(R, c, s, sh);
+    // chunk maxima (order-free)
+    vmax = warp_max(vmax);
+    tmax = warp_max(tmax);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0) {
+      shmax[0][warp] = vmax;
+      shmax[1][warp] = tmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      float a = 0.0f, b = 0.0f;
+      for (int w = 0; w < kBlock / 32; ++w) {
+        a = fmaxf(a, shmax[0][w]);
+        b = fmaxf(b, shmax[1][w]);
+      }
+      R.partials[(size_t)23 * R.max_chunks + c] = a;
+      R.partials[(size_t)24 * R.max_chunks + c] = b;
+    }
+    __syncthreads();
+  }
+  if (last_block(R.ticket)) {
+    // 25 values: one thread each
+    const int v = threadIdx.x;
+    if (v < 23) {
+      out[v] = sum_partials(R, v, nch);
+    } else if (v < 25) {
+      double mx = 0.0;
+      const double* p = R.partials + (size_t)v * R.max_chunks;
+      for (int k = 0; k < nch; ++k) mx = fmax(mx, __ldcg(p + k));
+      out[v] = mx;
+    }
+  }
+}
+
+}  // namespace cryo

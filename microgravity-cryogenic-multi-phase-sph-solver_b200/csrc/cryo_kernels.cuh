@@ -1,0 +1,109 @@
+// cryo_kernels.cuh -- declarations of the device kernels (one definition file
+// each: cryo_grid.cu, cryo_physics.cu, cryo_phase.cu, cryo_control.cu).
+#pragma once
+
+#include "cryo_common.cuh"
+
+namespace cryo {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_TILE = 4096;  // keys per radix tile (16 per thread)
+constexpr int RS_BITS = 8;
+constexpr int RS_BINS = 1 << RS_BITS;
+
+// Layout of the FP64 partials of one reduction: partials[v * max_chunks + c].
+struct Reduce {
+  double* partials;
+  unsigned* ticket;
+  int max_chunks;
+};
+
+
+// Last-block ticket: true in exactly one block, after every block of the grid
+// has published its partials (each block fences before taking a ticket).
+__device__ inline bool last_block(unsigned* ticket) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) is_last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (is_last && threadIdx.x == 0) *ticket = 0u;  // ready for the next launch
+  return is_last;
+}
+// Sum of value v over chunks [0, nchunks) (fixed order, compensated), run by
+// thread 0 of the last block.
+__device__ inline double sum_partials(const Reduce& R, int v, int nchunks) {
+  double s = 0, c = 0;
+  const double* p = R.partials + (size_t)v * R.max_chunks;
+  for (int k = 0; k < nchunks; ++k) {
+    const double x = __ldcg(p + k);
+    const double t = s + x;
+    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+    s = t;
+  }
+  return s + c;
+}
+// Writes the block sums of NV values for chunk c.
+template <int NV>
+__device__ inline void publish_chunk(const Reduce& R, int c, double (&v)[NV], double* sh) {
+  block_sum<NV>(v, sh);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) R.partials[(size_t)k * R.max_chunks + c] = v[k];
+}
+__device__ inline int num_chunks(int n) { return (n + kChunk - 1) / kChunk; }
+
+// grid (cryo_grid.cu)
+__global__ void k_keys(Params P, View V, uint32_t* keys);
+__global__ void k_rs_upsweep(const uint32_t* keys, int shift, int bits, const DynState* dyn, uint32_t* hist);
+__global__ void k_rs_scan(uint32_t* hist, const DynState* dyn);
+__global__ void k_rs_downsweep(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int shift,
+                               int bits, const DynState* dyn, const uint32_t* hist);
+__global__ void k_cells(Params P, const uint32_t* keys, DynState* dyn, int* cell_begin);
+__global__ void k_gather(View src, View dst, const uint32_t* perm);
+__global__ void k_nbr_count(Params P, View V, int* counts);
+__global__ void k_nbr_fill(Params P, View V, const long long* offsets, int* list);
+
+// physics (cryo_physics.cu)
+__global__ void k_density(Params P, View V, int fuse_eos);
+__global__ void k_normalize_masses(Params P, View V);
+__global__ void k_eos(Params P, View V);
+__global__ void k_wall(Params P, View V);
+// heat_sum: 0 none, 1 when thermal is on (step), 2 always (operator call)
+__global__ void k_interface(Params P, View V, Reduce R, int heat_sum);
+__global__ void k_sps(Params P, View V);
+__global__ void k_smooth_normals(Params P, View V);
+// Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
+enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8, FORCE_DRHO = 16,
+       FORCE_THERMAL = 32, FORCE_MAXIMA = 64, FORCE_THERMAL_ALWAYS = 128 };
+__global__ void k_forces(Params P, View V, int what);
+__global__ void k_shift_compute(Params P, View V);
+__global__ void k_shift_apply(Params P, View V);
+__global__ void k_probe(Params P, View V, const float* pts, int np, float* out);
+
+// integrator + phase change (cryo_phase.cu)
+__global__ void k_kick_drift(Params P, View V, int continuity, int tvf);
+__global__ void k_kick_drift_keys(Params P, View V, uint32_t* keys);
+enum { KICK_SOURCES = 1, KICK_HEAT = 2 };
+__global__ void k_kick(Params P, View V, int flags);
+__global__ void k_pc_sources(Params P, View V);
+__global__ void k_pc_normalize(Params P, View V, Reduce R, int sums);
+__global__ void k_pc_apply(Params P, View V, int gated);
+__global__ void k_rebalance1(Params P, View V, int gated);
+__global__ void k_rebalance2_mark(Params P, View V, Reduce R, uint32_t* flag, int rebalance, int gated);
+__global__ void k_split(Params P, View V, Reduce R, const uint32_t* flag, int gated);
+__global__ void k_venting(Params P, View V, Reduce R, float relax, int gated);
+__global__ void k_scale_velocities(View V, float factor, int scale_vmax);
+
+// step control + reductions (cryo_control.cu)
+enum { BEGIN_STEP = 0, BEGIN_RATES = 1 };
+__global__ void k_begin_step(Params P, View V, int mode);
+__global__ void k_heat_norm(Params P, View V, Reduce R);
+__global__ void k_maxima(Params P, View V);
+__global__ void k_saturation(Params P, View V, Reduce R, int end_of_step);
+__global__ void k_diagnostics(Params P, View V, Reduce R, double* out);
+
+// Number of FP64 values per chunk of the diagnostics reduction.
+constexpr int kDiagValues = 30;
+
+}  // namespace cryo

@@ -340,3 +340,27 @@ class Oracle(_Checker):
 
     def __init__(self, cfg, fluid):
         super().__init__(ORACLE_LIB, cfg, fluid)
+        self.L.orc_set_field.restype = C.c_int
+        self.L.orc_set_field.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        self.L.orc_grid_sort.restype = C.c_int
+        self.L.orc_grid_sort.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        self.L.orc_scalars.restype = C.c_int
+        self.L.orc_scalars.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+
+    def set_field(self, name, data):
+        n = self.num_particles()
+        a = np.ascontiguousarray(data, dtype=cabi.field_dtype(name, self.real)).reshape(cabi.field_shape(name, n))
+        self.check(self.L.orc_set_field(self.h, cabi.FIELD_ID[name], a.ctypes.data_as(C.c_void_p)))
+
+    def grid_sort(self):
+        n = self.num_particles()
+        k = np.empty(n, np.uint32)
+        p = np.empty(n, np.uint32)
+        self.check(self.L.orc_grid_sort(self.h, k.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p)))
+        return k, p
+
+    def scalars(self):
+        out = (C.c_double * 8)()
+        self.check(self.L.orc_scalars(self.h, out))
+        keys = ["p_ullage", "fluid_volume0", "v_max", "a_max", "Tv_max", "spacing_ratio", "nu_t_max", "heat_input"]
+        return dict(zip(keys, list(out)))

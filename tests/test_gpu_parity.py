@@ -1,0 +1,199 @@
+"""Parity of the CUDA path (libcryosph_b200.so, called through the C ABI)
+with the oracle (oracle/cryo_oracle.c, pinned bit-for-bit to the reference's
+CPU build by test_oracle_vs_ref.py).
+
+Bar:
+* bit-exact for integer and index results: sorted keys, permutation, cell
+  tables, neighbour lists, phase/flags/ids;
+* fields: normwise relative error max|gpu - oracle| / max|oracle| <= 1e-5 per
+  field and pass (most come out bit-identical: both sides run the same IEEE
+  single-precision operation sequence; libm calls powf/cosf/sinf/cbrtf/log
+  may differ in the last place);
+* diagnostics (FP64 sums in a different order): 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+import cryo_cabi as cabi
+import refpy
+import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+FIELD_RTOL = 1e-5
+PERSISTENT = ["x", "v", "vt", "nrm", "m", "m0", "rho", "T", "phase", "flags", "id"]
+INT_FIELDS = {"phase", "flags", "id"}
+
+
+def make_pair(name):
+    cfg, fl, parts, lo, hi = S.SCENARIOS[name]()
+    g = cabi.Context(cfg, fl)
+    o = refpy.Oracle(cfg, fl)
+    g.set_particles(parts, lo, hi)
+    o.set_particles(parts, lo, hi)
+    return cfg, g, o
+
+
+def masks(g):
+    ph = g.field("phase")
+    return {"all": np.ones(len(ph), bool), "fluid": ph <= 1, "wall": ph == 2, "liquid": ph == 0, "vapor": ph == 1}
+
+
+def compare(g, o, fields, where="all", tol=FIELD_RTOL, report=None, tag=""):
+    m = masks(o)[where]
+    for f in fields:
+        a, b = g.field(f), o.field(f)
+        assert a.shape == b.shape, (tag, f, a.shape, b.shape)
+        a, b = a[m], b[m]
+        if f in INT_FIELDS:
+            assert np.array_equal(a, b), f"{tag}: {f} differs at {np.flatnonzero(a != b)[:10]}"
+            continue
+        err = S.normwise(a, b)
+        exact = bool(np.array_equal(a.view(np.uint32), b.view(np.uint32)))
+        if report is not None:
+            report.append((tag, f, where, err, exact))
+        assert err <= tol, f"{tag}: {f} ({where}) normwise error {err:.3e} > {tol:.1e}"
+
+
+def resync(g, o, fields):
+    """Copies the oracle's values into the GPU state so the next pass starts
+    from identical inputs (isolates each pass's error)."""
+    for f in fields:
+        g.set_field(f, o.field(f))
+
+
+SCEN = ["c1", "box_split", "vented", "dam_break", "akinci", "options"]
+
+
+@pytest.mark.parametrize("name", SCEN)
+def test_grid_build_and_neighbor_lists_bit_exact(cuda_device, name):
+    cfg, g, o = make_pair(name)
+    g.run_pass("grid_build")
+    o.run_pass("grid_build")
+    keys, perm, cs, ce = g.grid_tables()
+    ok, op = o.grid_sort()
+    ocs, oce = o.cell_tables()
+    assert np.array_equal(keys, ok[: len(keys)]), "sorted keys differ"
+    assert np.array_equal(perm, op[: len(perm)]), "permutation differs (stable sort)"
+    assert np.array_equal(cs, ocs) and np.array_equal(ce, oce), "cell_start/cell_end differ"
+    for f in PERSISTENT:
+        a, b = g.field(f), o.field(f)
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), f"{f} differs after reorder"
+    gc, gl = g.neighbor_lists()
+    oc, ol = o.neighbor_lists()
+    assert np.array_equal(gc, oc), "neighbour counts differ"
+    assert np.array_equal(gl, ol), "neighbour lists differ (membership or order)"
+
+
+def pass_plan(cfg, has_vapor):
+    """(pass, fields written, particle subset) in Solver::step order."""
+    plan = [
+        ("normalize_masses", ["m", "m0"], "fluid"),
+        ("density", ["sigma", "rmin"], "all"),
+        ("density", ["rho"], "fluid"),
+        ("eos", ["p"], "fluid"),
+        ("wall_boundary", ["p", "p_wv", "alpha", "rho", "vw", "a"], "wall"),
+        ("interface", ["alpha", "wall_w", "heat_w", "nrm"] + (["vw"] if cfg.surface_tension != 2 else []), "fluid"),
+        ("transport", ["ab"], "all"),
+    ]
+    if cfg.sps_turbulence:
+        plan.append(("sps", ["nu_t"], "all"))
+    plan.append(("momentum", ["a", "fw", "mw"], "all"))
+    if cfg.surface_tension == 1 and has_vapor:
+        plan.append(("smooth_normals", ["ns"], "fluid"))
+        plan.append(("csf", ["kappa", "a"], "fluid"))
+    elif cfg.surface_tension == 2:
+        plan.append(("akinci", ["a"], "all"))
+    if cfg.density_mode == 1:
+        plan.append(("density_rate", ["drho"], "all"))
+    if cfg.thermal:
+        plan.append(("thermal", ["dTdt"], "all"))
+    plan.append(("kick", ["v", "T"], "fluid"))
+    if cfg.phase_change:
+        plan += [
+            ("pc_sources", ["out_m", "out_h", "w_norm", "flags"], "all"),
+            ("pc_normalize", ["out_m", "w_norm"], "all"),
+            ("pc_apply", ["m", "T", "phase"], "all"),
+        ]
+        if has_vapor and cfg.vapor_mass_rebalance > 0:
+            plan.append(("rebalance", ["out_m", "out_h", "ns", "m", "T", "v", "vt"], "all"))
+        if cfg.thermo_mode == 0 and has_vapor:
+            plan.append(("venting", ["out_m", "out_h", "m", "rho"], "all"))
+    return plan
+
+
+@pytest.mark.parametrize("name", SCEN)
+def test_pass_parity(cuda_device, name):
+    cfg, g, o = make_pair(name)
+    has_vapor = bool((o.field("phase") == 1).any())
+    report = []
+    g.run_pass("grid_build")
+    o.run_pass("grid_build")
+    dt = 1e-4
+    g.set_pass_dt(dt)
+    o.set_pass_dt(dt)
+    for pname, fields, where in pass_plan(cfg, has_vapor):
+        g.run_pass(pname)
+        o.run_pass(pname)
+        tol = FIELD_RTOL
+        compare(g, o, fields, where, tol=tol, report=report, tag=pname)
+        resync(g, o, [f for f in fields if f not in ("phase", "flags")])
+    exact = sum(1 for r in report if r[4])
+    print(f"\n[{name}] {exact}/{len(report)} pass outputs bit-exact; worst:",
+          max(report, key=lambda r: r[3]) if report else None)
+
+
+@pytest.mark.parametrize("name", ["c1", "box_split", "dam_break", "options"])
+def test_step_parity(cuda_device, name):
+    """Whole Solver::step sequences (adaptive dt, graphs) from identical inputs."""
+    cfg, g, o = make_pair(name)
+    nsteps = 5
+    g.step(nsteps)
+    o.step(nsteps)
+    tg, sg, dtg = g.time()
+    to, so, dto = o.time()
+    assert sg == so == nsteps
+    assert abs(tg - to) <= 1e-6 * abs(to), (tg, to)
+    assert g.num_particles() == o.num_particles()
+    worst = []
+    for f in ["x", "v", "m", "rho", "T", "p", "sigma", "a", "ab"]:
+        err = S.normwise(g.field(f), o.field(f))
+        worst.append((f, err))
+        assert err <= 1e-4, f"{f}: {err:.3e}"
+    for f in ["phase", "id"]:
+        assert np.array_equal(g.field(f), o.field(f)), f
+    dg, do = g.diagnostics().as_dict(), o.diagnostics().as_dict()
+    for k in ["mass_liquid", "mass_vapor", "mass_total", "enthalpy", "T_sat", "p_ullage", "heat_input",
+              "evaporated_mass", "condensed_mass"]:
+        ref = do[k]
+        assert abs(dg[k] - ref) <= 1e-6 * max(abs(ref), 1e-30) + 1e-30, (k, dg[k], ref)
+    assert dg["n_liquid"] == do["n_liquid"] and dg["n_vapor"] == do["n_vapor"] and dg["n_wall"] == do["n_wall"]
+    print(f"\n[{name}] step parity, worst fields:", sorted(worst, key=lambda t: -t[1])[:3])
+
+
+def test_graph_replay_matches_eager_bitwise(cuda_device):
+    cfg, fl, parts, lo, hi = S.c1()
+    runs = []
+    for graph in (True, False):
+        g = cabi.Context(cfg, fl)
+        g.set_graph_mode(graph)
+        g.set_particles(parts, lo, hi)
+        g.step(6)
+        runs.append({f: g.field(f) for f in PERSISTENT})
+    for f in PERSISTENT:
+        assert np.array_equal(runs[0][f].view(np.uint8), runs[1][f].view(np.uint8)), f
+
+
+def test_runs_are_bitwise_deterministic(cuda_device):
+    """test_determinism.cpp:40-54 on the GPU: two identical runs (with splits)."""
+    cfg, fl, parts, lo, hi = S.box_split()
+    out = []
+    for _ in range(2):
+        g = cabi.Context(cfg, fl)
+        g.set_particles(parts, lo, hi)
+        g.step(60)
+        d = g.diagnostics()
+        out.append(({f: g.field(f) for f in ["x", "v", "m", "T", "id"]}, d.splits, d.mass_total, d.enthalpy))
+    for f in out[0][0]:
+        assert np.array_equal(out[0][0][f].view(np.uint8), out[1][0][f].view(np.uint8)), f
+    assert out[0][1:] == out[1][1:]
