@@ -1,0 +1,461 @@
+"""Throughput of the per-step particle update on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--workload dam_break|c1|c3] [--impl ours|reference]
+
+Workload (default): the SPHERIC Test 2 dam break with an obstacle at dx 0.02 m
+(203 662 particles with walls, 82 350 fluid), continuity density, free-slip
+walls, no surface tension or heat, fluid lattice jittered +-0.05 dx from
+numpy PCG64(2002).  One step = one Solver::step.  The metric counts wall
+particles (as the reference's perf_scaling.cpp does).
+
+Timing: W untimed steps, then K steps, each bracketed by CUDA events on the
+solver's stream, with a 256 MiB memset between steps (outside the events) so
+every step starts with a cold L2 -- the dam-break state (~61 MB) would
+otherwise stay resident in the 126 MB L2.  value = particles * K / sum(step
+times).  Multi-GPU (torchrun): every rank runs its own replica, barrier on both
+sides, max over ranks.
+
+Also reported: e2e (the same steps through the public API with host buffers:
+per step the frame-motion input goes host->device and the diagnostics come
+back device->host, plus the initial state upload and the final download),
+the roofline of the dominant kernel (per-kernel CUDA-event times from a
+profiled run, algorithmic bytes from cryo_roofline.py, DRAM traffic from the
+committed ncu summary), SM clocks sampled during the timed region, and the
+reference's own CPU implementation timed on this host (rank 0, N=1).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "microgravity-cryogenic-multi-phase-sph-solver_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "particle-steps/s/GPU (plain)"
+UNIT = "particle-steps/s"
+SEED = 2002
+
+
+# ----------------------------------------------------------------- workloads
+def workload(name, cs):
+    """(label, SolverConfig, fluid, particle dict, domain lo, hi, config dict for the C ABI)."""
+    if name == "dam_break":
+        dx = 0.02
+        water = cs.FluidProperties.water()
+        water.mu_liquid = 1.0e-3
+        cfg = cs.SolverConfig()
+        cfg.dx = dx
+        cfg.gravity = (0.0, 0.0, -9.81)
+        cfg.surface_tension = cs.SurfaceTensionModel.NoTension
+        cfg.thermal = False
+        cfg.phase_change = False
+        cfg.density_mode = cs.DensityMode.Continuity
+        cfg.velocity_scale = (2 * 9.81 * 0.55) ** 0.5
+        cfg.artificial_viscosity = 0.02
+        cfg.delta_sph = 0.1
+        cfg.no_slip = False
+        x_front, box = 0.744, (0.161, 0.403, 0.161)
+        tank = cs.Translated(cs.BoxTank(3.22, 1.0, 1.0), (1.61, 0.0, 0.5))
+        obst = cs.Translated(cs.BoxTank(*box), (x_front - box[0] / 2, 0.0, box[2] / 2))
+        fill = cs.FillSpec()
+        fill.mode = cs.FillMode.Full
+        p = cs.tank_particles(cs.Difference(tank, obst), water, dx, fill)
+        x, ph = p["position"], p["phase"]
+        keep = (ph == 2) | ((x[:, 0] > 3.22 - 1.228) & (x[:, 2] < 0.55))
+        p = {k: v[keep] for k, v in p.items()}
+        pad = 4 * dx
+        lo, hi = (-pad, -0.5 - pad, -pad), (3.22 + pad, 0.5 + pad, 1.0 + pad)
+        label, fluid = "dam_break_spheric2_dx0.02", water
+    elif name in ("c1", "c3"):
+        if name == "c1":
+            fluid = cs.FluidProperties.liquid_nitrogen()
+            dx, geo, g = 0.004, cs.CylinderTank(0.05, 0.12), (0.0, 0.0, -9.81e-4)
+            label = "c1_ln2_cylinder_dx0.004"
+        else:
+            fluid = cs.FluidProperties.liquid_hydrogen()
+            dx, geo, g = 0.0052, cs.SphereTank(0.5), (0.0, 0.0, -9.81e-4)
+            label = "c3_lh2_sphere_dx0.0052"
+        cfg = cs.SolverConfig()
+        cfg.dx = dx
+        cfg.gravity = g
+        cfg.heater_power = 20.0 if name == "c1" else 0.0
+        cfg.thermo_mode = cs.TankThermoMode.Closed
+        fill = cs.FillSpec()
+        fill.fill_fraction = 0.5
+        p = cs.tank_particles(geo, fluid, dx, fill)
+        lo, hi = cs.tank_domain(geo, dx, 3)
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    fl = p["phase"] != 2
+    x = p["position"].astype(np.float32).copy()
+    x[fl] += rng.uniform(-0.05 * dx, 0.05 * dx, size=(int(fl.sum()), 3)).astype(np.float32)
+    p["position"] = x
+    return label, cfg, fluid, p, lo, hi
+
+
+def load(solver, p, lo, hi):
+    solver.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"], domain_lo=lo,
+                         domain_hi=hi, normal=p["normal"], flags=p["flags"])
+
+
+def c_config(cs_cfg):
+    """SolverConfig (module object) -> cryo_config_t fields (for the reference arm)."""
+    import cryo_cabi as cabi
+    kw = {}
+    for name, _ in cabi.CONFIG_FIELDS:
+        v = getattr(cs_cfg, name)
+        if name == "gravity":
+            kw[name] = tuple(v)
+        elif hasattr(v, "value"):
+            kw[name] = int(v.value)
+        elif isinstance(v, bool):
+            kw[name] = int(v)
+        else:
+            kw[name] = v
+    return cabi.py_config(**kw)
+
+
+def c_fluid(f):
+    import cryo_cabi as cabi
+    out = cabi.Fluid()
+    for k, _ in cabi.Fluid._fields_:
+        setattr(out, k, getattr(f, k))
+    return out
+
+
+# ---------------------------------------------------------------- clocks
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200", "-f", self.path],
+                                         stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            with open(self.path) as fh:
+                for line in fh:
+                    parts = [s.strip() for s in line.split(",")]
+                    if len(parts) >= 9:
+                        rows.append(parts)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------- reference arm
+def reference_rate(cs_cfg, fluid, p, lo, hi, steps, warmup, budget_s=60.0):
+    """The reference's CPU implementation (oracle/_ref, built from its own
+    sources) on the same workload, all host threads; returns (rate, threads,
+    steps timed, seconds)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refpy
+    if not refpy.ref_available():
+        return None
+    ref = refpy.Ref(c_config(cs_cfg), c_fluid(fluid))
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    arrays = {"x": p["position"], "m": p["mass"], "rho": p["density"], "T": p["temperature"], "phase": p["phase"],
+              "nrm": p["normal"], "flags": p["flags"]}
+    ref.set_particles(arrays, lo, hi)
+    ref.step(max(1, min(warmup, 2)))
+    t0 = time.perf_counter()
+    ref.step(1)
+    one = time.perf_counter() - t0
+    k = int(max(2, min(steps, budget_s / max(one, 1e-6))))
+    t0 = time.perf_counter()
+    ref.step(k)
+    el = time.perf_counter() - t0
+    n = ref.num_particles()
+    return n * k / el, threads, k, el
+
+
+# ------------------------------------------------------------------- main
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--workload", default="dam_break")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-steps", type=int, default=50)
+    ap.add_argument("--only-timed", action="store_true",
+                    help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import CryoSPH as cs
+
+    label, cfg, fluid, p, lo, hi = workload(args.workload, cs)
+    n_total = int(len(p["position"]))
+    n_wall = int((p["phase"] == 2).sum())
+    n_fluid = n_total - n_wall
+    has_vapor = bool((p["phase"] == 1).any())
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        r = reference_rate(cfg, fluid, p, lo, hi, args.steps, args.warmup)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
+            return 0
+        rate, threads, k, el = r
+        line = {
+            "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
+            "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": label, "particles": n_total, "fluid": n_fluid, "walls": n_wall},
+            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                             "sample": f"{k} steps of the workload after 2 warm-up steps (OpenMP, {threads} threads)"},
+            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import cryo_cabi as cabi
+
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    device = local
+
+    L = cabi.load()
+    solver = cs.Solver(cfg, fluid, device)
+    load(solver, p, lo, hi)
+    stream = torch.cuda.ExternalStream(solver.stream_handle, device=device)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
+
+    solver.run_steps(args.warmup)
+    torch.cuda.synchronize()
+
+    # ---- timed: device time of K steps, L2 flushed between steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(device) as clk:
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                solver.step()
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    clocks = clk.summary()
+    n_now = solver.num_particles
+    t = torch.tensor([total_ms], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    value = world * n_total * args.steps / (max_ms / 1e3)
+    per_step = ctypes_int(L, "cryo_kernels_per_step", solver.handle)
+
+    e2e = roof = None
+    if rank == 0 and not args.only_timed:
+        # ---- e2e through the public API with host buffers
+        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, min(args.steps, 200), device, stream, flush)
+        # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
+        roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
+        r = reference_rate(cfg, fluid, p, lo, hi, 200, 2, budget_s=20.0)
+        if r is not None:
+            rate, threads, k, el = r
+            cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                   "sample": f"{k} steps of {label} after 2 warm-up steps ({el:.1f} s, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 fields, f64 reductions", "data": "synthetic",
+            "config": {"workload": label, "particles": n_total, "fluid": n_fluid, "walls": n_wall,
+                       "particles_after": int(n_now), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+                       "l2": "flushed between timed steps (256 MiB memset outside the events)",
+                       "execution": "CUDA graph per step", "seed": SEED},
+            "per_gpu": value / world,
+            "gpu_launches": per_step * args.steps,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "e2e": e2e,
+            "roofline": roof,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def ctypes_int(L, fn, handle):
+    import ctypes as C
+    v = C.c_int()
+    getattr(L, fn)(C.c_void_p(handle), C.byref(v))
+    return v.value
+
+
+def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
+    """Public-API run with host buffers: state upload, then per step the
+    frame-motion input (host->device) and the diagnostics (device->host), then
+    the state download.  Device-timed per step with L2 flushed between steps."""
+    import torch
+    solver = cs.Solver(cfg, fluid, device)
+    x = np.ascontiguousarray(p["position"], np.float64)
+    arrays = [x, p["mass"].astype(np.float64), p["density"].astype(np.float64), p["temperature"].astype(np.float64)]
+    state_in = sum(a.nbytes for a in arrays) + p["phase"].nbytes + p["normal"].nbytes + p["flags"].nbytes
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    st = torch.cuda.ExternalStream(solver.stream_handle, device=device)
+    torch.cuda.synchronize()
+    state_out = 0
+    with torch.cuda.stream(st):
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(st)
+            if k == 0:
+                load(solver, p, lo, hi)
+            a = 0.01 * math.sin(0.01 * k)
+            solver.set_frame_motion(acceleration=(a, 0.0, 0.0))
+            solver.step()
+            d = solver.diagnostics()
+            _ = d.slosh_force
+            if k == steps - 1:
+                parts = solver.particles()
+                state_out = sum(v.nbytes for v in parts.values())
+            ev[k][1].record(st)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    n = solver.num_particles
+    ctl = 3 * 4 * 4          # acceleration, omega, omega_dot, origin (float3 each)
+    diag = 8 * 25 + 8 * 64   # diagnostics reduction + scalar block
+    return {"value": n * steps / (ms / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": int(state_in / steps + ctl), "d2h_bytes_per_step": int(diag + state_out / steps),
+            "steps": steps, "timing": "CUDA events per step (host work inside), L2 flushed between steps"}
+
+
+def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vapor, label):
+    import ctypes as C
+    import cryo_roofline as RF
+    solver = cs.Solver(cfg, fluid)
+    load(solver, p, lo, hi)
+    solver.run_steps(3)
+    h = C.c_void_p(solver.handle)
+    L.cryo_set_profiling.argtypes = [C.c_void_p, C.c_int]
+    L.cryo_kernel_times.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.c_char_p, C.POINTER(C.c_double),
+                                    C.POINTER(C.c_longlong)]
+    L.cryo_set_profiling(h, 1)
+    solver.run_steps(steps)
+    cnt = C.c_int(0)
+    L.cryo_kernel_times(h, C.byref(cnt), None, None, None)
+    k = cnt.value
+    names = C.create_string_buffer(64 * k)
+    ms = (C.c_double * k)()
+    launches = (C.c_longlong * k)()
+    cnt2 = C.c_int(k)
+    L.cryo_kernel_times(h, C.byref(cnt2), names, ms, launches)
+    L.cryo_set_profiling(h, 0)
+    rows = []
+    for i in range(k):
+        nm = names.raw[64 * i: 64 * i + 64].split(b"\0")[0].decode()
+        rows.append((nm, ms[i], launches[i]))
+    total = sum(r[1] for r in rows)
+    top = max(rows, key=lambda r: r[1])
+    peaks = {}
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as fh:
+            peaks = json.load(fh)
+    except OSError:
+        pass
+    peak = peaks.get("hbm_gbs", 6650.0)
+    nc = 0
+    avg_ms = top[1] / max(top[2], 1)
+    alg = RF.kernel_bytes(top[0], cfg_dict(cfg), n_fluid, n_wall, has_vapor, nc)
+    achieved = alg / (avg_ms / 1e3) / 1e9
+    traffic = ncu_traffic(top[0], label)
+    return {"kernel": top[0], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg, "avg_launch_ms": avg_ms,
+            "share": top[1] / total if total else None, "peak_source": "measured" if peaks else "fallback",
+            "kernels": {r[0]: {"ms_per_step": r[1] / steps, "launches": r[2]} for r in sorted(rows, key=lambda r: -r[1])}}
+
+
+def cfg_dict(cfg):
+    out = {}
+    for k in ["density_mode", "transport_velocity", "thermal", "phase_change", "surface_tension", "wetting_model",
+              "sps_turbulence", "transport_stress"]:
+        v = getattr(cfg, k)
+        out[k] = int(v.value) if hasattr(v, "value") else int(v)
+    return out
+
+
+def ncu_traffic(kernel, label):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary (null if absent)."""
+    path = os.path.join(REPO, "profiles", "ncu_dram.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        e = d.get(label, {}).get(kernel)
+        return None if e is None else float(e)
+    except (OSError, ValueError):
+        return None
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -290,6 +290,30 @@ int cryo_state_size(cryo_ctx* ctx, size_t* bytes);
 int cryo_save_state(cryo_ctx* ctx, void* blob, size_t cap);
 int cryo_load_state(cryo_ctx* ctx, const void* blob, size_t bytes);
 
+/* ------------------------------------------------------------ telemetry
+ * TelemetryStream (telemetry.hpp:13-70, telemetry.cu:27-127): a non-blocking
+ * capture of x, T, p, |v| and phase.  mode 0 = AsyncCopy (device staging +
+ * pinned host buffer on a copy stream), 1 = ZeroCopy (kernel writes mapped
+ * pinned memory).  request returns *accepted = 0 while a frame is pending. */
+int cryo_telemetry_configure(cryo_ctx* ctx, int mode);
+int cryo_telemetry_mode(cryo_ctx* ctx, int* mode);
+int cryo_telemetry_request(cryo_ctx* ctx, int* accepted);
+int cryo_telemetry_ready(cryo_ctx* ctx, int* ready);
+int cryo_telemetry_pending(cryo_ctx* ctx, int* pending);
+/* Waits for the pending frame.  *got = 0 when nothing was requested.  Arrays
+ * must hold *n entries (query with positions == NULL first: returns n only). */
+int cryo_telemetry_fetch(cryo_ctx* ctx, int* got, double* time, long long* step, int* n, float* position,
+                         float* temperature, float* pressure, float* speed, uint8_t* phase);
+
+/* ------------------------------------------------------------ profiling
+ * With profiling on, steps run as individual launches bracketed by CUDA
+ * events and the device time of every kernel is accumulated per kernel name. */
+int cryo_set_profiling(cryo_ctx* ctx, int enable);
+/* Kernel count and names/totals: names is a buffer of count*64 chars. */
+int cryo_kernel_times(cryo_ctx* ctx, int* count, char* names, double* total_ms, long long* launches);
+/* Number of kernel launches one step issues with the current settings. */
+int cryo_kernels_per_step(cryo_ctx* ctx, int* launches);
+
 /* Execution mode: 1 = capture each step as a CUDA graph and replay it (default),
  * 0 = launch the kernels one by one. */
 int cryo_set_graph_mode(cryo_ctx* ctx, int enable);

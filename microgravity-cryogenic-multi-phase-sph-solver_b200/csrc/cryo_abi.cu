@@ -34,6 +34,16 @@ struct CudaError : std::runtime_error {
 
 #define LAUNCH_CHECK() CK(cudaGetLastError())
 
+// Kernel launch inside a cryo_ctx member: counted, and bracketed by events
+// when profiling is on.
+#define LAUNCH(K, G, B, ...)                     \
+  do {                                           \
+    this->before_launch(#K);                     \
+    K<<<(G), (B), 0, this->stream>>>(__VA_ARGS__); \
+    LAUNCH_CHECK();                              \
+    this->after_launch();                        \
+  } while (0)
+
 struct Persist {
   float4 *xp = nullptr, *vT = nullptr, *vt = nullptr, *nrm = nullptr, *mrps = nullptr;
   uint32_t* id = nullptr;
@@ -129,7 +139,89 @@ struct cryo_ctx {
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool use_lists = true;
 
+  // launch accounting / profiling
+  long long launch_counter = 0;
+  int step_launches = 0;
+  bool profiling = false;
+  struct Mark { cudaEvent_t a, b; int kernel; };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+  size_t event_used = 0;
+  std::vector<std::string> prof_names;
+  std::vector<double> prof_ms;
+  std::vector<long long> prof_count;
+  int prof_current = -1;
+
+  // telemetry (TelemetryStream, telemetry.cu)
+  int tele_mode = 0;
+  size_t tele_cap = 0;
+  TelemetryRecord* tele_host = nullptr;
+  TelemetryRecord* tele_host_dev = nullptr;
+  TelemetryRecord* tele_stage = nullptr;
+  cudaStream_t tele_stream = nullptr;
+  cudaEvent_t tele_computed = nullptr, tele_landed = nullptr;
+  bool tele_pending = false;
+  double tele_time = 0;
+  long long tele_step = 0;
+  int tele_n = 0;
+
+  cudaEvent_t next_event() {
+    if (event_used == event_pool.size()) {
+      cudaEvent_t e;
+      CK(cudaEventCreate(&e));
+      event_pool.push_back(e);
+    }
+    return event_pool[event_used++];
+  }
+  void before_launch(const char* name) {
+    ++launch_counter;
+    if (!profiling) return;
+    int k = 0;
+    while (k < (int)prof_names.size() && prof_names[k] != name) ++k;
+    if (k == (int)prof_names.size()) {
+      prof_names.push_back(name);
+      prof_ms.push_back(0.0);
+      prof_count.push_back(0);
+    }
+    Mark m{next_event(), next_event(), k};
+    CK(cudaEventRecord(m.a, stream));
+    marks.push_back(m);
+  }
+  void after_launch() {
+    if (!profiling) return;
+    CK(cudaEventRecord(marks.back().b, stream));
+  }
+  void collect_marks() {
+    if (marks.empty()) return;
+    CK(cudaStreamSynchronize(stream));
+    for (const Mark& m : marks) {
+      float ms = 0;
+      CK(cudaEventElapsedTime(&ms, m.a, m.b));
+      prof_ms[m.kernel] += ms;
+      prof_count[m.kernel] += 1;
+    }
+    marks.clear();
+    event_used = 0;
+  }
+  void telemetry_release() {
+    if (tele_pending) {
+      cudaEventSynchronize(tele_mode == 1 ? tele_computed : tele_landed);
+      tele_pending = false;
+    }
+    if (tele_host) cudaFreeHost(tele_host);
+    if (tele_stage) cudaFree(tele_stage);
+    if (tele_stream) cudaStreamDestroy(tele_stream);
+    if (tele_computed) cudaEventDestroy(tele_computed);
+    if (tele_landed) cudaEventDestroy(tele_landed);
+    tele_host = tele_host_dev = tele_stage = nullptr;
+    tele_stream = nullptr;
+    tele_computed = tele_landed = nullptr;
+    tele_cap = 0;
+  }
+
   ~cryo_ctx() {
+    telemetry_release();
+    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (int k = 0; k < 2; ++k)
       if (graph[k]) cudaGraphExecDestroy(graph[k]);
     if (stream) cudaStreamSynchronize(stream);
@@ -432,8 +524,7 @@ void cryo_ctx::configure_grid(const float* lo, const float* hi) {
 // (SpatialHash::build, spatial_hash.cu:48-114).  Flips `cur`.
 void cryo_ctx::grid_build(int src) {
   const int G = grid_blocks();
-  k_keys<<<G, kBlock, 0, stream>>>(P, view(src), keys_a);
-  LAUNCH_CHECK();
+  LAUNCH(k_keys, G, kBlock, P, view(src), keys_a);
   sort_and_gather(src);
 }
 
@@ -446,12 +537,9 @@ void cryo_ctx::sort_and_gather(int src) {
   uint32_t* vout = vals_b;
   for (int shift = 0; shift < P.key_bits; shift += RS_BITS) {
     const int bits = std::min(RS_BITS, P.key_bits - shift);
-    k_rs_upsweep<<<tiles, RS_THREADS, 0, stream>>>(kin, shift, bits, dyn, hist);
-    LAUNCH_CHECK();
-    k_rs_scan<<<1, 1024, 0, stream>>>(hist, dyn);
-    LAUNCH_CHECK();
-    k_rs_downsweep<<<tiles, RS_THREADS, 0, stream>>>(kin, vin, kout, vout, shift, bits, dyn, hist);
-    LAUNCH_CHECK();
+    LAUNCH(k_rs_upsweep, tiles, RS_THREADS, kin, shift, bits, dyn, hist);
+    LAUNCH(k_rs_scan, 1, 1024, hist, dyn);
+    LAUNCH(k_rs_downsweep, tiles, RS_THREADS, kin, vin, kout, vout, shift, bits, dyn, hist);
     kin = kout;
     vin = vout;
     kout = (kout == keys_b) ? keys_a : keys_b;
@@ -459,10 +547,8 @@ void cryo_ctx::sort_and_gather(int src) {
   }
   sorted_keys = kin;
   sorted_perm = vin;
-  k_cells<<<G, kBlock, 0, stream>>>(P, kin, dyn, cell_begin);
-  LAUNCH_CHECK();
-  k_gather<<<G, kBlock, 0, stream>>>(view(src), view(1 - src), vin);
-  LAUNCH_CHECK();
+  LAUNCH(k_cells, G, kBlock, P, kin, dyn, cell_begin);
+  LAUNCH(k_gather, G, kBlock, view(src), view(1 - src), vin);
 }
 
 // Solver::evaluate_rates (sph_solver.cu:449-480) on set s.
@@ -470,77 +556,66 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset) {
   const int G = grid_blocks();
   const View V = view(s);
   if (maxima_reset) {
-    k_begin_step<<<1, 1, 0, stream>>>(P, V, BEGIN_RATES);
-    LAUNCH_CHECK();
+    LAUNCH(k_begin_step, 1, 1, P, V, BEGIN_RATES);
   }
-  k_density<<<G, kBlock, 0, stream>>>(P, V, 1);
-  LAUNCH_CHECK();
-  k_wall<<<G, kBlock, 0, stream>>>(P, V);
-  LAUNCH_CHECK();
-  k_interface<<<G, kBlock, 0, stream>>>(P, V, reduce(), P.thermal ? 1 : 0);
-  LAUNCH_CHECK();
+  LAUNCH(k_density, G, kBlock, P, V, 1);
+  LAUNCH(k_wall, G, kBlock, P, V);
+  LAUNCH(k_interface, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
   if (P.sps) {
-    k_sps<<<G, kBlock, 0, stream>>>(P, V);
-    LAUNCH_CHECK();
+    LAUNCH(k_sps, G, kBlock, P, V);
   }
   if (P.csf_active && P.csf_smooth) {
-    k_smooth_normals<<<G, kBlock, 0, stream>>>(P, V);
-    LAUNCH_CHECK();
+    LAUNCH(k_smooth_normals, G, kBlock, P, V);
   }
   int what = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
   if (P.csf_active) what |= FORCE_CSF;
   if (P.st_model == CRYO_ST_AKINCI) what |= FORCE_AKINCI;
   if (P.density_mode == CRYO_DENSITY_CONTINUITY) what |= FORCE_DRHO;
   if (P.thermal) what |= FORCE_THERMAL;
-  k_forces<<<G, kBlock, 0, stream>>>(P, V, what);
-  LAUNCH_CHECK();
+  LAUNCH(k_forces, G, kBlock, P, V, what);
 }
 
 // One Solver::step (sph_solver.cu:511-533) starting from set s; all device side.
 void cryo_ctx::enqueue_step(int s) {
   const int G = grid_blocks();
-  k_begin_step<<<1, 1, 0, stream>>>(P, view(s), BEGIN_STEP);
-  LAUNCH_CHECK();
-  k_kick_drift_keys<<<G, kBlock, 0, stream>>>(P, view(s), keys_a);
-  LAUNCH_CHECK();
+  LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
+  LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
   sort_and_gather(s);
   const int d = 1 - s;
   const View V = view(d);
   evaluate_rates(d, false);
-  k_kick<<<G, kBlock, 0, stream>>>(P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
-  LAUNCH_CHECK();
+  LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   if (P.shift_strength > 0.0f) {
-    k_shift_compute<<<G, kBlock, 0, stream>>>(P, V);
-    LAUNCH_CHECK();
-    k_shift_apply<<<G, kBlock, 0, stream>>>(P, V);
-    LAUNCH_CHECK();
+    LAUNCH(k_shift_compute, G, kBlock, P, V);
+    LAUNCH(k_shift_apply, G, kBlock, P, V);
   }
   if (P.cfg_phase_change) {
     const Reduce R = reduce();
-    k_pc_normalize<<<G, kBlock, 0, stream>>>(P, V, R, 1);
-    LAUNCH_CHECK();
-    k_pc_apply<<<G, kBlock, 0, stream>>>(P, V, 1);
-    LAUNCH_CHECK();
+    LAUNCH(k_pc_normalize, G, kBlock, P, V, R, 1);
+    LAUNCH(k_pc_apply, G, kBlock, P, V, 1);
     const bool reb = P.vapor_rebalance > 0.0f && has_vapor;
     if (reb) {
-      k_rebalance1<<<G, kBlock, 0, stream>>>(P, V, 1);
-      LAUNCH_CHECK();
+      LAUNCH(k_rebalance1, G, kBlock, P, V, 1);
     }
-    k_rebalance2_mark<<<G, kBlock, 0, stream>>>(P, V, R, split_flag, reb ? 1 : 0, 1);
-    LAUNCH_CHECK();
-    k_split<<<G, kBlock, 0, stream>>>(P, V, R, split_flag, 1);
-    LAUNCH_CHECK();
+    LAUNCH(k_rebalance2_mark, G, kBlock, P, V, R, split_flag, reb ? 1 : 0, 1);
+    LAUNCH(k_split, G, kBlock, P, V, R, split_flag, 1);
     if (cfg.thermo_mode == CRYO_THERMO_VENTED && has_vapor) {
-      k_venting<<<G, kBlock, 0, stream>>>(P, V, R, cfg.vent_relaxation, 1);
-      LAUNCH_CHECK();
+      LAUNCH(k_venting, G, kBlock, P, V, R, cfg.vent_relaxation, 1);
     }
   }
-  k_saturation<<<G, kBlock, 0, stream>>>(P, V, reduce(), 1);
-  LAUNCH_CHECK();
+  LAUNCH(k_saturation, G, kBlock, P, V, reduce(), 1);
 }
 
 void cryo_ctx::launch_step() {
   const int s = cur;
+  if (profiling) {
+    const long long c0 = launch_counter;
+    enqueue_step(s);
+    step_launches = (int)(launch_counter - c0);
+    collect_marks();
+    cur = 1 - s;
+    return;
+  }
   if (graph_mode) {
     if (!graph_valid[s]) {
       if (graph[s]) CK(cudaGraphExecDestroy(graph[s]));
@@ -548,7 +623,9 @@ void cryo_ctx::launch_step() {
       cudaGraph_t g = nullptr;
       CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       try {
+        const long long c0 = launch_counter;
         enqueue_step(s);
+        step_launches = (int)(launch_counter - c0);
       } catch (...) {
         cudaStreamEndCapture(stream, &g);
         if (g) cudaGraphDestroy(g);
@@ -561,7 +638,9 @@ void cryo_ctx::launch_step() {
     }
     CK(cudaGraphLaunch(graph[s], stream));
   } else {
+    const long long c0 = launch_counter;
     enqueue_step(s);
+    step_launches = (int)(launch_counter - c0);
   }
   cur = 1 - s;
 }
@@ -574,12 +653,10 @@ void cryo_ctx::ensure_initialized() {
   cur = 1 - cur;
   const int G = grid_blocks();
   if (cfg.normalize_initial_masses) {
-    k_normalize_masses<<<G, kBlock, 0, stream>>>(P, view(cur));
-    LAUNCH_CHECK();
+    LAUNCH(k_normalize_masses, G, kBlock, P, view(cur));
   }
   evaluate_rates(cur, true);
-  k_saturation<<<G, kBlock, 0, stream>>>(P, view(cur), reduce(), 0);
-  LAUNCH_CHECK();
+  LAUNCH(k_saturation, G, kBlock, P, view(cur), reduce(), 0);
   initialized = true;
 }
 
@@ -1556,6 +1633,142 @@ int cryo_load_state(cryo_ctx* c, const void* blob, size_t bytes) {
     c->has_vapor = h.has_vapor != 0;
     CK(cudaMemcpyAsync(c->cell_begin, p, cells, cudaMemcpyHostToDevice, c->stream));
     c->sync();
+  });
+}
+
+int cryo_set_profiling(cryo_ctx* c, int enable) {
+  return guard(c, [&] {
+    c->sync();
+    c->profiling = enable != 0;
+    c->prof_names.clear();
+    c->prof_ms.clear();
+    c->prof_count.clear();
+    c->marks.clear();
+    c->event_used = 0;
+  });
+}
+
+int cryo_kernel_times(cryo_ctx* c, int* count, char* names, double* total_ms, long long* launches) {
+  return guard(c, [&] {
+    const int k = (int)c->prof_names.size();
+    if (names) {
+      const int cap = *count;
+      for (int i = 0; i < k && i < cap; ++i) {
+        std::strncpy(names + 64 * i, c->prof_names[i].c_str(), 63);
+        names[64 * i + 63] = 0;
+        if (total_ms) total_ms[i] = c->prof_ms[i];
+        if (launches) launches[i] = c->prof_count[i];
+      }
+    }
+    *count = k;
+  });
+}
+
+int cryo_kernels_per_step(cryo_ctx* c, int* launches) {
+  return guard(c, [&] { *launches = c->step_launches; });
+}
+
+// TelemetryStream::configure (telemetry.cu:27-55)
+int cryo_telemetry_configure(cryo_ctx* c, int mode) {
+  return guard(c, [&] {
+    if (mode != 0 && mode != 1) throw std::invalid_argument("telemetry mode must be AsyncCopy (0) or ZeroCopy (1)");
+    c->sync();
+    c->telemetry_release();
+    c->tele_mode = mode;
+    const size_t cap = (size_t)std::max(c->capacity, 1);
+    const size_t bytes = cap * sizeof(TelemetryRecord);
+    if (mode == 1) {
+      if (cudaHostAlloc(&c->tele_host, bytes, cudaHostAllocMapped) == cudaSuccess &&
+          cudaHostGetDevicePointer(&c->tele_host_dev, c->tele_host, 0) == cudaSuccess) {
+      } else {
+        cudaGetLastError();
+        if (c->tele_host) cudaFreeHost(c->tele_host);
+        c->tele_host = c->tele_host_dev = nullptr;
+        c->tele_mode = 0;  // platform without mapped pinned memory
+      }
+    }
+    if (c->tele_mode == 0) {
+      CK(cudaHostAlloc(&c->tele_host, bytes, cudaHostAllocDefault));
+      CK(cudaMalloc(&c->tele_stage, bytes));
+      CK(cudaStreamCreateWithFlags(&c->tele_stream, cudaStreamNonBlocking));
+    }
+    CK(cudaEventCreateWithFlags(&c->tele_computed, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&c->tele_landed, cudaEventDisableTiming));
+    c->tele_cap = cap;
+  });
+}
+
+int cryo_telemetry_mode(cryo_ctx* c, int* mode) {
+  return guard(c, [&] { *mode = c->tele_mode; });
+}
+
+// TelemetryStream::request (telemetry.cu:57-96) + Solver::request_telemetry
+int cryo_telemetry_request(cryo_ctx* c, int* accepted) {
+  return guard(c, [&] {
+    *accepted = 0;
+    c->ensure_initialized();
+    c->pull();
+    const int n = c->hdyn->n;
+    if (!c->tele_host || (size_t)std::max(c->capacity, 1) != c->tele_cap) cryo_telemetry_configure(c, c->tele_mode);
+    if (c->tele_pending || (size_t)n > c->tele_cap) return;
+    TelemetryRecord* dst = c->tele_mode == 1 ? c->tele_host_dev : c->tele_stage;
+    k_telemetry_pack<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->view(c->cur), dst);
+    LAUNCH_CHECK();
+    CK(cudaEventRecord(c->tele_computed, c->stream));
+    if (c->tele_mode == 0) {
+      CK(cudaStreamWaitEvent(c->tele_stream, c->tele_computed, 0));
+      CK(cudaMemcpyAsync(c->tele_host, c->tele_stage, (size_t)n * sizeof(TelemetryRecord), cudaMemcpyDeviceToHost,
+                         c->tele_stream));
+      CK(cudaEventRecord(c->tele_landed, c->tele_stream));
+    }
+    c->tele_pending = true;
+    c->tele_time = c->hdyn->time;
+    c->tele_step = c->hdyn->step;
+    c->tele_n = n;
+    *accepted = 1;
+  });
+}
+
+int cryo_telemetry_ready(cryo_ctx* c, int* ready) {
+  return guard(c, [&] {
+    if (!c->tele_pending) {
+      *ready = 1;
+      return;
+    }
+    const cudaError_t st = cudaEventQuery(c->tele_mode == 1 ? c->tele_computed : c->tele_landed);
+    if (st == cudaSuccess) *ready = 1;
+    else if (st == cudaErrorNotReady) *ready = 0;
+    else CK(st);
+  });
+}
+
+int cryo_telemetry_pending(cryo_ctx* c, int* pending) {
+  return guard(c, [&] { *pending = c->tele_pending ? 1 : 0; });
+}
+
+// TelemetryStream::fetch (telemetry.cu:104-127)
+int cryo_telemetry_fetch(cryo_ctx* c, int* got, double* time, long long* step, int* n, float* position,
+                         float* temperature, float* pressure, float* speed, uint8_t* phase) {
+  return guard(c, [&] {
+    *got = 0;
+    if (!c->tele_pending) return;
+    *n = c->tele_n;
+    if (!position) return;
+    CK(cudaEventSynchronize(c->tele_mode == 1 ? c->tele_computed : c->tele_landed));
+    c->tele_pending = false;
+    *got = 1;
+    *time = c->tele_time;
+    *step = c->tele_step;
+    for (int i = 0; i < c->tele_n; ++i) {
+      const TelemetryRecord& r = c->tele_host[i];
+      position[3 * i] = r.x;
+      position[3 * i + 1] = r.y;
+      position[3 * i + 2] = r.z;
+      if (temperature) temperature[i] = r.T;
+      if (pressure) pressure[i] = r.p;
+      if (speed) speed[i] = r.speed;
+      if (phase) phase[i] = (uint8_t)r.phase;
+    }
   });
 }
 

@@ -243,4 +243,22 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
   }
 }
 
+// Telemetry record pack (telemetry.cu:70-84): x, T, p, |v|, phase.
+__global__ void __launch_bounds__(kBlock) k_telemetry_pack(View V, TelemetryRecord* __restrict__ out) {
+  const int n = V.dyn->n;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 xp = V.xp[i];
+    const float4 vT = V.vT[i];
+    TelemetryRecord r;
+    r.x = xp.x;
+    r.y = xp.y;
+    r.z = xp.z;
+    r.T = vT.w;
+    r.p = V.mrps[i].z;
+    r.speed = norm(xyz(vT));
+    r.phase = (uint32_t)ph_of(xp);
+    out[i] = r;
+  }
+}
+
 }  // namespace cryo

@@ -103,6 +103,13 @@ __global__ void k_maxima(Params P, View V);
 __global__ void k_saturation(Params P, View V, Reduce R, int end_of_step);
 __global__ void k_diagnostics(Params P, View V, Reduce R, double* out);
 
+// Packed per-particle telemetry record (telemetry.hpp:28-31).
+struct TelemetryRecord {
+  float x, y, z, T, p, speed;
+  uint32_t phase;
+};
+__global__ void k_telemetry_pack(View V, TelemetryRecord* out);
+
 // Number of FP64 values per chunk of the diagnostics reduction.
 constexpr int kDiagValues = 30;
 

@@ -1,0 +1,350 @@
+// solver.cpp -- cryosph::Solver over the C ABI.  Each method is one cryo_*
+// call; status codes come back as the reference's exception types
+// (CRYO_EINVAL -> std::invalid_argument, CRYO_ERANGE -> std::out_of_range,
+// otherwise std::runtime_error).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+
+#include "cryosph.hpp"
+
+namespace cryosph {
+
+namespace {
+void raise(int rc, const char* msg) {
+  const std::string m = msg ? msg : "";
+  switch (rc) {
+    case CRYO_OK: return;
+    case CRYO_EINVAL: throw std::invalid_argument(m);
+    case CRYO_ERANGE: throw std::out_of_range(m);
+    default: throw std::runtime_error(m);
+  }
+}
+void put3(float* d, Vec3 v) { d[0] = v.x; d[1] = v.y; d[2] = v.z; }
+Vec3 get3(const float* s) { return Vec3{s[0], s[1], s[2]}; }
+}  // namespace
+
+// ----------------------------------------------------------- fluids
+// fluid_properties.cpp:7-14
+real FluidProperties::saturation_temperature(real p) const {
+  const cryo_fluid_t f = to_c();
+  return cryo_saturation_temperature(&f, p);
+}
+real FluidProperties::saturation_pressure(real T) const {
+  const cryo_fluid_t f = to_c();
+  return cryo_saturation_pressure(&f, T);
+}
+cryo_fluid_t FluidProperties::to_c() const {
+  return cryo_fluid_t{rho_liquid, rho_vapor, mu_liquid, mu_vapor, k_liquid, k_vapor, cp_liquid,
+                      cp_vapor,   sigma,     h_fg,      T_sat,    p_sat,   R_gas};
+}
+namespace {
+FluidProperties preset(int which, const char* name) {
+  cryo_fluid_t f{};
+  raise(cryo_fluid_preset(which, &f), "unknown fluid preset");
+  FluidProperties p;
+  p.name = name;
+  p.rho_liquid = f.rho_liquid; p.rho_vapor = f.rho_vapor; p.mu_liquid = f.mu_liquid; p.mu_vapor = f.mu_vapor;
+  p.k_liquid = f.k_liquid; p.k_vapor = f.k_vapor; p.cp_liquid = f.cp_liquid; p.cp_vapor = f.cp_vapor;
+  p.sigma = f.sigma; p.h_fg = f.h_fg; p.T_sat = f.T_sat; p.p_sat = f.p_sat; p.R_gas = f.R_gas;
+  return p;
+}
+}  // namespace
+FluidProperties FluidProperties::liquid_hydrogen() { return preset(CRYO_FLUID_LH2, "LH2"); }
+FluidProperties FluidProperties::liquid_nitrogen() { return preset(CRYO_FLUID_LN2, "LN2"); }
+FluidProperties FluidProperties::liquid_oxygen() { return preset(CRYO_FLUID_LOX, "LOX"); }
+FluidProperties FluidProperties::liquid_methane() { return preset(CRYO_FLUID_LCH4, "LCH4"); }
+FluidProperties FluidProperties::water() { return preset(CRYO_FLUID_H2O, "H2O"); }
+
+cryo_config_t SolverConfig::to_c() const {
+  cryo_config_t c{};
+  c.dx = dx; c.h_factor = h_factor; c.kernel = static_cast<int>(kernel);
+  c.density_mode = static_cast<int>(density_mode); c.normalize_initial_masses = normalize_initial_masses;
+  put3(c.gravity, gravity);
+  c.velocity_scale = velocity_scale; c.sound_speed = sound_speed; c.tait_gamma = tait_gamma;
+  c.background_pressure = background_pressure; c.vapor_stiffness = vapor_stiffness;
+  c.clamp_negative_pressure = clamp_negative_pressure; c.transport_velocity = transport_velocity;
+  c.transport_background_factor = transport_background_factor; c.transport_stress = transport_stress;
+  c.transport_interface_only = transport_interface_only; c.particle_shifting = particle_shifting;
+  c.shifting_strength = shifting_strength; c.artificial_viscosity = artificial_viscosity;
+  c.artificial_viscosity_vapor = artificial_viscosity_vapor; c.delta_sph = delta_sph; c.no_slip = no_slip;
+  c.sps_turbulence = sps_turbulence; c.smagorinsky_cs = smagorinsky_cs;
+  c.surface_tension = static_cast<int>(surface_tension); c.contact_angle_deg = contact_angle_deg;
+  c.contact_angle_wall_weight = contact_angle_wall_weight; c.wall_colour = wall_colour;
+  c.wetting_model = static_cast<int>(wetting_model); c.csf_smooth_normals = csf_smooth_normals;
+  c.csf_balanced = csf_balanced; c.akinci_gamma = akinci_gamma; c.akinci_beta = akinci_beta;
+  c.thermal = thermal; c.phase_change = phase_change; c.wall_thermal_bc = static_cast<int>(wall_thermal_bc);
+  c.heater_power = heater_power; c.conductivity_scale = conductivity_scale; c.lee_evaporation = lee_evaporation;
+  c.lee_condensation = lee_condensation; c.thermo_mode = static_cast<int>(thermo_mode);
+  c.vent_relaxation = vent_relaxation; c.merge_ratio = merge_ratio; c.split_ratio = split_ratio;
+  c.max_transfer_fraction = max_transfer_fraction; c.phase_change_density_limit = phase_change_density_limit;
+  c.vapor_mass_rebalance = vapor_mass_rebalance; c.cfl = cfl; c.viscous_number = viscous_number;
+  c.force_number = force_number; c.capillary_number = capillary_number; c.thermal_number = thermal_number;
+  c.dt_max = dt_max; c.dt_min = dt_min; c.fixed_dt = fixed_dt;
+  return c;
+}
+
+// ------------------------------------------------------------ maneuver
+// ManeuverProfile::validate / evaluate (sph_solver.cu:234-268)
+void ManeuverProfile::validate() const {
+  if (time.empty()) throw std::invalid_argument("ManeuverProfile: empty time table");
+  if (acceleration.size() != time.size())
+    throw std::invalid_argument("ManeuverProfile: acceleration must have one entry per time");
+  if (!angular_velocity.empty() && angular_velocity.size() != time.size())
+    throw std::invalid_argument("ManeuverProfile: angular_velocity must be empty or have one entry per time");
+  for (std::size_t k = 1; k < time.size(); ++k)
+    if (!(time[k] > time[k - 1])) throw std::invalid_argument("ManeuverProfile: time must be strictly increasing");
+}
+void ManeuverProfile::evaluate(double t, Vec3& a, Vec3& omega, Vec3& omega_dot) const {
+  std::vector<float> acc(3 * time.size()), om;
+  for (std::size_t k = 0; k < time.size(); ++k) put3(acc.data() + 3 * k, acceleration[k]);
+  if (!angular_velocity.empty()) {
+    om.resize(3 * time.size());
+    for (std::size_t k = 0; k < time.size(); ++k) put3(om.data() + 3 * k, angular_velocity[k]);
+  }
+  float A[3], W[3], WD[3];
+  raise(cryo_maneuver_evaluate(static_cast<int>(time.size()), time.data(), acc.data(), om.empty() ? nullptr : om.data(),
+                               t, A, W, WD),
+        "ManeuverProfile: empty time table");
+  a = get3(A);
+  omega = get3(W);
+  omega_dot = get3(WD);
+}
+
+// -------------------------------------------------------------- solver
+Solver::Solver(const SolverConfig& config, const FluidProperties& fluid, int device) : cfg_(config), fluid_(fluid) {
+  const cryo_config_t c = cfg_.to_c();
+  const cryo_fluid_t f = fluid_.to_c();
+  const int rc = cryo_create(&c, &f, device, &ctx_);
+  if (rc) raise(rc, cryo_last_error(nullptr));
+}
+
+Solver::~Solver() { cryo_destroy(ctx_); }
+
+void Solver::check(int rc) const {
+  if (rc) raise(rc, cryo_last_error(ctx_));
+}
+
+void Solver::set_particles(const HostParticles& hp, const AABB& domain) {
+  const int n = static_cast<int>(hp.size());
+  std::vector<float> x(3 * hp.size()), v(3 * hp.size()), nrm(3 * hp.size());
+  for (std::size_t i = 0; i < hp.size(); ++i) {
+    put3(x.data() + 3 * i, hp.x[i]);
+    put3(v.data() + 3 * i, hp.v[i]);
+    put3(nrm.data() + 3 * i, hp.nrm[i]);
+  }
+  cryo_host_particles_t p{n, x.data(), v.data(), nrm.data(), hp.m.data(), hp.rho.data(), hp.T.data(),
+                          hp.phase.data(), hp.flags.data(), hp.id.data()};
+  float lo[3], hi[3];
+  put3(lo, domain.lo);
+  put3(hi, domain.hi);
+  check(cryo_set_particles(ctx_, &p, lo, hi));
+}
+
+// Solver::build_tank (sph_solver.cu:430-437)
+void Solver::build_tank(const Geometry& geometry, const FillSpec& fill) {
+  const HostParticles hp = build_tank_particles(geometry, fluid_, cfg_.dx, fill);
+  AABB dom = geometry.bounds();
+  const real pad = (fill.wall_layers + 1) * cfg_.dx;
+  dom.lo = dom.lo - Vec3{pad, pad, pad};
+  dom.hi = dom.hi + Vec3{pad, pad, pad};
+  set_particles(hp, dom);
+}
+
+void Solver::step() { check(cryo_step(ctx_)); }
+void Solver::run_steps(long long n) { check(cryo_run_steps(ctx_, n)); }
+void Solver::run_until(double t_end) { check(cryo_run_until(ctx_, t_end)); }
+
+double Solver::time() const {
+  double t, dt;
+  long long s;
+  check(cryo_time(ctx_, &t, &s, &dt));
+  return t;
+}
+long long Solver::step_count() const {
+  double t, dt;
+  long long s;
+  check(cryo_time(ctx_, &t, &s, &dt));
+  return s;
+}
+double Solver::last_dt() const {
+  double t, dt;
+  long long s;
+  check(cryo_time(ctx_, &t, &s, &dt));
+  return dt;
+}
+double Solver::next_dt() {
+  double dt = 0;
+  check(cryo_next_dt(ctx_, &dt));
+  return dt;
+}
+
+Diagnostics Solver::diagnostics() {
+  cryo_diagnostics_t d{};
+  check(cryo_diagnostics(ctx_, &d));
+  Diagnostics o;
+  o.time = d.time; o.step = d.step; o.dt = d.dt;
+  o.n_total = d.n_total; o.n_liquid = d.n_liquid; o.n_vapor = d.n_vapor; o.n_wall = d.n_wall;
+  o.mass_liquid = d.mass_liquid; o.mass_vapor = d.mass_vapor; o.mass_total = d.mass_total;
+  o.kinetic_energy = d.kinetic_energy; o.enthalpy = d.enthalpy; o.heat_input = d.heat_input;
+  o.evaporated_mass = d.evaporated_mass; o.condensed_mass = d.condensed_mass;
+  o.vented_mass = d.vented_mass; o.vented_enthalpy = d.vented_enthalpy;
+  o.T_sat = d.T_sat; o.p_ullage = d.p_ullage; o.max_speed = d.max_speed;
+  o.T_liquid_mean = d.T_liquid_mean; o.T_liquid_max = d.T_liquid_max; o.T_vapor_mean = d.T_vapor_mean;
+  o.liquid_com = get3(d.liquid_com); o.liquid_momentum = get3(d.liquid_momentum);
+  o.splits = d.splits; o.merges = d.merges;
+  o.slosh_force = get3(d.slosh_force); o.slosh_moment = get3(d.slosh_moment);
+  o.frame_acceleration = get3(d.frame_acceleration); o.frame_angular_velocity = get3(d.frame_angular_velocity);
+  return o;
+}
+
+HostParticles Solver::particles() const {
+  const std::size_t n = num_particles();
+  HostParticles h;
+  std::vector<float> x(3 * n), v(3 * n), nrm(3 * n);
+  h.m.resize(n); h.rho.resize(n); h.T.resize(n); h.phase.resize(n); h.flags.resize(n); h.id.resize(n);
+  cryo_host_particles_out_t o{static_cast<int>(n), x.data(), v.data(), nrm.data(), h.m.data(), h.rho.data(),
+                              h.T.data(), h.phase.data(), h.flags.data(), h.id.data()};
+  check(cryo_download(ctx_, &o));
+  h.x.resize(n); h.v.resize(n); h.nrm.resize(n);
+  for (std::size_t i = 0; i < n; ++i) {
+    h.x[i] = get3(x.data() + 3 * i);
+    h.v[i] = get3(v.data() + 3 * i);
+    h.nrm[i] = get3(nrm.data() + 3 * i);
+  }
+  return h;
+}
+
+std::vector<real> Solver::field(int f) const {
+  const std::size_t n = num_particles();
+  const bool vec = f == CRYO_F_X || f == CRYO_F_V || f == CRYO_F_VT || f == CRYO_F_NRM || f == CRYO_F_A ||
+                   f == CRYO_F_AB || f == CRYO_F_FW || f == CRYO_F_MW || f == CRYO_F_NS || f == CRYO_F_VW;
+  std::vector<real> out(vec ? 3 * n : n);
+  check(cryo_get_field(ctx_, f, out.data(), out.size() * sizeof(real)));
+  return out;
+}
+std::vector<real> Solver::pressure() const { return field(CRYO_F_P); }
+std::vector<real> Solver::curvature() const { return field(CRYO_F_KAPPA); }
+
+std::size_t Solver::num_particles() const {
+  int n = 0;
+  check(cryo_num_particles(ctx_, &n));
+  return static_cast<std::size_t>(n);
+}
+
+void Solver::set_gravity(Vec3 g) {
+  cfg_.gravity = g;
+  float a[3];
+  put3(a, g);
+  check(cryo_set_gravity(ctx_, a));
+}
+void Solver::set_frame_motion(Vec3 acceleration, Vec3 angular_velocity, Vec3 angular_acceleration, Vec3 origin) {
+  float a[3], w[3], wd[3], o[3];
+  put3(a, acceleration); put3(w, angular_velocity); put3(wd, angular_acceleration); put3(o, origin);
+  check(cryo_set_frame_motion(ctx_, a, w, wd, o));
+}
+void Solver::set_maneuver(const ManeuverProfile& p) {
+  p.validate();
+  std::vector<float> acc(3 * p.time.size()), om;
+  for (std::size_t k = 0; k < p.time.size(); ++k) put3(acc.data() + 3 * k, p.acceleration[k]);
+  if (!p.angular_velocity.empty()) {
+    om.resize(3 * p.time.size());
+    for (std::size_t k = 0; k < p.time.size(); ++k) put3(om.data() + 3 * k, p.angular_velocity[k]);
+  }
+  float o[3];
+  put3(o, p.origin);
+  check(cryo_set_maneuver(ctx_, static_cast<int>(p.time.size()), p.time.data(), acc.data(),
+                          om.empty() ? nullptr : om.data(), o));
+}
+void Solver::clear_frame_motion() { check(cryo_clear_frame_motion(ctx_)); }
+void Solver::set_heater_power(real watts) {
+  cfg_.heater_power = watts;
+  check(cryo_set_heater_power(ctx_, watts));
+}
+void Solver::set_contact_angle(real degrees) {
+  check(cryo_set_contact_angle(ctx_, degrees));
+  cfg_.contact_angle_deg = degrees;
+}
+void Solver::damp_velocities(real factor) { check(cryo_damp_velocities(ctx_, factor)); }
+void Solver::relax(double duration, real damping) { check(cryo_relax(ctx_, duration, damping)); }
+
+real Solver::sound_speed() const {
+  float c = 0;
+  check(cryo_sound_speed(ctx_, &c));
+  return c;
+}
+real Solver::smoothing_length() const {
+  float h = 0;
+  check(cryo_smoothing_length(ctx_, &h));
+  return h;
+}
+std::string Solver::device() const { return device_name(0); }
+
+void Solver::configure_telemetry(TelemetryMode mode) { check(cryo_telemetry_configure(ctx_, static_cast<int>(mode))); }
+TelemetryMode Solver::telemetry_mode() const {
+  int m = 0;
+  check(cryo_telemetry_mode(ctx_, &m));
+  return static_cast<TelemetryMode>(m);
+}
+bool Solver::request_telemetry() {
+  int ok = 0;
+  check(cryo_telemetry_request(ctx_, &ok));
+  return ok != 0;
+}
+bool Solver::telemetry_ready() const {
+  int r = 0;
+  check(cryo_telemetry_ready(ctx_, &r));
+  return r != 0;
+}
+bool Solver::telemetry_pending() const {
+  int p = 0;
+  check(cryo_telemetry_pending(ctx_, &p));
+  return p != 0;
+}
+bool Solver::fetch_telemetry(TelemetryFrame& f) {
+  int got = 0, n = 0;
+  double t = 0;
+  long long s = 0;
+  check(cryo_telemetry_fetch(ctx_, &got, &t, &s, &n, nullptr, nullptr, nullptr, nullptr, nullptr));
+  if (n == 0 && !telemetry_pending()) return false;
+  f.position.resize(3 * static_cast<std::size_t>(n));
+  f.temperature.resize(n); f.pressure.resize(n); f.speed.resize(n); f.phase.resize(n);
+  check(cryo_telemetry_fetch(ctx_, &got, &t, &s, &n, f.position.data(), f.temperature.data(), f.pressure.data(),
+                             f.speed.data(), f.phase.data()));
+  if (!got) return false;
+  f.time = t;
+  f.step = s;
+  f.n = n;
+  return true;
+}
+
+std::vector<real> Solver::probe_pressure(const std::vector<Vec3>& points) {
+  std::vector<float> p(3 * points.size()), out(points.size());
+  for (std::size_t k = 0; k < points.size(); ++k) put3(p.data() + 3 * k, points[k]);
+  if (!points.empty()) check(cryo_probe_pressure(ctx_, p.data(), static_cast<int>(points.size()), out.data()));
+  return out;
+}
+
+std::uintptr_t Solver::stream_handle() const { return cryo_stream(ctx_); }
+void Solver::set_graph_mode(bool on) { check(cryo_set_graph_mode(ctx_, on ? 1 : 0)); }
+
+std::vector<std::uint8_t> Solver::save_state() const {
+  std::size_t bytes = 0;
+  check(cryo_state_size(ctx_, &bytes));
+  std::vector<std::uint8_t> blob(bytes);
+  check(cryo_save_state(ctx_, blob.data(), blob.size()));
+  return blob;
+}
+void Solver::load_state(const std::vector<std::uint8_t>& blob) {
+  check(cryo_load_state(ctx_, blob.data(), blob.size()));
+}
+
+std::string device_name(int device) {
+  char buf[256] = {0};
+  if (cryo_device_name(device, buf, sizeof(buf)) != CRYO_OK) return "no CUDA device";
+  return buf;
+}
+int device_count() { return cryo_device_count(); }
+
+}  // namespace cryosph
