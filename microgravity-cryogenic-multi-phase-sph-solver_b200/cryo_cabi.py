@@ -357,6 +357,14 @@ class Context:
         a = np.ascontiguousarray(data, dtype=field_dtype(name)).reshape(field_shape(name, n))
         self.check(self.L.cryo_set_field(self.h, FIELD_ID[name], a.ctypes.data_as(C.c_void_p), a.nbytes))
 
+    def set_neighbor_mode(self, use_lists):
+        self.check(self.L.cryo_set_neighbor_mode(self.h, int(bool(use_lists))))
+
+    def device_status(self):
+        st = C.c_uint()
+        self.check(self.L.cryo_device_status(self.h, C.byref(st)))
+        return st.value
+
     def set_graph_mode(self, on):
         self.check(self.L.cryo_set_graph_mode(self.h, int(bool(on))))
 

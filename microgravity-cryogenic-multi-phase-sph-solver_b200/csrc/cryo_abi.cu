@@ -75,10 +75,11 @@ size_t particle_bytes(size_t cap) {
   t += 7 * r(cap * 16) + 4 * r(cap * 4);                            // scratch
   t += 5 * r(cap * 4);                                              // sort keys/vals, split flags
   const size_t tiles = (cap + RS_TILE - 1) / RS_TILE + 1;
-  t += r(tiles * RS_BINS * 4);                                      // radix histogram
+  t += r((tiles + 1) * RS_BINS * 4);                                // radix histogram + digit totals
   const size_t chunks = cap / kChunk + 2;
   t += r(chunks * 32 * 8);                                          // reduction partials
   t += r(64 * 8) + r(64);                                           // diagnostics out, tickets
+  t += r(cap * 4 * (size_t)kMaxNbr) + 3 * r(cap * 4);              // neighbour lists, counts, phase lists
   return t;
 }
 
@@ -103,6 +104,7 @@ struct cryo_ctx {
   float *rmin = nullptr, *wall_w = nullptr, *heat_w = nullptr, *nu_t = nullptr;
   uint32_t *keys_a = nullptr, *keys_b = nullptr, *vals_a = nullptr, *vals_b = nullptr, *split_flag = nullptr;
   uint32_t* hist = nullptr;
+  int *nbr = nullptr, *nbr_cnt = nullptr, *fluid_idx = nullptr, *wall_idx = nullptr;
   double* partials = nullptr;
   int max_chunks = 0;
   double* diag_out = nullptr;
@@ -173,9 +175,13 @@ struct cryo_ctx {
     }
     return event_pool[event_used++];
   }
-  void before_launch(const char* name) {
+  void before_launch(const char* raw) {
     ++launch_counter;
     if (!profiling) return;
+    std::string name(raw);
+    const size_t lt = name.find('<');
+    if (lt != std::string::npos) name = name.substr(0, lt);
+    if (name == "k_forces_t") name = "k_forces";
     int k = 0;
     while (k < (int)prof_names.size() && prof_names[k] != name) ++k;
     if (k == (int)prof_names.size()) {
@@ -248,6 +254,10 @@ struct cryo_ctx {
     V.partials = partials;
     V.counters = ticket;
     V.capacity = capacity;
+    V.nbr = nbr;
+    V.nbr_cnt = nbr_cnt;
+    V.fluid_idx = fluid_idx;
+    V.wall_idx = wall_idx;
     return V;
   }
   Reduce reduce() const { return Reduce{partials, ticket, max_chunks}; }
@@ -294,11 +304,15 @@ struct cryo_ctx {
     uint32_t* nva = a.take<uint32_t>(cap); uint32_t* nvb = a.take<uint32_t>(cap);
     uint32_t* nsf = a.take<uint32_t>(cap);
     const size_t tiles = (size_t)(cap + RS_TILE - 1) / RS_TILE + 1;
-    uint32_t* nhist = a.take<uint32_t>(tiles * RS_BINS);
+    uint32_t* nhist = a.take<uint32_t>(tiles * RS_BINS + RS_BINS);
     const int nchunks = cap / kChunk + 2;
     double* npart = a.take<double>((size_t)nchunks * 32);
     double* ndiag = a.take<double>(64);
     unsigned* ntick = a.take<unsigned>(64);
+    int* nnbr = a.take<int>((size_t)cap * kMaxNbr);
+    int* nnc = a.take<int>(cap);
+    int* nfi = a.take<int>(cap);
+    int* nwi = a.take<int>(cap);
     if (a.used > a.size) throw std::runtime_error("internal: arena overflow");
     // keep the first n particles of every array (ParticleSystem::grow,
     // particle_system.cpp:66-71)
@@ -323,6 +337,7 @@ struct cryo_ctx {
     rmin = nrmin; wall_w = nwall; heat_w = nheat; nu_t = nnut;
     keys_a = nka; keys_b = nkb; vals_a = nva; vals_b = nvb; split_flag = nsf;
     hist = nhist; partials = npart; max_chunks = nchunks; diag_out = ndiag; ticket = ntick;
+    nbr = nnbr; nbr_cnt = nnc; fluid_idx = nfi; wall_idx = nwi;
     sorted_keys = nullptr;
     sorted_perm = nullptr;
     capacity = cap;
@@ -338,9 +353,9 @@ struct cryo_ctx {
   void configure_grid(const float* lo, const float* hi);
 
   // ------------------------------------------------------ step pieces
-  void grid_build(int src);               // keys of current positions, sort, cells, gather
-  void sort_and_gather(int src);          // after keys_a holds the keys
-  void evaluate_rates(int s, bool maxima_reset);
+  void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
+  void sort_and_gather(int src, int list_mode);  // after keys_a holds the keys
+  void evaluate_rates(int s, bool maxima_reset, bool density_done);
   void enqueue_step(int s);
   void launch_step();
   void ensure_initialized();
@@ -491,6 +506,7 @@ void cryo_ctx::init_params() {
   p.f_p_sat = fluid.p_sat;
   p.f_R_gas = fluid.R_gas;
   p.f_h_fg = fluid.h_fg;
+  p.use_lists = use_lists ? 1 : 0;
 }
 
 // SpatialHash::configure (spatial_hash.cu:15-30) + view() (:36-46)
@@ -525,10 +541,12 @@ void cryo_ctx::configure_grid(const float* lo, const float* hi) {
 void cryo_ctx::grid_build(int src) {
   const int G = grid_blocks();
   LAUNCH(k_keys, G, kBlock, P, view(src), keys_a);
-  sort_and_gather(src);
+  sort_and_gather(src, LISTS_PHASE);
 }
 
-void cryo_ctx::sort_and_gather(int src) {
+// Radix sort of keys_a, cell table, reorder gather into the other set and
+// (with lists on) the neighbour / phase lists of the new order.
+void cryo_ctx::sort_and_gather(int src, int list_mode) {
   const int G = grid_blocks();
   const int tiles = (capacity + RS_TILE - 1) / RS_TILE;
   const uint32_t* kin = keys_a;
@@ -538,7 +556,7 @@ void cryo_ctx::sort_and_gather(int src) {
   for (int shift = 0; shift < P.key_bits; shift += RS_BITS) {
     const int bits = std::min(RS_BITS, P.key_bits - shift);
     LAUNCH(k_rs_upsweep, tiles, RS_THREADS, kin, shift, bits, dyn, hist);
-    LAUNCH(k_rs_scan, 1, 1024, hist, dyn);
+    LAUNCH(k_rs_scan, RS_BINS, RS_SCAN_THREADS, hist, dyn);
     LAUNCH(k_rs_downsweep, tiles, RS_THREADS, kin, vin, kout, vout, shift, bits, dyn, hist);
     kin = kout;
     vin = vout;
@@ -548,31 +566,44 @@ void cryo_ctx::sort_and_gather(int src) {
   sorted_keys = kin;
   sorted_perm = vin;
   LAUNCH(k_cells, G, kBlock, P, kin, dyn, cell_begin);
-  LAUNCH(k_gather, G, kBlock, view(src), view(1 - src), vin);
+  LAUNCH(k_gather, G, kBlock, view(src), view(1 - src), vin, reduce());
+  if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
 }
 
-// Solver::evaluate_rates (sph_solver.cu:449-480) on set s.
-void cryo_ctx::evaluate_rates(int s, bool maxima_reset) {
+// Solver::evaluate_rates (sph_solver.cu:449-480) on set s.  density_done:
+// the density/EOS pass already ran inside the list build.
+void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
   const int G = grid_blocks();
   const View V = view(s);
-  if (maxima_reset) {
-    LAUNCH(k_begin_step, 1, 1, P, V, BEGIN_RATES);
-  }
-  LAUNCH(k_density, G, kBlock, P, V, 1);
+  if (maxima_reset) LAUNCH(k_begin_step, 1, 1, P, V, BEGIN_RATES);
+  if (!density_done) LAUNCH(k_density, G, kBlock, P, V, 1);
   LAUNCH(k_wall, G, kBlock, P, V);
   LAUNCH(k_interface, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
-  if (P.sps) {
-    LAUNCH(k_sps, G, kBlock, P, V);
-  }
-  if (P.csf_active && P.csf_smooth) {
-    LAUNCH(k_smooth_normals, G, kBlock, P, V);
-  }
+  if (P.sps) LAUNCH(k_sps, G, kBlock, P, V);
+  if (P.csf_active && P.csf_smooth) LAUNCH(k_smooth_normals, G, kBlock, P, V);
   int what = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
   if (P.csf_active) what |= FORCE_CSF;
   if (P.st_model == CRYO_ST_AKINCI) what |= FORCE_AKINCI;
   if (P.density_mode == CRYO_DENSITY_CONTINUITY) what |= FORCE_DRHO;
   if (P.thermal) what |= FORCE_THERMAL;
-  LAUNCH(k_forces, G, kBlock, P, V, what);
+  switch (what) {
+#define FORCES_CASE(W) \
+  case W: LAUNCH(k_forces_t<W>, G, kBlock, P, V, W); break;
+    FORCES_CASE(FORCE_BASE)
+    FORCES_CASE(FORCE_BASE | FORCE_THERMAL)
+    FORCES_CASE(FORCE_BASE | FORCE_DRHO)
+    FORCES_CASE(FORCE_BASE | FORCE_DRHO | FORCE_THERMAL)
+    FORCES_CASE(FORCE_BASE | FORCE_AKINCI)
+    FORCES_CASE(FORCE_BASE | FORCE_AKINCI | FORCE_THERMAL)
+    FORCES_CASE(FORCE_BASE | FORCE_AKINCI | FORCE_DRHO)
+    FORCES_CASE(FORCE_BASE | FORCE_AKINCI | FORCE_DRHO | FORCE_THERMAL)
+    FORCES_CASE(FORCE_BASE | FORCE_CSF)
+    FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_THERMAL)
+    FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO)
+    FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO | FORCE_THERMAL)
+#undef FORCES_CASE
+    default: LAUNCH(k_forces_t<-1>, G, kBlock, P, V, what);
+  }
 }
 
 // One Solver::step (sph_solver.cu:511-533) starting from set s; all device side.
@@ -580,14 +611,17 @@ void cryo_ctx::enqueue_step(int s) {
   const int G = grid_blocks();
   LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
   LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
-  sort_and_gather(s);
+  sort_and_gather(s, LISTS_DENSITY);
   const int d = 1 - s;
   const View V = view(d);
-  evaluate_rates(d, false);
+  evaluate_rates(d, false, P.use_lists != 0);
   LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   if (P.shift_strength > 0.0f) {
     LAUNCH(k_shift_compute, G, kBlock, P, V);
     LAUNCH(k_shift_apply, G, kBlock, P, V);
+    // the phase-change passes search around the shifted positions
+    // (old cell table), as for_each_neighbor does in the reference
+    if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, V, reduce(), LISTS_ONLY);
   }
   if (P.cfg_phase_change) {
     const Reduce R = reduce();
@@ -655,7 +689,7 @@ void cryo_ctx::ensure_initialized() {
   if (cfg.normalize_initial_masses) {
     LAUNCH(k_normalize_masses, G, kBlock, P, view(cur));
   }
-  evaluate_rates(cur, true);
+  evaluate_rates(cur, true, false);
   LAUNCH(k_saturation, G, kBlock, P, view(cur), reduce(), 0);
   initialized = true;
 }
@@ -1046,7 +1080,7 @@ int cryo_relax(cryo_ctx* c, double duration, float damping) {
     d.heat_input = d.evaporated = d.condensed = d.vented = d.vented_h = 0;
     d.splits = d.merges = 0;
     c->push();
-    c->evaluate_rates(c->cur, true);
+    c->evaluate_rates(c->cur, true, false);
     k_saturation<<<G, kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), 0);
     LAUNCH_CHECK();
     c->sync();
@@ -1429,17 +1463,17 @@ int cryo_pass(cryo_ctx* c, int pass) {
       case CRYO_PASS_EOS: k_eos<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_WALL_BOUNDARY: k_wall<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_INTERFACE: k_interface<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
-      case CRYO_PASS_TRANSPORT: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_TRANSPORT); break;
+      case CRYO_PASS_TRANSPORT: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_TRANSPORT); break;
       case CRYO_PASS_SPS: k_sps<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_MOMENTUM: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_MOMENTUM); break;
+      case CRYO_PASS_MOMENTUM: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_MOMENTUM); break;
       case CRYO_PASS_SMOOTH_NORMALS: k_smooth_normals<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_CSF: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_CSF); break;
-      case CRYO_PASS_AKINCI: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_AKINCI); break;
-      case CRYO_PASS_DENSITY_RATE: k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_DRHO); break;
+      case CRYO_PASS_CSF: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_CSF); break;
+      case CRYO_PASS_AKINCI: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_AKINCI); break;
+      case CRYO_PASS_DENSITY_RATE: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_DRHO); break;
       case CRYO_PASS_THERMAL:
         k_heat_norm<<<G, kBlock, 0, st>>>(P, V, R);
         LAUNCH_CHECK();
-        k_forces<<<G, kBlock, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
+        k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
         break;
       case CRYO_PASS_MAXIMA:
         k_begin_step<<<1, 1, 0, st>>>(P, V, BEGIN_RATES);
@@ -1451,6 +1485,8 @@ int cryo_pass(cryo_ctx* c, int pass) {
         k_shift_compute<<<G, kBlock, 0, st>>>(P, V);
         LAUNCH_CHECK();
         k_shift_apply<<<G, kBlock, 0, st>>>(P, V);
+        LAUNCH_CHECK();
+        if (P.use_lists) k_build_lists<<<G, kBlock, 0, st>>>(P, V, R, LISTS_ONLY);
         break;
       case CRYO_PASS_PC_SOURCES: k_pc_sources<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_PC_NORMALIZE: k_pc_normalize<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
@@ -1781,7 +1817,12 @@ int cryo_set_graph_mode(cryo_ctx* c, int enable) {
 }
 
 int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {
-  return guard(c, [&] { c->use_lists = use_lists != 0; });
+  return guard(c, [&] {
+    c->sync();
+    c->use_lists = use_lists != 0;
+    c->P.use_lists = c->use_lists ? 1 : 0;
+    c->invalidate_graphs();
+  });
 }
 
 }  // extern "C"

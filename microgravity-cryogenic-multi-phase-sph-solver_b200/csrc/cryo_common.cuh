@@ -114,7 +114,13 @@ struct Params {
   // grid
   float ox, oy, oz, inv_cell, cell;
   int nx, ny, nz, num_cells, key_bits;
+  // neighbour lists (0: every pass scans the 27 cells)
+  int use_lists;
 };
+
+// Capacity of the per-particle neighbour list; a particle with more
+// in-support neighbours falls back to the 27-cell scan.
+constexpr int kMaxNbr = 128;
 
 // Device-resident scalar block: everything the host used to keep between
 // kernel launches (dt, frame state, maxima, FP64 bookkeeping, counts).
@@ -140,6 +146,7 @@ struct DynState {
   // cumulative bookkeeping
   double evaporated, condensed, vented, vented_h;
   int merges, splits;
+  int n_fluid_list, n_wall_list;  // lengths of the phase index lists
   unsigned status;    // CRYO_DEV_* guard bits
   int split_requested;
   // relax / damping applied after the step (0 = none)
@@ -194,6 +201,13 @@ struct View {
   double* partials;   // per-chunk FP64 partials
   unsigned* counters; // last-block tickets
   int capacity;
+  // neighbour lists: nbr[k * capacity + i] = k-th in-support neighbour of i
+  // (reference iteration order), nbr_cnt[i] = count (> kMaxNbr: overflow)
+  int* nbr;
+  int* nbr_cnt;
+  // ordered phase index lists (built after each reorder)
+  int* fluid_idx;
+  int* wall_idx;
 };
 
 // --------------------------------------------------------- SPH kernels
@@ -317,6 +331,41 @@ __device__ inline void for_each_neighbor(const Params& P, const int* __restrict_
       }
     }
   }
+}
+
+// Neighbour iteration of particle i through its list (same j order and the
+// same r2 bits as for_each_neighbor); falls back to the scan on overflow or
+// when lists are off.
+template <class F>
+__device__ inline void for_each_nbr(const Params& P, const View& V, int i, V3 xi, F&& f) {
+  const int c = P.use_lists ? __ldg(V.nbr_cnt + i) : kMaxNbr + 1;
+  if (c <= kMaxNbr) {
+    const int* __restrict__ list = V.nbr + i;
+    const size_t stride = (size_t)V.capacity;
+    for (int k = 0; k < c; ++k) {
+      const int j = __ldg(list + (size_t)k * stride);
+      const float4 xj = __ldg(V.xp + j);
+      const V3 rij = xi - xyz(xj);
+      const float r2 = norm2(rij);
+      f(j, xj, rij, r2);
+    }
+  } else {
+    for_each_neighbor(P, V.cell_begin, V.xp, xi, f);
+  }
+}
+
+// The particles a pass visits: with lists, an ordered phase index list
+// (fluid or wall); otherwise every particle (the pass filters by phase).
+struct Range {
+  const int* idx;
+  int count;
+};
+__device__ inline int particle_at(const Range& r, int t) { return r.idx ? __ldg(r.idx + t) : t; }
+__device__ inline Range fluid_range(const Params& P, const View& V) {
+  return P.use_lists ? Range{V.fluid_idx, V.dyn->n_fluid_list} : Range{nullptr, V.dyn->n};
+}
+__device__ inline Range wall_range(const Params& P, const View& V) {
+  return P.use_lists ? Range{V.wall_idx, V.dyn->n_wall_list} : Range{nullptr, V.dyn->n};
 }
 
 // Same iteration, every candidate (no distance filter); for passes whose

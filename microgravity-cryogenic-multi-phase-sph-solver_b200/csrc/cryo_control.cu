@@ -114,12 +114,16 @@ __global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce 
     }
   }
   const bool last = closed ? last_block(R.ticket) : (blockIdx.x == 0);
-  if (!last || threadIdx.x != 0) return;
+  if (!last) return;
+  double m_liq = 0, m_vap = 0, mT_vap = 0;
+  if (closed) {
+    m_liq = block_sum_partials(R, 0, nch);
+    m_vap = block_sum_partials(R, 1, nch);
+    mT_vap = block_sum_partials(R, 2, nch);
+  }
+  if (threadIdx.x != 0) return;
   bool done = false;
   if (closed) {
-    const double m_liq = sum_partials(R, 0, nch);
-    const double m_vap = sum_partials(R, 1, nch);
-    const double mT_vap = sum_partials(R, 2, nch);
     if (!(d->fluid_volume0 > 0)) d->fluid_volume0 = m_liq / P.f_rho_l + m_vap / P.f_rho_v;
     const double v_ullage = d->fluid_volume0 - m_liq / P.f_rho_l;
     const double ratio = v_ullage > 0 && m_vap > 0 ? (mT_vap / v_ullage) / ((double)P.f_rho_v * P.f_T_sat) : 0.0;
@@ -156,9 +160,10 @@ __global__ void __launch_bounds__(kBlock) k_heat_norm(Params P, View V, Reduce R
     if (i < n && is_fluid(ph_of(V.xp[i]))) s[0] = (double)V.heat_w[i];
     publish_chunk<1>(R, c, s, sh);
   }
-  if (last_block(R.ticket) && threadIdx.x == 0) {
+  if (last_block(R.ticket)) {
+    const double S = block_sum_partials(R, 0, nch);
+    if (threadIdx.x != 0) return;
     if (P.heat_power != 0.0f) {
-      const double S = sum_partials(R, 0, nch);
       d->heat_inv_norm = S > 0 ? (float)(1.0 / S) : 0.0f;
     } else {
       d->heat_inv_norm = 0.0f;
@@ -230,15 +235,23 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
     __syncthreads();
   }
   if (last_block(R.ticket)) {
-    // 25 values: one thread each
-    const int v = threadIdx.x;
-    if (v < 23) {
-      out[v] = sum_partials(R, v, nch);
-    } else if (v < 25) {
-      double mx = 0.0;
+    for (int v = 0; v < 23; ++v) {
+      const double s = block_sum_partials(R, v, nch);
+      if (threadIdx.x == 0) out[v] = s;
+    }
+    __shared__ float wm[2][kBlock / 32];
+    for (int v = 23; v < 25; ++v) {
+      float mx = 0.0f;
       const double* p = R.partials + (size_t)v * R.max_chunks;
-      for (int k = 0; k < nch; ++k) mx = fmax(mx, __ldcg(p + k));
-      out[v] = mx;
+      for (int k = threadIdx.x; k < nch; k += blockDim.x) mx = fmaxf(mx, (float)__ldcg(p + k));
+      mx = warp_max(mx);
+      if ((threadIdx.x & 31) == 0) wm[v - 23][threadIdx.x >> 5] = mx;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2) {
+      float mx = 0.0f;
+      for (int w = 0; w < kBlock / 32; ++w) mx = fmaxf(mx, wm[threadIdx.x][w]);
+      out[23 + threadIdx.x] = mx;
     }
   }
 }

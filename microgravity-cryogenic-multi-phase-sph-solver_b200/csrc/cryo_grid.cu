@@ -43,15 +43,19 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_upsweep(const uint32_t* __res
   for (int d = threadIdx.x; d < RS_BINS; d += blockDim.x) hist[d * nt + b] = cnt[d];
 }
 
-// Exclusive scan of hist[RS_BINS * nt] in place (one block).
-__global__ void __launch_bounds__(1024) k_rs_scan(uint32_t* __restrict__ hist, const DynState* __restrict__ dyn) {
+// Per digit (one block each): exclusive scan of the tile counts hist[d][*]
+// in place and the digit total in hist_tot[d].  The downsweep adds the
+// exclusive prefix of the digit totals.
+__global__ void __launch_bounds__(RS_SCAN_THREADS) k_rs_scan(uint32_t* __restrict__ hist,
+                                                              const DynState* __restrict__ dyn) {
   const int n = dyn->n;
   const int nt = (n + RS_TILE - 1) / RS_TILE;
-  const int total = RS_BINS * nt;
-  const int per = (total + blockDim.x - 1) / blockDim.x;
-  const int lo = threadIdx.x * per, hi = min(lo + per, total);
+  const int d = blockIdx.x;
+  uint32_t* row = hist + (size_t)d * nt;
+  const int per = (nt + blockDim.x - 1) / blockDim.x;
+  const int lo = threadIdx.x * per, hi = min(lo + per, nt);
   uint32_t s = 0;
-  for (int k = lo; k < hi; ++k) s += hist[k];
+  for (int k = lo; k < hi; ++k) s += row[k];
   __shared__ uint32_t warp_tot[32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   uint32_t incl = s;
@@ -72,10 +76,11 @@ __global__ void __launch_bounds__(1024) k_rs_scan(uint32_t* __restrict__ hist, c
   __syncthreads();
   uint32_t run = (incl - s) + (warp > 0 ? warp_tot[warp - 1] : 0);
   for (int k = lo; k < hi; ++k) {
-    const uint32_t c = hist[k];
-    hist[k] = run;
+    const uint32_t c = row[k];
+    row[k] = run;
     run += c;
   }
+  if (threadIdx.x == blockDim.x - 1) hist[(size_t)RS_BINS * nt + d] = run;  // digit total
 }
 
 __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __restrict__ kin,
@@ -117,9 +122,27 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
     __syncwarp();
   }
   __syncthreads();
+  // digit offsets: exclusive scan of the digit totals (RS_BINS entries)
+  __shared__ uint32_t dig[RS_BINS];
+  for (int d = threadIdx.x; d < RS_BINS; d += blockDim.x) dig[d] = hist[(size_t)RS_BINS * nt + d];
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    uint32_t carry = 0;
+    for (int base = 0; base < RS_BINS; base += 32) {
+      const uint32_t x = dig[base + threadIdx.x];
+      uint32_t incl = x;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (threadIdx.x >= o) incl += t;
+      }
+      dig[base + threadIdx.x] = carry + incl - x;
+      carry += __shfl_sync(0xffffffffu, incl, 31);
+    }
+  }
+  __syncthreads();
   // exclusive scan of the per-warp counts across warps, per digit
   for (int d = threadIdx.x; d < RS_BINS; d += blockDim.x) {
-    uint32_t run = hist[d * nt + b];
+    uint32_t run = dig[d] + hist[d * nt + b];
 #pragma unroll
     for (int w = 0; w < kWarps; ++w) {
       const uint32_t c = wcnt[w][d];
@@ -155,19 +178,116 @@ __global__ void k_cells(Params P, const uint32_t* __restrict__ keys, DynState* d
 
 // Reorder gather of the persistent arrays (spatial_hash.cu:116-138), fused
 // into one pass: dst[i] = src[perm[i]] for i < n_alive; then n = n_alive.
-__global__ void k_gather(View src, View dst, const uint32_t* __restrict__ perm) {
+// Also counts fluid and wall particles per chunk; the last block turns the
+// counts into the chunk offsets of the ordered phase index lists
+// (partials rows 0 and 1) and their lengths.
+__global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uint32_t* __restrict__ perm, Reduce R) {
+  __shared__ double sh[2 * kBlock / 32];
   DynState* dyn = src.dyn;
   const int na = dyn->n_alive;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < na; i += gridDim.x * blockDim.x) {
-    const uint32_t j = perm[i];
-    dst.xp[i] = src.xp[j];
-    dst.vT[i] = src.vT[j];
-    dst.vt[i] = src.vt[j];
-    dst.nrm[i] = src.nrm[j];
-    dst.mrps[i] = src.mrps[j];
-    dst.id[i] = src.id[j];
+  const int nch = num_chunks(na);
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int i = c * kChunk + threadIdx.x;
+    double cnt[2] = {0.0, 0.0};
+    if (i < na) {
+      const uint32_t j = perm[i];
+      const float4 xp = src.xp[j];
+      dst.xp[i] = xp;
+      dst.vT[i] = src.vT[j];
+      dst.vt[i] = src.vt[j];
+      dst.nrm[i] = src.nrm[j];
+      dst.mrps[i] = src.mrps[j];
+      dst.id[i] = src.id[j];
+      const int ph = ph_of(xp);
+      if (is_fluid(ph)) cnt[0] = 1.0;
+      else if (ph == kWall) cnt[1] = 1.0;
+    }
+    publish_chunk<2>(R, c, cnt, sh);
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) dyn->n = na;
+  if (last_block(R.ticket)) {
+    const double nf = block_exclusive_scan(R, 0, nch);
+    const double nw = block_exclusive_scan(R, 1, nch);
+    if (threadIdx.x == 0) {
+      dyn->n_fluid_list = (int)nf;
+      dyn->n_wall_list = (int)nw;
+      dyn->n = na;
+    }
+  }
+}
+
+// Neighbour lists of every particle in the reference's iteration order
+// (for_each_neighbor filtered by r^2 < support^2, self included), stored
+// transposed so a warp reads consecutive words.  mode LISTS_PHASE also fills
+// the ordered fluid / wall index lists from the gather's chunk offsets;
+// mode LISTS_DENSITY additionally runs compute_density_summation
+// (SPH_kernels.cu:6-34) and the equation of state (navier_stokes.cu:5-14)
+// on the same candidate scan.
+__global__ void __launch_bounds__(kBlock) k_build_lists(Params P, View V, Reduce R, int mode) {
+  __shared__ int wcnt[2][kBlock / 32];
+  DynState* dyn = V.dyn;
+  const int n = dyn->n;
+  const int nch = num_chunks(n);
+  const size_t stride = (size_t)V.capacity;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned overflow = 0;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int i = c * kChunk + threadIdx.x;
+    const bool valid = i < n;
+    const float4 xpi = valid ? V.xp[i] : make_float4(0, 0, 0, 0);
+    const int ph = valid ? ph_of(xpi) : kDead;
+    if (mode != LISTS_ONLY) {
+      // ordered phase lists: chunk offset + rank inside the chunk
+      const bool isf = valid && is_fluid(ph), isw = valid && ph == kWall;
+      const unsigned bf = __ballot_sync(0xffffffffu, isf), bw = __ballot_sync(0xffffffffu, isw);
+      if (lane == 0) {
+        wcnt[0][warp] = __popc(bf);
+        wcnt[1][warp] = __popc(bw);
+      }
+      __syncthreads();
+      int pf = 0, pw = 0;
+      for (int w = 0; w < warp; ++w) {
+        pf += wcnt[0][w];
+        pw += wcnt[1][w];
+      }
+      const unsigned lt = (1u << lane) - 1u;
+      if (isf) V.fluid_idx[(int)__ldcg(R.partials + c) + pf + __popc(bf & lt)] = i;
+      if (isw) V.wall_idx[(int)__ldcg(R.partials + R.max_chunks + c) + pw + __popc(bw & lt)] = i;
+      __syncthreads();
+    }
+    if (!valid) continue;
+    const V3 xi = xyz(xpi);
+    const bool dens = mode == LISTS_DENSITY && is_fluid(ph);
+    int cnt = 0;
+    float sum = 0.0f, r2min = P.support2;
+    int* list = V.nbr + i;
+    for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4, V3, float r2) {
+      if (cnt < kMaxNbr) list[(size_t)cnt * stride] = j;
+      ++cnt;
+      if (dens) {
+        sum += kernel_W(P, sqrtf(r2));
+        if (j != i && r2 < r2min) r2min = r2;
+      }
+    });
+    V.nbr_cnt[i] = cnt;
+    if (cnt > kMaxNbr) overflow = CRYO_DEV_NBR_OVERFLOW;
+    if (mode == LISTS_DENSITY) {
+      float* mr = reinterpret_cast<float*>(V.mrps + i);
+      if (!is_fluid(ph)) {
+        mr[3] = 1.0f / P.vol0;
+        V.rmin[i] = P.support;
+      } else {
+        mr[3] = sum;
+        V.rmin[i] = sqrtf(r2min);
+        float rho = mr[1];
+        if (P.density_mode == CRYO_DENSITY_SUMMATION) {
+          rho = (ph == kLiquid ? V.vt[i].w : mr[0]) * sum;
+          mr[1] = rho;
+        }
+        mr[2] = eos_pressure(P, ph, rho, V.vT[i].w);
+      }
+    }
+  }
+  if (overflow) atomicOr(&dyn->status, overflow);
 }
 
 // Neighbour list dump (test hook): counts, then the lists at given offsets.

@@ -10,6 +10,7 @@ constexpr int RS_THREADS = 256;
 constexpr int RS_TILE = 4096;  // keys per radix tile (16 per thread)
 constexpr int RS_BITS = 8;
 constexpr int RS_BINS = 1 << RS_BITS;
+constexpr int RS_SCAN_THREADS = 256;
 
 // Layout of the FP64 partials of one reduction: partials[v * max_chunks + c].
 struct Reduce {
@@ -30,18 +31,70 @@ __device__ inline bool last_block(unsigned* ticket) {
   if (is_last && threadIdx.x == 0) *ticket = 0u;  // ready for the next launch
   return is_last;
 }
-// Sum of value v over chunks [0, nchunks) (fixed order, compensated), run by
-// thread 0 of the last block.
-__device__ inline double sum_partials(const Reduce& R, int v, int nchunks) {
+// Compensated two-sum accumulation (Neumaier).
+__device__ inline void neumaier(double& s, double& c, double x) {
+  const double t = s + x;
+  c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
+  s = t;
+}
+// Sum of value v over chunks [0, nchunks), computed by the whole (last) block
+// in a fixed order: thread t sums chunks t, t + blockDim, ... (compensated),
+// then thread 0 combines the per-thread sums in thread order (compensated).
+// Every thread of the block must call it; the result is valid in thread 0.
+__device__ inline double block_sum_partials(const Reduce& R, int v, int nchunks) {
+  __shared__ double hs[kBlock], hc[kBlock];
   double s = 0, c = 0;
   const double* p = R.partials + (size_t)v * R.max_chunks;
-  for (int k = 0; k < nchunks; ++k) {
-    const double x = __ldcg(p + k);
-    const double t = s + x;
-    c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
-    s = t;
+  for (int k = threadIdx.x; k < nchunks; k += blockDim.x) neumaier(s, c, __ldcg(p + k));
+  hs[threadIdx.x] = s;
+  hc[threadIdx.x] = c;
+  __syncthreads();
+  double r = 0;
+  if (threadIdx.x == 0) {
+    double S = 0, Cc = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      neumaier(S, Cc, hs[t]);
+      neumaier(S, Cc, hc[t]);
+    }
+    r = S + Cc;
   }
-  return s + c;
+  __syncthreads();
+  return r;
+}
+// In-place exclusive scan of the (integral) chunk values of row v by the whole
+// block; returns the total (all threads).
+__device__ inline double block_exclusive_scan(const Reduce& R, int v, int nchunks) {
+  __shared__ double seg[kBlock];
+  double* p = R.partials + (size_t)v * R.max_chunks;
+  const int per = (nchunks + blockDim.x - 1) / blockDim.x;
+  const int lo = threadIdx.x * per, hi = min(lo + per, nchunks);
+  double s = 0;
+  for (int k = lo; k < hi; ++k) s += __ldcg(p + k);
+  seg[threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double run = 0;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      const double x = seg[t];
+      seg[t] = run;
+      run += x;
+    }
+  }
+  __syncthreads();
+  double run = seg[threadIdx.x];
+  for (int k = lo; k < hi; ++k) {
+    const double x = __ldcg(p + k);
+    p[k] = run;
+    run += x;
+  }
+  __syncthreads();
+  // total = last segment's exclusive prefix + its sum
+  __shared__ double total;
+  if (threadIdx.x == blockDim.x - 1) total = run;
+  __syncthreads();
+  const double t = total;
+  __syncthreads();
+  return t;
 }
 // Writes the block sums of NV values for chunk c.
 template <int NV>
@@ -60,7 +113,9 @@ __global__ void k_rs_scan(uint32_t* hist, const DynState* dyn);
 __global__ void k_rs_downsweep(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int shift,
                                int bits, const DynState* dyn, const uint32_t* hist);
 __global__ void k_cells(Params P, const uint32_t* keys, DynState* dyn, int* cell_begin);
-__global__ void k_gather(View src, View dst, const uint32_t* perm);
+__global__ void k_gather(View src, View dst, const uint32_t* perm, Reduce R);
+enum { LISTS_ONLY = 0, LISTS_PHASE = 1, LISTS_DENSITY = 2 };
+__global__ void k_build_lists(Params P, View V, Reduce R, int mode);
 __global__ void k_nbr_count(Params P, View V, int* counts);
 __global__ void k_nbr_fill(Params P, View V, const long long* offsets, int* list);
 
@@ -76,7 +131,9 @@ __global__ void k_smooth_normals(Params P, View V);
 // Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
 enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8, FORCE_DRHO = 16,
        FORCE_THERMAL = 32, FORCE_MAXIMA = 64, FORCE_THERMAL_ALWAYS = 128 };
-__global__ void k_forces(Params P, View V, int what);
+template <int WHAT>
+__global__ void k_forces_t(Params P, View V, int what_rt);
+constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
 __global__ void k_shift_compute(Params P, View V);
 __global__ void k_shift_apply(Params P, View V);
 __global__ void k_probe(Params P, View V, const float* pts, int np, float* out);

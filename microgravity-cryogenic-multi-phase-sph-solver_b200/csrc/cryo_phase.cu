@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
       if (fl & kSource) {
         const int target = (fl & kTargetVapor) ? kVapor : kLiquid;
         float wsum = 0.0f, wr_max = 0.0f;
-        for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
+        for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
           if (j == i || ph_of(xj) != target || (fl_of(xj) & kDying)) return;
           const float w = kernel_W(P, sqrtf(r2));
           const float4 mr = __ldg(V.mrps + j);
@@ -186,10 +186,15 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
     }
     if (sums) publish_chunk<3>(R, c, s, sh);
   }
-  if (sums && last_block(R.ticket) && threadIdx.x == 0) {
-    dyn->evaporated += sum_partials(R, 0, nch);
-    dyn->condensed += sum_partials(R, 1, nch);
-    dyn->merges += (int)sum_partials(R, 2, nch);
+  if (sums && last_block(R.ticket)) {
+    const double ev = block_sum_partials(R, 0, nch);
+    const double co = block_sum_partials(R, 1, nch);
+    const double me = block_sum_partials(R, 2, nch);
+    if (threadIdx.x == 0) {
+      dyn->evaporated += ev;
+      dyn->condensed += co;
+      dyn->merges += (int)me;
+    }
   }
 }
 
@@ -208,7 +213,7 @@ __global__ void __launch_bounds__(kBlock) k_pc_apply(Params P, View V, int gated
     const float Vi = mi / mr.y;
     float in_m = 0.0f, in_H = 0.0f;
     if (!(fl & kDying)) {
-      for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
+      for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
         if (j == i) return;
         const float4 pcj = __ldg(V.pc + j);
         const float om = pcj.x;
@@ -259,7 +264,7 @@ __global__ void __launch_bounds__(kBlock) k_rebalance1(Params P, View V, int gat
     const V3 vi = xyz(vTi);
     float dm = 0.0f, dH = 0.0f;
     V3 dP{0, 0, 0};
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
+    for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
       if (j == i || ph_of(xj) != kVapor) return;
       const float mj = __ldg(V.mrps + j).x;
       const float flow = beta * P.vol0 * kernel_W(P, sqrtf(r2)) * (mj - mi);
@@ -319,15 +324,10 @@ __global__ void __launch_bounds__(kBlock) k_rebalance2_mark(Params P, View V, Re
     }
     publish_chunk<1>(R, c, cnt, sh);
   }
-  if (last_block(R.ticket) && threadIdx.x == 0) {
+  if (last_block(R.ticket)) {
     // exclusive scan of the chunk counts (in place, exact in double)
-    double run = 0;
-    for (int k = 0; k < nch; ++k) {
-      const double v = R.partials[k];
-      R.partials[k] = run;
-      run += v;
-    }
-    dyn->split_requested = (int)run;
+    const double total = block_exclusive_scan(R, 0, nch);
+    if (threadIdx.x == 0) dyn->split_requested = (int)total;
   }
 }
 
@@ -465,9 +465,13 @@ __global__ void __launch_bounds__(kBlock) k_venting(Params P, View V, Reduce R, 
     }
     publish_chunk<2>(R, c, s, sh);
   }
-  if (last_block(R.ticket) && threadIdx.x == 0) {
-    dyn->vented += sum_partials(R, 0, nch);
-    dyn->vented_h += sum_partials(R, 1, nch);
+  if (last_block(R.ticket)) {
+    const double vm = block_sum_partials(R, 0, nch);
+    const double vh = block_sum_partials(R, 1, nch);
+    if (threadIdx.x == 0) {
+      dyn->vented += vm;
+      dyn->vented_h += vh;
+    }
   }
 }
 

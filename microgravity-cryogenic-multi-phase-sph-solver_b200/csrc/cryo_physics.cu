@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params P, View V, int fuse_e
     }
     const V3 xi = xyz(xpi);
     float sum = 0.0f, r2min = P.support2;
-    for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4, V3, float r2) {
+    for_each_nbr(P, V, i, xi, [&](int j, float4, V3, float r2) {
       sum += kernel_W(P, sqrtf(r2));
       if (j != i && r2 < r2min) r2min = r2;
     });
@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(kBlock) k_normalize_masses(Params P, View V) {
     const float4 xpi = V.xp[i];
     if (!is_fluid(ph_of(xpi))) continue;
     float sum = 0.0f;
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int, float4, V3, float r2) {
+    for_each_nbr(P, V, i, xyz(xpi), [&](int, float4, V3, float r2) {
       sum += kernel_W(P, sqrtf(r2));
     });
     if (sum > 0.0f) {
@@ -72,17 +72,18 @@ __global__ void __launch_bounds__(kBlock) k_eos(Params P, View V) {
 
 // compute_wall_boundary (navier_stokes.cu:16-69)
 __global__ void __launch_bounds__(kBlock) k_wall(Params P, View V) {
-  const int n = V.dyn->n;
   const DynState* dyn = V.dyn;
+  const Range rg = wall_range(P, V);
   const V3 g = v3(dyn->gravity[0], dyn->gravity[1], dyn->gravity[2]);
-  PARTICLE_LOOP(i, n) {
+  PARTICLE_LOOP(t, rg.count) {
+    const int i = particle_at(rg, t);
     const float4 xpi = V.xp[i];
     if (ph_of(xpi) != kWall) continue;
     const V3 xi = xyz(xpi);
     float sw[2] = {0, 0}, sp[2] = {0, 0}, sgr[2] = {0, 0};
     float srho = 0.0f;
     V3 sv{0, 0, 0};
-    for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4 xj, V3 rwf, float r2) {
+    for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rwf, float r2) {
       const int phj = ph_of(xj);
       if (!is_fluid(phj)) return;
       const float w = kernel_W(P, sqrtf(r2));
@@ -126,13 +127,14 @@ __global__ void __launch_bounds__(kBlock) k_wall(Params P, View V) {
 // is written when the CSF model is active.
 __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R, int heat_sum) {
   __shared__ double sh[kBlock / 32];
-  const int n = V.dyn->n;
-  const int nch = num_chunks(n);
+  const Range rg = fluid_range(P, V);
+  const int nch = num_chunks(rg.count);
   const bool write_ns = P.csf_active && !P.csf_smooth;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-    const int i = c * kChunk + threadIdx.x;
+    const int t = c * kChunk + threadIdx.x;
     double hsum[1] = {0.0};
-    if (i < n) {
+    if (t < rg.count) {
+      const int i = particle_at(rg, t);
       const float4 xpi = V.xp[i];
       const int ph = ph_of(xpi);
       if (is_fluid(ph)) {
@@ -140,7 +142,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
         const float ci = ph == kLiquid ? 1.0f : 0.0f;
         V3 gradc{0, 0, 0}, wall_n{0, 0, 0}, akn{0, 0, 0}, gradphi{0, 0, 0};
         float s_all = 0, s_other = 0, ww = 0, hw = 0;
-        for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4 xj, V3 rij, float r2) {
+        for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
           const float r = sqrtf(r2);
           const float w = kernel_W(P, r);
           const int phj = ph_of(xj);
@@ -210,11 +212,12 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
     }
     if (heat_sum) publish_chunk<1>(R, c, hsum, sh);
   }
-  if (heat_sum && last_block(R.ticket) && threadIdx.x == 0) {
+  if (heat_sum && last_block(R.ticket)) {
     DynState* dyn = V.dyn;
+    const double S = block_sum_partials(R, 0, nch);
+    if (threadIdx.x != 0) return;
     if (heat_sum == 2 || dyn->thermal_on) {
       if (P.heat_power != 0.0f) {
-        const double S = sum_partials(R, 0, nch);
         dyn->heat_inv_norm = S > 0 ? (float)(1.0 / S) : 0.0f;
       } else {
         dyn->heat_inv_norm = 0.0f;
@@ -234,7 +237,7 @@ __global__ void __launch_bounds__(kBlock) k_sps(Params P, View V) {
     }
     const V3 vi = xyz(V.vT[i]);
     float L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3 rij, float r2) {
+    for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3 rij, float r2) {
       if (j == i) return;
       const V3 gw = kernel_gradW(P, rij, sqrtf(r2));
       V3 vj;
@@ -288,7 +291,7 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
       continue;
     }
     V3 acc{0, 0, 0};
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
+    for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
       if (!is_fluid(ph_of(xj))) return;
       const V3 gj = xyz(__ldg(V.nrm + j));
       const float gjm = norm(gj);
@@ -300,6 +303,9 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
   }
 }
 
+#ifndef FORCES_MIN_BLOCKS
+#define FORCES_MIN_BLOCKS 2
+#endif
 // Fused force pass: compute_transport_acceleration (SPH_kernels.cu:56-104),
 // compute_momentum (navier_stokes.cu:121-245), apply_csf_surface_tension
 // (surface_tension.cu:120-177) or apply_akinci_surface_tension (:179-213),
@@ -307,17 +313,16 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
 // (phase_change.cu:31-75) and the dt maxima (sph_solver.cu:59-99, 475-479),
 // in one neighbour loop.  Each sub-pass reads only what the previous passes
 // wrote, never what this pass writes, so fusing keeps the reference's values.
-__global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
+template <int WHAT>
+__global__ void __launch_bounds__(kBlock, FORCES_MIN_BLOCKS) k_forces_t(Params P, View V, int what_rt) {
+  // WHAT >= 0: the sub-pass set is a compile-time constant (the step path);
+  // -1: read at run time (operator-level calls)
+  const int what = WHAT >= 0 ? WHAT : what_rt;
   DynState* dyn = V.dyn;
   const int n = dyn->n;
   const bool thermal = ((what & FORCE_THERMAL) && dyn->thermal_on) || (what & FORCE_THERMAL_ALWAYS);
-  const float heat_inv_norm = dyn->heat_inv_norm;
   const float dt = dyn->dt;
-  const V3 grav = v3(dyn->gravity[0], dyn->gravity[1], dyn->gravity[2]);
-  const V3 omega = v3(dyn->omega[0], dyn->omega[1], dyn->omega[2]);
-  const V3 omega_dot = v3(dyn->omega_dot[0], dyn->omega_dot[1], dyn->omega_dot[2]);
   const V3 origin = v3(dyn->frame_origin[0], dyn->frame_origin[1], dyn->frame_origin[2]);
-  const int frame_rot = dyn->frame_rot;
   const float h = P.h;
   const float eta2 = 0.01f * h * h;
   const float r_guard = 0.6f * P.dx;
@@ -327,10 +332,12 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
   const bool iso_walls = P.wall_bc == CRYO_WALL_ISOTHERMAL;
   float vmax_l = 0.0f, amax_l = 0.0f, tv_l = 0.0f, sr_l = 0.0f, nut_l = 0.0f;
 
-  PARTICLE_LOOP(i, n) {
-    const float4 xpi = V.xp[i];
-    const int ph = ph_of(xpi);
-    if (!is_fluid(ph)) {
+  // walls (and, without lists, every particle that is not fluid): zero outputs
+  {
+    const Range wr = P.use_lists ? wall_range(P, V) : Range{nullptr, n};
+    PARTICLE_LOOP(t, wr.count) {
+      const int i = particle_at(wr, t);
+      if (is_fluid(ph_of(V.xp[i]))) continue;
       if (what & FORCE_TRANSPORT) V.ab4[i] = make_float4(0.0f, 0.0f, 0.0f, V.ab4[i].w);
       if (what & FORCE_MOMENTUM) {
         V.a4[i] = make_float4(0.0f, 0.0f, 0.0f, V.a4[i].w);
@@ -339,8 +346,14 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
       }
       if (what & FORCE_DRHO) reinterpret_cast<float*>(V.ab4 + i)[3] = 0.0f;
       if (thermal) reinterpret_cast<float*>(V.a4 + i)[3] = 0.0f;
-      continue;
     }
+  }
+  const Range fr = fluid_range(P, V);
+  PARTICLE_LOOP(t, fr.count) {
+    const int i = particle_at(fr, t);
+    const float4 xpi = V.xp[i];
+    const int ph = ph_of(xpi);
+    if (!is_fluid(ph)) continue;
     const int pi_idx = phase_index(ph);
     const V3 xi = xyz(xpi);
     const float4 vTi = V.vT[i];
@@ -391,7 +404,7 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
     const float ki = P.k[pi_idx];
     float q = 0.0f;
 
-    for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4 xj, V3 rij, float r2) {
+    for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
       if (j == i) return;
       const float r = sqrtf(r2);
       const float dW = kernel_dWdr(P, r);
@@ -524,8 +537,11 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
     float4 a4 = V.a4[i];
     V3 acc = xyz(a4);
     if (what & FORCE_MOMENTUM) {
+      const V3 grav = v3(dyn->gravity[0], dyn->gravity[1], dyn->gravity[2]);
       acc = grav + force / mi + acc_av;
-      if (frame_rot) {
+      if (dyn->frame_rot) {
+        const V3 omega = v3(dyn->omega[0], dyn->omega[1], dyn->omega[2]);
+        const V3 omega_dot = v3(dyn->omega_dot[0], dyn->omega_dot[1], dyn->omega_dot[2]);
         const V3 rr = xi - origin;
         acc -= cross(omega_dot, rr) + cross(omega, cross(omega, rr)) + cross(omega, vi) * 2.0f;
       }
@@ -548,7 +564,7 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
     if (do_A) acc += accA;
     if (do_D) reinterpret_cast<float*>(V.ab4 + i)[3] = rhoi * div + P.delta_sph * h * P.c0 * diff;
     if (thermal) {
-      q += P.heat_power * V.heat_w[i] * heat_inv_norm;
+      q += P.heat_power * V.heat_w[i] * dyn->heat_inv_norm;
       a4.w = q / (mi * P.cp[pi_idx]);
     }
     V.a4[i] = f4(acc, a4.w);
@@ -579,6 +595,21 @@ __global__ void __launch_bounds__(kBlock) k_forces(Params P, View V, int what) {
     }
   }
 }
+
+// Instances: the generic one and every step-path sub-pass set.
+template __global__ void k_forces_t<-1>(Params, View, int);
+template __global__ void k_forces_t<67>(Params, View, int);
+template __global__ void k_forces_t<99>(Params, View, int);
+template __global__ void k_forces_t<83>(Params, View, int);
+template __global__ void k_forces_t<115>(Params, View, int);
+template __global__ void k_forces_t<75>(Params, View, int);
+template __global__ void k_forces_t<107>(Params, View, int);
+template __global__ void k_forces_t<91>(Params, View, int);
+template __global__ void k_forces_t<123>(Params, View, int);
+template __global__ void k_forces_t<71>(Params, View, int);
+template __global__ void k_forces_t<103>(Params, View, int);
+template __global__ void k_forces_t<87>(Params, View, int);
+template __global__ void k_forces_t<119>(Params, View, int);
 
 // Maxima only (CRYO_PASS_MAXIMA; sph_solver.cu:475-479), from the stored fields.
 __global__ void __launch_bounds__(kBlock) k_maxima(Params P, View V) {
@@ -629,7 +660,7 @@ __global__ void __launch_bounds__(kBlock) k_shift_compute(Params P, View V) {
     const float sigmai = V.mrps[i].w;
     if (!is_fluid(ph) || sigmai < P.tvf_sigma_min) continue;
     V3 sum{0, 0, 0};
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(xpi), [&](int j, float4 xj, V3 rij, float r2) {
+    for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3 rij, float r2) {
       if (j == i) return;
       const int phj = ph_of(xj);
       if (phj == kDead) return;
