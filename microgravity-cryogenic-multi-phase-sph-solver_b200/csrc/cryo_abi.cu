@@ -120,6 +120,15 @@ struct cryo_ctx {
   // scalar block
   DynState* dyn = nullptr;   // device
   DynState* hdyn = nullptr;  // pinned host mirror
+  double* diag_host = nullptr;  // pinned, 64 doubles
+  // Host-owned frame state (authoritative unless a manoeuvre table drives the
+  // frame on the device); updates go out through a ring of pinned slots.
+  DynState::Frame hframe{};
+  bool man_active = false;
+  static constexpr int kFrameSlots = 16;
+  DynState::Frame* frame_ring = nullptr;
+  cudaEvent_t frame_ev[kFrameSlots] = {};
+  int frame_next = 0;
 
   // maneuver table (device)
   double* man_t = nullptr;
@@ -235,6 +244,10 @@ struct cryo_ctx {
     if (cell_begin) cudaFree(cell_begin);
     if (dyn) cudaFree(dyn);
     if (hdyn) cudaFreeHost(hdyn);
+    if (diag_host) cudaFreeHost(diag_host);
+    if (frame_ring) cudaFreeHost(frame_ring);
+    for (cudaEvent_t e : frame_ev)
+      if (e) cudaEventDestroy(e);
     if (man_t) cudaFree(man_t);
     if (man_acc) cudaFree(man_acc);
     if (man_omega) cudaFree(man_omega);
@@ -276,10 +289,22 @@ struct cryo_ctx {
   void pull() {  // device scalar block -> host mirror
     CK(cudaMemcpyAsync(hdyn, dyn, sizeof(DynState), cudaMemcpyDeviceToHost, stream));
     sync();
+    if (man_active) hframe = hdyn->fr;
   }
   void push() {  // host mirror -> device scalar block
+    if (!man_active) hdyn->fr = hframe;
     CK(cudaMemcpyAsync(dyn, hdyn, sizeof(DynState), cudaMemcpyHostToDevice, stream));
     sync();
+  }
+  // Sends the host frame state without synchronising: the copy reads a
+  // pinned ring slot that is not reused until its previous copy completed.
+  void push_frame() {
+    const int k = frame_next;
+    frame_next = (frame_next + 1) % kFrameSlots;
+    CK(cudaEventSynchronize(frame_ev[k]));
+    frame_ring[k] = hframe;
+    CK(cudaMemcpyAsync(&dyn->fr, frame_ring + k, sizeof(DynState::Frame), cudaMemcpyHostToDevice, stream));
+    CK(cudaEventRecord(frame_ev[k], stream));
   }
 
   // -------------------------------------------------------- allocation
@@ -611,10 +636,10 @@ void cryo_ctx::enqueue_step(int s) {
   const int G = grid_blocks();
   LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
   LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
-  sort_and_gather(s, LISTS_DENSITY);
+  sort_and_gather(s, LISTS_PHASE);
   const int d = 1 - s;
   const View V = view(d);
-  evaluate_rates(d, false, P.use_lists != 0);
+  evaluate_rates(d, false, false);
   LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   if (P.shift_strength > 0.0f) {
     LAUNCH(k_shift_compute, G, kBlock, P, V);
@@ -901,12 +926,16 @@ int cryo_create(const cryo_config_t* cfg, const cryo_fluid_t* fluid, int device,
       CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault));
       CK(cudaMalloc(&c->dyn, sizeof(DynState)));
       CK(cudaMallocHost(&c->hdyn, sizeof(DynState)));
+      CK(cudaMallocHost(&c->diag_host, 64 * sizeof(double)));
+      CK(cudaMallocHost(&c->frame_ring, cryo_ctx::kFrameSlots * sizeof(DynState::Frame)));
+      for (int k = 0; k < cryo_ctx::kFrameSlots; ++k)
+        CK(cudaEventCreateWithFlags(&c->frame_ev[k], cudaEventDisableTiming));
       std::memset(c->hdyn, 0, sizeof(DynState));
+      set3(c->hframe.cfg_gravity, cfg->gravity);
+      set3(c->hframe.gravity, cfg->gravity);
       c->hdyn->p_ullage = fluid->p_sat;
       c->hdyn->spacing_ratio = 1.0f;
       c->hdyn->T_sat = fluid->T_sat;
-      set3(c->hdyn->cfg_gravity, cfg->gravity);
-      set3(c->hdyn->gravity, cfg->gravity);
       c->push();
     } catch (...) {
       delete c;
@@ -996,10 +1025,9 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
     d.last_dt = 0;
     d.step = 0;
     d.dt = 0;
-    set3(d.cfg_gravity, c->cfg.gravity);
-    d.gravity[0] = c->cfg.gravity[0] - d.frame_acc[0];
-    d.gravity[1] = c->cfg.gravity[1] - d.frame_acc[1];
-    d.gravity[2] = c->cfg.gravity[2] - d.frame_acc[2];
+    DynState::Frame& f = c->man_active ? d.fr : c->hframe;
+    set3(f.cfg_gravity, c->cfg.gravity);
+    for (int k = 0; k < 3; ++k) f.gravity[k] = c->cfg.gravity[k] - f.frame_acc[k];
     d.T_sat = c->fluid.T_sat;
     d.heat_inv_norm = 0;
     d.p_ullage = c->fluid.p_sat;
@@ -1119,22 +1147,22 @@ int cryo_capacity(cryo_ctx* c, int* cap) {
   return guard(c, [&] { *cap = c->capacity; });
 }
 
-// Solver::diagnostics (sph_solver.cu:609-653)
+// Solver::diagnostics (sph_solver.cu:609-653): one reduction kernel and one
+// device-to-host copy.
 int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
   return guard(c, [&] {
     c->ensure_initialized();
     const int G = c->grid_blocks();
     k_diagnostics<<<G, kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), c->diag_out);
     LAUNCH_CHECK();
-    double v[25];
-    CK(cudaMemcpyAsync(v, c->diag_out, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
-    c->pull();
-    const DynState& d = *c->hdyn;
+    double* v = c->diag_host;
+    CK(cudaMemcpyAsync(v, c->diag_out, 44 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
     std::memset(o, 0, sizeof(*o));
-    o->time = d.time;
-    o->step = d.step;
-    o->dt = d.last_dt;
-    o->n_total = d.n;
+    o->time = v[25];
+    o->step = (long long)v[26];
+    o->dt = v[27];
+    o->n_total = (int)v[28];
     o->n_liquid = (int)v[0];
     o->n_vapor = (int)v[1];
     o->n_wall = (int)v[2];
@@ -1143,13 +1171,13 @@ int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
     o->mass_total = o->mass_liquid + o->mass_vapor;
     o->kinetic_energy = v[5] + v[6];
     o->enthalpy = v[7] + v[8];
-    o->heat_input = d.heat_input;
-    o->evaporated_mass = d.evaporated;
-    o->condensed_mass = d.condensed;
-    o->vented_mass = d.vented;
-    o->vented_enthalpy = d.vented_h;
-    o->T_sat = d.T_sat;
-    o->p_ullage = d.p_ullage;
+    o->heat_input = v[29];
+    o->evaporated_mass = v[30];
+    o->condensed_mass = v[31];
+    o->vented_mass = v[32];
+    o->vented_enthalpy = v[33];
+    o->T_sat = v[34];
+    o->p_ullage = v[35];
     o->max_speed = (double)(float)v[23];
     if (o->mass_liquid > 0) {
       o->T_liquid_mean = v[9] / o->mass_liquid;
@@ -1160,13 +1188,13 @@ int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
       }
     }
     if (o->mass_vapor > 0) o->T_vapor_mean = v[10] / o->mass_vapor;
-    o->splits = d.splits;
-    o->merges = d.merges;
+    o->splits = (int)v[36];
+    o->merges = (int)v[37];
     for (int k = 0; k < 3; ++k) {
       o->slosh_force[k] = -(float)v[17 + k];
       o->slosh_moment[k] = -(float)v[20 + k];
-      o->frame_acceleration[k] = d.frame_acc[k];
-      o->frame_angular_velocity[k] = d.omega[k];
+      o->frame_acceleration[k] = (float)v[38 + k];
+      o->frame_angular_velocity[k] = (float)v[41 + k];
     }
   });
 }
@@ -1263,23 +1291,23 @@ int cryo_download(cryo_ctx* c, cryo_host_particles_out_t* o) {
 int cryo_set_gravity(cryo_ctx* c, const float* g) {
   return guard(c, [&] {
     set3(c->cfg.gravity, g);
-    c->pull();
-    set3(c->hdyn->cfg_gravity, g);
-    for (int k = 0; k < 3; ++k) c->hdyn->gravity[k] = g[k] - c->hdyn->frame_acc[k];
-    c->push();
+    if (c->man_active) c->pull();  // the device holds the manoeuvre's frame
+    set3(c->hframe.cfg_gravity, g);
+    for (int k = 0; k < 3; ++k) c->hframe.gravity[k] = g[k] - c->hframe.frame_acc[k];
+    c->push_frame();
   });
 }
 
 namespace {
-void host_apply_frame(DynState& d, const float* a, const float* w, const float* wd, const float* o) {
-  set3(d.frame_acc, a);
-  for (int k = 0; k < 3; ++k) d.gravity[k] = d.cfg_gravity[k] - a[k];
-  set3(d.omega, w);
-  set3(d.omega_dot, wd);
-  set3(d.frame_origin, o);
+void host_apply_frame(DynState::Frame& f, const float* a, const float* w, const float* wd, const float* o) {
+  set3(f.frame_acc, a);
+  for (int k = 0; k < 3; ++k) f.gravity[k] = f.cfg_gravity[k] - a[k];
+  set3(f.omega, w);
+  set3(f.omega_dot, wd);
+  set3(f.frame_origin, o);
   const float n1 = w[0] * w[0] + w[1] * w[1] + w[2] * w[2];
   const float n2 = wd[0] * wd[0] + wd[1] * wd[1] + wd[2] * wd[2];
-  d.frame_rot = (n1 > 0.0f || n2 > 0.0f) ? 1 : 0;
+  f.frame_rot = (n1 > 0.0f || n2 > 0.0f) ? 1 : 0;
 }
 
 // ManeuverProfile::evaluate (sph_solver.cu:244-268), host
@@ -1314,10 +1342,11 @@ void host_maneuver(int n, const double* t, const float* acc, const float* om, do
 // Solver::set_frame_motion (sph_solver.cu:669-672)
 int cryo_set_frame_motion(cryo_ctx* c, const float* a, const float* w, const float* wd, const float* o) {
   return guard(c, [&] {
-    c->pull();
-    c->hdyn->has_maneuver = 0;
-    host_apply_frame(*c->hdyn, a, w, wd, o);
-    c->push();
+    if (c->man_active) c->pull();
+    c->man_active = false;
+    c->hframe.has_maneuver = 0;
+    host_apply_frame(c->hframe, a, w, wd, o);
+    c->push_frame();
   });
 }
 
@@ -1344,14 +1373,17 @@ int cryo_set_maneuver(cryo_ctx* c, int n, const double* t, const float* acc, con
     if (omega) CK(cudaMemcpyAsync(c->man_omega, omega, n * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     c->pull();
     DynState& d = *c->hdyn;
-    d.has_maneuver = 1;
+    c->hframe = c->man_active ? d.fr : c->hframe;
+    c->man_active = true;
+    c->hframe.has_maneuver = 1;
     d.man_n = n;
     d.man_rot = omega ? 1 : 0;
     const float zero[3] = {0, 0, 0};
     set3(d.man_origin, origin ? origin : zero);
     float a[3], w[3], wd[3];
     host_maneuver(n, t, acc, omega, d.time, a, w, wd);
-    host_apply_frame(d, a, w, wd, d.man_origin);
+    host_apply_frame(c->hframe, a, w, wd, d.man_origin);
+    d.fr = c->hframe;
     c->push();
   });
 }
@@ -1367,11 +1399,12 @@ int cryo_maneuver_evaluate(int n, const double* t, const float* acc, const float
 // Solver::clear_frame_motion (sph_solver.cu:683-686)
 int cryo_clear_frame_motion(cryo_ctx* c) {
   return guard(c, [&] {
-    c->pull();
-    c->hdyn->has_maneuver = 0;
+    if (c->man_active) c->pull();
+    c->man_active = false;
+    c->hframe.has_maneuver = 0;
     const float z[3] = {0, 0, 0};
-    host_apply_frame(*c->hdyn, z, z, z, z);
-    c->push();
+    host_apply_frame(c->hframe, z, z, z, z);
+    c->push_frame();
   });
 }
 
@@ -1664,6 +1697,8 @@ int cryo_load_state(cryo_ctx* c, const void* blob, size_t bytes) {
     }
     *c->hdyn = h.dyn;
     c->hdyn->capacity = c->capacity;
+    c->man_active = c->hdyn->fr.has_maneuver != 0;
+    c->hframe = c->hdyn->fr;
     c->push();
     c->initialized = h.initialized != 0;
     c->has_vapor = h.has_vapor != 0;

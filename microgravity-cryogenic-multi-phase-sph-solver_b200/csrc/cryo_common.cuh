@@ -134,10 +134,14 @@ struct DynState {
   double time, last_dt;
   long long step;
   float dt;           // dt of the current step (SimParams::dt)
-  // frame (SimParams gravity/omega..., sph_solver.cu:660-667)
-  float gravity[3], omega[3], omega_dot[3], frame_origin[3], frame_acc[3];
-  int frame_rot;
-  float cfg_gravity[3];
+  // frame (SimParams gravity/omega..., sph_solver.cu:660-667); one contiguous
+  // block so the host can replace it with a single asynchronous copy
+  struct Frame {
+    float gravity[3], omega[3], omega_dot[3], frame_origin[3], frame_acc[3];
+    int frame_rot;
+    float cfg_gravity[3];
+    int has_maneuver;
+  } fr;
   // thermodynamics
   float T_sat, heat_inv_norm;
   double p_ullage, fluid_volume0, heat_input;
@@ -155,7 +159,7 @@ struct DynState {
   int thermal_on;     // SimParams::thermal (relax turns it off)
   int phase_change_on;  // SolverConfig::phase_change (relax turns it off)
   // maneuver
-  int has_maneuver, man_n, man_rot;
+  int man_n, man_rot;
   float man_origin[3];
 };
 
@@ -342,9 +346,17 @@ __device__ inline void for_each_nbr(const Params& P, const View& V, int i, V3 xi
   if (c <= kMaxNbr) {
     const int* __restrict__ list = V.nbr + i;
     const size_t stride = (size_t)V.capacity;
+    // software pipeline: the next index and position are in flight while the
+    // current neighbour is processed
+    int jn = c > 0 ? __ldg(list) : 0;
+    float4 xn = c > 0 ? __ldg(V.xp + jn) : make_float4(0, 0, 0, 0);
+    int jnn = c > 1 ? __ldg(list + stride) : 0;
     for (int k = 0; k < c; ++k) {
-      const int j = __ldg(list + (size_t)k * stride);
-      const float4 xj = __ldg(V.xp + j);
+      const int j = jn;
+      const float4 xj = xn;
+      jn = jnn;
+      if (k + 1 < c) xn = __ldg(V.xp + jn);
+      if (k + 2 < c) jnn = __ldg(list + (size_t)(k + 2) * stride);
       const V3 rij = xi - xyz(xj);
       const float r2 = norm2(rij);
       f(j, xj, rij, r2);

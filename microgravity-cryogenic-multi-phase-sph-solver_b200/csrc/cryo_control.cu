@@ -44,14 +44,14 @@ __device__ void maneuver_evaluate(const View& V, int n, int rot, double t, V3& a
 
 // Solver::apply_frame (sph_solver.cu:660-667)
 __device__ void apply_frame(DynState* d, V3 a, V3 w, V3 wd, const float* origin) {
-  d->frame_acc[0] = a.x; d->frame_acc[1] = a.y; d->frame_acc[2] = a.z;
-  d->gravity[0] = d->cfg_gravity[0] - a.x;
-  d->gravity[1] = d->cfg_gravity[1] - a.y;
-  d->gravity[2] = d->cfg_gravity[2] - a.z;
-  d->omega[0] = w.x; d->omega[1] = w.y; d->omega[2] = w.z;
-  d->omega_dot[0] = wd.x; d->omega_dot[1] = wd.y; d->omega_dot[2] = wd.z;
-  d->frame_origin[0] = origin[0]; d->frame_origin[1] = origin[1]; d->frame_origin[2] = origin[2];
-  d->frame_rot = (norm2(w) > 0.0f || norm2(wd) > 0.0f) ? 1 : 0;
+  d->fr.frame_acc[0] = a.x; d->fr.frame_acc[1] = a.y; d->fr.frame_acc[2] = a.z;
+  d->fr.gravity[0] = d->fr.cfg_gravity[0] - a.x;
+  d->fr.gravity[1] = d->fr.cfg_gravity[1] - a.y;
+  d->fr.gravity[2] = d->fr.cfg_gravity[2] - a.z;
+  d->fr.omega[0] = w.x; d->fr.omega[1] = w.y; d->fr.omega[2] = w.z;
+  d->fr.omega_dot[0] = wd.x; d->fr.omega_dot[1] = wd.y; d->fr.omega_dot[2] = wd.z;
+  d->fr.frame_origin[0] = origin[0]; d->fr.frame_origin[1] = origin[1]; d->fr.frame_origin[2] = origin[2];
+  d->fr.frame_rot = (norm2(w) > 0.0f || norm2(wd) > 0.0f) ? 1 : 0;
 }
 
 // Start of Solver::step (sph_solver.cu:513-522): the step size from the maxima
@@ -64,7 +64,7 @@ __global__ void k_begin_step(Params P, View V, int mode) {
   if (mode == BEGIN_STEP) {
     const float dt = compute_dt(P, *d);
     d->dt = dt;
-    if (d->has_maneuver) {
+    if (d->fr.has_maneuver) {
       V3 a, w, wd;
       maneuver_evaluate(V, d->man_n, d->man_rot, d->time + (double)dt, a, w, wd);
       apply_frame(d, a, w, wd, d->man_origin);
@@ -175,7 +175,8 @@ __global__ void __launch_bounds__(kBlock) k_heat_norm(Params P, View V, Reduce R
 // maximum in one FP64 pass.  out[] layout:
 //   0-2 counts L/V/W, 3-4 mass L/V, 5-6 KE L/V, 7-8 enthalpy L/V, 9-10 mT L/V,
 //   11-13 m x (L), 14-16 m v (L), 17-19 sum fw (fluid), 20-22 sum mw (fluid),
-//   23 max fluid speed, 24 max liquid T
+//   23 max fluid speed, 24 max liquid T, 25-43 the scalar state (clock,
+//   counters, ullage, frame)
 __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce R, double* __restrict__ out) {
   __shared__ double sh[23 * kBlock / 32];
   __shared__ float shmax[2][kBlock / 32];
@@ -252,6 +253,15 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
       float mx = 0.0f;
       for (int w = 0; w < kBlock / 32; ++w) mx = fmaxf(mx, wm[threadIdx.x][w]);
       out[23 + threadIdx.x] = mx;
+    }
+    if (threadIdx.x == 0) {  // the scalar state, so the host needs one copy
+      out[25] = d->time; out[26] = (double)d->step; out[27] = d->last_dt; out[28] = d->n;
+      out[29] = d->heat_input; out[30] = d->evaporated; out[31] = d->condensed; out[32] = d->vented;
+      out[33] = d->vented_h; out[34] = d->T_sat; out[35] = d->p_ullage; out[36] = d->splits; out[37] = d->merges;
+      for (int k = 0; k < 3; ++k) {
+        out[38 + k] = d->fr.frame_acc[k];
+        out[41 + k] = d->fr.omega[k];
+      }
     }
   }
 }

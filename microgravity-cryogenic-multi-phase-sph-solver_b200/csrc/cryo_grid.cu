@@ -218,10 +218,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uin
 // Neighbour lists of every particle in the reference's iteration order
 // (for_each_neighbor filtered by r^2 < support^2, self included), stored
 // transposed so a warp reads consecutive words.  mode LISTS_PHASE also fills
-// the ordered fluid / wall index lists from the gather's chunk offsets;
-// mode LISTS_DENSITY additionally runs compute_density_summation
-// (SPH_kernels.cu:6-34) and the equation of state (navier_stokes.cu:5-14)
-// on the same candidate scan.
+// the ordered fluid / wall index lists from the gather's chunk offsets.
 __global__ void __launch_bounds__(kBlock) k_build_lists(Params P, View V, Reduce R, int mode) {
   __shared__ int wcnt[2][kBlock / 32];
   DynState* dyn = V.dyn;
@@ -256,36 +253,31 @@ __global__ void __launch_bounds__(kBlock) k_build_lists(Params P, View V, Reduce
     }
     if (!valid) continue;
     const V3 xi = xyz(xpi);
-    const bool dens = mode == LISTS_DENSITY && is_fluid(ph);
     int cnt = 0;
-    float sum = 0.0f, r2min = P.support2;
     int* list = V.nbr + i;
-    for_each_neighbor(P, V.cell_begin, V.xp, xi, [&](int j, float4, V3, float r2) {
-      if (cnt < kMaxNbr) list[(size_t)cnt * stride] = j;
-      ++cnt;
-      if (dens) {
-        sum += kernel_W(P, sqrtf(r2));
-        if (j != i && r2 < r2min) r2min = r2;
-      }
-    });
-    V.nbr_cnt[i] = cnt;
-    if (cnt > kMaxNbr) overflow = CRYO_DEV_NBR_OVERFLOW;
-    if (mode == LISTS_DENSITY) {
-      float* mr = reinterpret_cast<float*>(V.mrps + i);
-      if (!is_fluid(ph)) {
-        mr[3] = 1.0f / P.vol0;
-        V.rmin[i] = P.support;
-      } else {
-        mr[3] = sum;
-        V.rmin[i] = sqrtf(r2min);
-        float rho = mr[1];
-        if (P.density_mode == CRYO_DENSITY_SUMMATION) {
-          rho = (ph == kLiquid ? V.vt[i].w : mr[0]) * sum;
-          mr[1] = rho;
+    int cx, cy, cz;
+    cell_coords(P, xi, cx, cy, cz);
+    const int z0 = cz > 0 ? cz - 1 : 0, z1 = cz < P.nz - 1 ? cz + 1 : cz;
+    const int y0 = cy > 0 ? cy - 1 : 0, y1 = cy < P.ny - 1 ? cy + 1 : cy;
+    const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < P.nx - 1 ? cx + 1 : cx;
+    for (int z = z0; z <= z1; ++z) {
+      for (int y = y0; y <= y1; ++y) {
+        const int row = (z * P.ny + y) * P.nx;
+        const int s = __ldg(V.cell_begin + row + x0);
+        const int e = __ldg(V.cell_begin + row + x1 + 1);
+#pragma unroll 4
+        for (int j = s; j < e; ++j) {
+          const float4 xj = __ldg(V.xp + j);
+          const V3 rij = xi - xyz(xj);
+          const float r2 = norm2(rij);
+          const bool in = r2 < P.support2;
+          if (in && cnt < kMaxNbr) list[(size_t)cnt * stride] = j;
+          cnt += in ? 1 : 0;
         }
-        mr[2] = eos_pressure(P, ph, rho, V.vT[i].w);
       }
     }
+    V.nbr_cnt[i] = cnt;
+    if (cnt > kMaxNbr) overflow = CRYO_DEV_NBR_OVERFLOW;
   }
   if (overflow) atomicOr(&dyn->status, overflow);
 }

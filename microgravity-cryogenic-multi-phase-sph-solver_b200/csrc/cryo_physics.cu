@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(kBlock) k_eos(Params P, View V) {
 __global__ void __launch_bounds__(kBlock) k_wall(Params P, View V) {
   const DynState* dyn = V.dyn;
   const Range rg = wall_range(P, V);
-  const V3 g = v3(dyn->gravity[0], dyn->gravity[1], dyn->gravity[2]);
+  const V3 g = v3(dyn->fr.gravity[0], dyn->fr.gravity[1], dyn->fr.gravity[2]);
   PARTICLE_LOOP(t, rg.count) {
     const int i = particle_at(rg, t);
     const float4 xpi = V.xp[i];
@@ -322,7 +322,7 @@ __global__ void __launch_bounds__(kBlock, FORCES_MIN_BLOCKS) k_forces_t(Params P
   const int n = dyn->n;
   const bool thermal = ((what & FORCE_THERMAL) && dyn->thermal_on) || (what & FORCE_THERMAL_ALWAYS);
   const float dt = dyn->dt;
-  const V3 origin = v3(dyn->frame_origin[0], dyn->frame_origin[1], dyn->frame_origin[2]);
+  const V3 origin = v3(dyn->fr.frame_origin[0], dyn->fr.frame_origin[1], dyn->fr.frame_origin[2]);
   const float h = P.h;
   const float eta2 = 0.01f * h * h;
   const float r_guard = 0.6f * P.dx;
@@ -537,11 +537,11 @@ __global__ void __launch_bounds__(kBlock, FORCES_MIN_BLOCKS) k_forces_t(Params P
     float4 a4 = V.a4[i];
     V3 acc = xyz(a4);
     if (what & FORCE_MOMENTUM) {
-      const V3 grav = v3(dyn->gravity[0], dyn->gravity[1], dyn->gravity[2]);
+      const V3 grav = v3(dyn->fr.gravity[0], dyn->fr.gravity[1], dyn->fr.gravity[2]);
       acc = grav + force / mi + acc_av;
-      if (dyn->frame_rot) {
-        const V3 omega = v3(dyn->omega[0], dyn->omega[1], dyn->omega[2]);
-        const V3 omega_dot = v3(dyn->omega_dot[0], dyn->omega_dot[1], dyn->omega_dot[2]);
+      if (dyn->fr.frame_rot) {
+        const V3 omega = v3(dyn->fr.omega[0], dyn->fr.omega[1], dyn->fr.omega[2]);
+        const V3 omega_dot = v3(dyn->fr.omega_dot[0], dyn->fr.omega_dot[1], dyn->fr.omega_dot[2]);
         const V3 rr = xi - origin;
         acc -= cross(omega_dot, rr) + cross(omega, cross(omega, rr)) + cross(omega, vi) * 2.0f;
       }
