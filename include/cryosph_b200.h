@@ -263,6 +263,19 @@ int cryo_maneuver_evaluate(int n, const double* time, const float* acc, const fl
 /* Solver::probe_pressure (sph_solver.cu:738-748): np points (np*3 floats). */
 int cryo_probe_pressure(cryo_ctx* ctx, const float* points, int np, float* out);
 
+/* Solver::probe_pressure without device allocation; no counterpart in the
+   reference. For callers that must not allocate device memory once running
+   (a control loop probing pressure every cycle under a fixed memory budget,
+   where a pool allocation can fail or stall once the particle arena has
+   filled the device). Points and results go through one fixed device array
+   per device of CRYO_PROBE_STATIC_MAX points; more points return CRYO_ERANGE.
+   The first call on a device sets that array up and should come before any
+   stream capture. Calls whose GPU work overlapped would race on the shared
+   array, so calls are serialised by a process-wide lock and return only once
+   their stream has finished. Same results as cryo_probe_pressure. */
+#define CRYO_PROBE_STATIC_MAX 16384
+int cryo_probe_pressure_noalloc(cryo_ctx* ctx, const float* points, int np, float* out);
+
 /* Derived parameters (the SimParams scalars the Python API exposes). */
 int cryo_sound_speed(cryo_ctx* ctx, float* c0);
 int cryo_smoothing_length(cryo_ctx* ctx, float* h);

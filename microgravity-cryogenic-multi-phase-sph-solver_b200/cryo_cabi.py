@@ -268,6 +268,7 @@ def load(path=None):
         "cryo_damp_velocities": (i, [vp, f]),
         "cryo_maneuver_evaluate": (i, [i, dp, fp, fp, d, fp, fp, fp]),
         "cryo_probe_pressure": (i, [vp, fp, i, fp]),
+        "cryo_probe_pressure_noalloc": (i, [vp, fp, i, fp]),
         "cryo_sound_speed": (i, [vp, fp]),
         "cryo_smoothing_length": (i, [vp, fp]),
         "cryo_pass": (i, [vp, i]),

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <limits>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -1454,6 +1455,57 @@ int cryo_probe_pressure(cryo_ctx* c, const float* pts, int np, float* out) {
     LAUNCH_CHECK();
     CK(cudaMemcpyAsync(out, d + 3 * (size_t)np, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaFreeAsync(d, c->stream));
+    c->sync();
+  });
+}
+
+// Solver::probe_pressure without device allocation. cryo_probe_pressure
+// takes its point/result buffer from the stream-ordered pool on every call;
+// this variant stages through one fixed array per device instead. It is for
+// callers that must not allocate device memory once running: a monitoring or
+// control loop that probes tank pressure every cycle under a fixed memory
+// budget, where a pool allocation can fail or stall once the particle arena
+// has filled the device. The array is set up on the first call on each device
+// (cudaGetSymbolAddress with that device current), so that first call should
+// come before any stream capture. It is shared by every context on the
+// device: calls whose GPU work overlapped would race on it, so calls hold a
+// process-wide lock and wait for their stream before returning. Nothing in
+// the array has to start at zero: each call writes the points it reads and a
+// result for every point before copying the results back.
+namespace {
+constexpr int kProbeStaticMaxDevices = 64;
+__device__ __align__(256) float g_probe_scratch[4 * CRYO_PROBE_STATIC_MAX];  // xyz per point, then results
+std::mutex g_probe_scratch_mu;
+float* g_probe_scratch_ptr[kProbeStaticMaxDevices] = {};
+}  // namespace
+
+int cryo_probe_pressure_noalloc(cryo_ctx* c, const float* pts, int np, float* out) {
+  return guard(c, [&] {
+    if (np > CRYO_PROBE_STATIC_MAX)
+      throw std::out_of_range("cryo_probe_pressure_noalloc: " + std::to_string(np) +
+                              " points exceed the fixed scratch of " + std::to_string(CRYO_PROBE_STATIC_MAX) +
+                              " points; split the call or use cryo_probe_pressure");
+    if (c->device < 0 || c->device >= kProbeStaticMaxDevices)
+      throw std::out_of_range("cryo_probe_pressure_noalloc: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_probe_scratch_mu);
+    float* d = g_probe_scratch_ptr[c->device];
+    if (!d) {
+      int prev = 0;
+      CK(cudaGetDevice(&prev));
+      CK(cudaSetDevice(c->device));
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_probe_scratch);
+      CK(cudaSetDevice(prev));
+      CK(e);
+      d = g_probe_scratch_ptr[c->device] = static_cast<float*>(p);
+    }
+    c->ensure_initialized();
+    if (np <= 0) return;
+    CK(cudaMemcpyAsync(d, pts, (size_t)np * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    const int blocks = std::max(1, std::min((np + 127) / 128, c->sm_count * 8));
+    k_probe<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(out, d + 3 * (size_t)np, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     c->sync();
   });
 }
