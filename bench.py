@@ -311,7 +311,7 @@ def main():
     e2e = roof = None
     if rank == 0 and not args.only_timed:
         # ---- e2e through the public API with host buffers
-        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, min(args.steps, 200), device, stream, flush)
+        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, args.steps, device, stream, flush)
         # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
         roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
 

@@ -279,6 +279,11 @@ struct cryo_ctx {
     const int need = (capacity + kBlock - 1) / kBlock;
     return std::max(1, std::min(need, sm_count * 8));
   }
+  // force pass: one thread per particle up to two full-occupancy waves
+  int forces_blocks() const {
+    const int need = (capacity + FORCES_BLOCK - 1) / FORCES_BLOCK;
+    return std::max(1, std::min(need, sm_count * (2048 / FORCES_BLOCK) * 2));
+  }
   void invalidate_graphs() {
     for (int k = 0; k < 2; ++k) {
       if (graph[k]) cudaGraphExecDestroy(graph[k]);
@@ -607,6 +612,7 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
   LAUNCH(k_interface, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
   if (P.sps) LAUNCH(k_sps, G, kBlock, P, V);
   if (P.csf_active && P.csf_smooth) LAUNCH(k_smooth_normals, G, kBlock, P, V);
+  const int GF = forces_blocks();
   int what = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
   if (P.csf_active) what |= FORCE_CSF;
   if (P.st_model == CRYO_ST_AKINCI) what |= FORCE_AKINCI;
@@ -614,7 +620,7 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
   if (P.thermal) what |= FORCE_THERMAL;
   switch (what) {
 #define FORCES_CASE(W) \
-  case W: LAUNCH(k_forces_t<W>, G, kBlock, P, V, W); break;
+  case W: LAUNCH(k_forces_t<W>, GF, FORCES_BLOCK, P, V, W); break;
     FORCES_CASE(FORCE_BASE)
     FORCES_CASE(FORCE_BASE | FORCE_THERMAL)
     FORCES_CASE(FORCE_BASE | FORCE_DRHO)
@@ -628,7 +634,7 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
     FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO)
     FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO | FORCE_THERMAL)
 #undef FORCES_CASE
-    default: LAUNCH(k_forces_t<-1>, G, kBlock, P, V, what);
+    default: LAUNCH(k_forces_t<-1>, GF, FORCES_BLOCK, P, V, what);
   }
 }
 
@@ -1548,17 +1554,17 @@ int cryo_pass(cryo_ctx* c, int pass) {
       case CRYO_PASS_EOS: k_eos<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_WALL_BOUNDARY: k_wall<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_INTERFACE: k_interface<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
-      case CRYO_PASS_TRANSPORT: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_TRANSPORT); break;
+      case CRYO_PASS_TRANSPORT: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_TRANSPORT); break;
       case CRYO_PASS_SPS: k_sps<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_MOMENTUM: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_MOMENTUM); break;
+      case CRYO_PASS_MOMENTUM: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_MOMENTUM); break;
       case CRYO_PASS_SMOOTH_NORMALS: k_smooth_normals<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_CSF: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_CSF); break;
-      case CRYO_PASS_AKINCI: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_AKINCI); break;
-      case CRYO_PASS_DENSITY_RATE: k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_DRHO); break;
+      case CRYO_PASS_CSF: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_CSF); break;
+      case CRYO_PASS_AKINCI: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_AKINCI); break;
+      case CRYO_PASS_DENSITY_RATE: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_DRHO); break;
       case CRYO_PASS_THERMAL:
         k_heat_norm<<<G, kBlock, 0, st>>>(P, V, R);
         LAUNCH_CHECK();
-        k_forces_t<-1><<<G, kBlock, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
+        k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
         break;
       case CRYO_PASS_MAXIMA:
         k_begin_step<<<1, 1, 0, st>>>(P, V, BEGIN_RATES);

@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uin
 // (for_each_neighbor filtered by r^2 < support^2, self included), stored
 // transposed so a warp reads consecutive words.  mode LISTS_PHASE also fills
 // the ordered fluid / wall index lists from the gather's chunk offsets.
-__global__ void __launch_bounds__(kBlock) k_build_lists(Params P, View V, Reduce R, int mode) {
+__global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params P, View V, Reduce R, int mode) {
   __shared__ int wcnt[2][kBlock / 32];
   DynState* dyn = V.dyn;
   const int n = dyn->n;
@@ -265,15 +265,24 @@ __global__ void __launch_bounds__(kBlock) k_build_lists(Params P, View V, Reduce
         const int row = (z * P.ny + y) * P.nx;
         const int s = __ldg(V.cell_begin + row + x0);
         const int e = __ldg(V.cell_begin + row + x1 + 1);
-#pragma unroll 4
-        for (int j = s; j < e; ++j) {
-          const float4 xj = __ldg(V.xp + j);
+        // candidates in groups of LIST_GROUP: all loads issued before the
+        // tests, so a thread has that many positions in flight
+        auto test = [&](const float4& xj, int j) {
           const V3 rij = xi - xyz(xj);
           const float r2 = norm2(rij);
           const bool in = r2 < P.support2;
           if (in && cnt < kMaxNbr) list[(size_t)cnt * stride] = j;
           cnt += in ? 1 : 0;
+        };
+        int j = s;
+        for (; j + LIST_GROUP <= e; j += LIST_GROUP) {
+          float4 xg[LIST_GROUP];
+#pragma unroll
+          for (int u = 0; u < LIST_GROUP; ++u) xg[u] = __ldg(V.xp + j + u);
+#pragma unroll
+          for (int u = 0; u < LIST_GROUP; ++u) test(xg[u], j + u);
         }
+        for (; j < e; ++j) test(__ldg(V.xp + j), j);
       }
     }
     V.nbr_cnt[i] = cnt;

@@ -134,6 +134,26 @@ enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8,
 template <int WHAT>
 __global__ void k_forces_t(Params P, View V, int what_rt);
 constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
+// Block shape of the force pass.  The pass is bound by the latency of each
+// particle's neighbour chain, so what matters is how many particles are in
+// flight at once: 64-thread blocks under a 112-register cap (9 per SM) keep
+// 18 warps per SM resident, which covers the 82k fluid particles of the dam
+// break in one wave (256-thread blocks at 117 registers held 16 warps and
+// needed two).
+// Neighbour-list build: candidate positions loaded per group, and the block
+// count per SM the register cap keeps resident.
+#ifndef LIST_GROUP
+#define LIST_GROUP 8
+#endif
+#ifndef LIST_MIN_BLOCKS
+#define LIST_MIN_BLOCKS 4
+#endif
+#ifndef FORCES_BLOCK
+#define FORCES_BLOCK 64
+#endif
+#ifndef FORCES_MIN_BLOCKS
+#define FORCES_MIN_BLOCKS 9
+#endif
 __global__ void k_shift_compute(Params P, View V);
 __global__ void k_shift_apply(Params P, View V);
 __global__ void k_probe(Params P, View V, const float* pts, int np, float* out);

@@ -303,9 +303,6 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
   }
 }
 
-#ifndef FORCES_MIN_BLOCKS
-#define FORCES_MIN_BLOCKS 2
-#endif
 // Fused force pass: compute_transport_acceleration (SPH_kernels.cu:56-104),
 // compute_momentum (navier_stokes.cu:121-245), apply_csf_surface_tension
 // (surface_tension.cu:120-177) or apply_akinci_surface_tension (:179-213),
@@ -314,7 +311,7 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
 // in one neighbour loop.  Each sub-pass reads only what the previous passes
 // wrote, never what this pass writes, so fusing keeps the reference's values.
 template <int WHAT>
-__global__ void __launch_bounds__(kBlock, FORCES_MIN_BLOCKS) k_forces_t(Params P, View V, int what_rt) {
+__global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Params P, View V, int what_rt) {
   // WHAT >= 0: the sub-pass set is a compile-time constant (the step path);
   // -1: read at run time (operator-level calls)
   const int what = WHAT >= 0 ? WHAT : what_rt;
