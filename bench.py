@@ -20,8 +20,14 @@ per step the frame-motion input goes host->device and the diagnostics come
 back device->host, plus the initial state upload and the final download),
 the roofline of the dominant kernel (per-kernel CUDA-event times from a
 profiled run, algorithmic bytes from cryo_roofline.py, DRAM traffic from the
-committed ncu summary), SM clocks sampled during the timed region, and the
-reference's own CPU implementation timed on this host (rank 0, N=1).
+committed ncu summary), SM clocks sampled during the timed region, the
+reference's own CPU implementation timed on this host (rank 0, N=1), and
+`batched`: BASELINE config 4 (64 seeded tanks of 5k-200k particles) advanced
+by one cs.Ensemble -- one graph launch per ensemble step, branch count
+autotuned -- against the same tanks stepped back to back by plain Solvers,
+with every tank's diagnostics compared bit for bit.  Under torchrun the
+tanks are sharded over ranks (longest-processing-time first); the step has
+no collective.
 """
 from __future__ import annotations
 
@@ -102,6 +108,57 @@ def workload(name, cs):
     x[fl] += rng.uniform(-0.05 * dx, 0.05 * dx, size=(int(fl.sum()), 3)).astype(np.float32)
     p["position"] = x
     return label, cfg, fluid, p, lo, hi
+
+
+def c4_tanks(cs, count=64, n_lo=5_000, n_hi=200_000, seed=SEED):
+    """BASELINE config 4 as seeded synthetic tanks: shape cylinder or sphere,
+    radius U[0.03, 0.3] m (cylinder height 2R x U[1, 2.5]), fill U[0.2, 0.8],
+    dx chosen so the particle count (walls included) is log-uniform in
+    [n_lo, n_hi], fluid LN2 / LOX / LCH4, gravity 1e-4 g, a lateral pulse of
+    U[0, 0.1] m/s^2 (ramped in over 10 ms, held to 50 ms, out by 60 ms)."""
+    rng = np.random.Generator(np.random.PCG64(seed + 4))
+    presets = [cs.FluidProperties.liquid_nitrogen, cs.FluidProperties.liquid_oxygen,
+               cs.FluidProperties.liquid_methane]
+    tanks = []
+    for t in range(count):
+        sphere = bool(rng.random() < 0.5)
+        R = float(rng.uniform(0.03, 0.3))
+        H = float(2.0 * R * rng.uniform(1.0, 2.5))
+        fill_fraction = float(rng.uniform(0.2, 0.8))
+        n_target = math.exp(rng.uniform(math.log(n_lo), math.log(n_hi)))
+        which = int(rng.integers(3))
+        amp = float(rng.uniform(0.0, 0.1))
+        if sphere:
+            geo, vol, area = cs.SphereTank(R), 4.0 / 3.0 * math.pi * R ** 3, 4.0 * math.pi * R ** 2
+        else:
+            geo, vol, area = cs.CylinderTank(R, H), math.pi * R * R * H, 2.0 * math.pi * R * (H + R)
+        lo_dx, hi_dx = 1e-5, 1.0  # interior lattice + 3 wall layers ~ n_target
+        for _ in range(60):
+            dx = math.sqrt(lo_dx * hi_dx)
+            if vol / dx ** 3 + 3.0 * area / dx ** 2 > n_target:
+                lo_dx = dx
+            else:
+                hi_dx = dx
+        dx = math.sqrt(lo_dx * hi_dx)
+        fluid = presets[which]()
+        cfg = cs.SolverConfig()
+        cfg.dx = dx
+        cfg.gravity = (0.0, 0.0, -9.81e-4)
+        cfg.thermo_mode = cs.TankThermoMode.Closed
+        fill = cs.FillSpec()
+        fill.fill_fraction = fill_fraction
+        p = cs.tank_particles(geo, fluid, dx, fill)
+        lo, hi = cs.tank_domain(geo, dx, 3)
+        jr = np.random.Generator(np.random.PCG64(seed + 1000 + t))
+        fl = p["phase"] != 2
+        x = p["position"].astype(np.float32).copy()
+        x[fl] += jr.uniform(-0.05 * dx, 0.05 * dx, size=(int(fl.sum()), 3)).astype(np.float32)
+        p["position"] = x
+        man = cs.ManeuverProfile([0.0, 0.01, 0.05, 0.06],
+                                 np.array([[0, 0, 0], [amp, 0, 0], [amp, 0, 0], [0, 0, 0]], np.float64))
+        tanks.append(dict(cfg=cfg, fluid=fluid, p=p, lo=lo, hi=hi, maneuver=man, n=int(len(x)),
+                          shape="sphere" if sphere else "cylinder", fluid_name=["LN2", "LOX", "LCH4"][which]))
+    return tanks
 
 
 def load(solver, p, lo, hi):
@@ -224,6 +281,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=50)
+    ap.add_argument("--batched-steps", type=int, default=100,
+                    help="steps of the batched-ensemble comparison (0 = skip it)")
+    ap.add_argument("--batched-tanks", type=int, default=64)
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
     args = ap.parse_args()
@@ -315,6 +375,31 @@ def main():
         # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
         roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
 
+    # ---- batched ensemble (config 4): tanks sharded over ranks, no collective in the step
+    batched = None
+    if args.batched_steps > 0 and not args.only_timed:
+        import cryo_shard
+        del solver
+        torch.cuda.empty_cache()
+        all_tanks = c4_tanks(cs, count=args.batched_tanks)
+        mine = cryo_shard.shard_of([tk["n"] for tk in all_tanks], rank, world)
+        b = batched_run(cs, [all_tanks[t] for t in mine], args.batched_steps, args.warmup, device)
+        agg = torch.tensor([b["ms_per_step"], b["back_to_back_ms_per_step"], 0.0 if b["diagnostics_bit_identical"] else 1.0],
+                           dtype=torch.float64, device=device)
+        if dist:
+            dist.all_reduce(agg, op=dist.ReduceOp.MAX)
+        ms_e, ms_s, differs = (float(v) for v in agg.tolist())
+        n_all = sum(tk["n"] for tk in all_tanks)
+        batched = dict(b)
+        batched.update({
+            "tanks": len(all_tanks), "particles": n_all, "ranks": world,
+            "particles_min": min(tk["n"] for tk in all_tanks), "particles_max": max(tk["n"] for tk in all_tanks),
+            "value": n_all / (ms_e / 1e3), "ms_per_step": ms_e,
+            "back_to_back": n_all / (ms_s / 1e3), "back_to_back_ms_per_step": ms_s, "speedup": ms_s / ms_e,
+            "diagnostics_bit_identical": differs == 0.0,
+            "sharding": "tanks split over ranks longest-processing-time first by particle count" if world > 1 else None,
+        })
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
         r = reference_rate(cfg, fluid, p, lo, hi, 200, 2, budget_s=20.0)
@@ -338,6 +423,7 @@ def main():
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line))
     if dist:
@@ -389,6 +475,63 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
     return {"value": n * steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": int(state_in / steps + ctl), "d2h_bytes_per_step": int(diag + state_out / steps),
             "steps": steps, "timing": "CUDA events per step (host work inside), L2 flushed between steps"}
+
+
+def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
+    """the tanks advanced together by one cs.Ensemble (one
+    graph launch per ensemble step, branch count autotuned) against the same
+    tanks stepped back to back by plain Solvers.  Both sides take the same
+    total number of steps, so every tank's diagnostics can be compared bit for
+    bit at the end.  Device time from CUDA events; the ensemble's state
+    (hundreds of MB) exceeds L2, the back-to-back tanks are each L2-sized (an
+    advantage to the back-to-back side)."""
+    import torch
+
+    def make():
+        out = []
+        for tk in tanks:
+            sv = cs.Solver(tk["cfg"], tk["fluid"], device)
+            load(sv, tk["p"], tk["lo"], tk["hi"])
+            sv.set_maneuver(tk["maneuver"])
+            out.append(sv)
+        return out
+
+    ens_tanks = make()
+    ens = cs.Ensemble(device)
+    for sv in ens_tanks:
+        ens.add(sv)
+    cands = sorted({k for k in (len(tanks), 32, 16, 8, 4) if 1 <= k <= len(tanks)}, reverse=True)
+    branches, _ = ens.tune(cands, tune_steps)
+    ens.run_steps(warmup)
+    ms_ens = ens.step_time(steps)
+    total_steps = len(cands) * (tune_steps + 1) + warmup + 1 + steps
+    n_total = sum(tk["n"] for tk in tanks)
+    launches = ens.launches_per_step
+    d_ens = [d.as_dict() for d in ens.diagnostics()]
+    del ens
+
+    solo = make()
+    ms_solo = 0.0
+    for sv in solo:
+        sv.run_steps(total_steps - steps)
+        st = torch.cuda.ExternalStream(sv.stream_handle, device=device)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        sv.run_steps(steps)
+        b.record(st)
+        b.synchronize()
+        ms_solo += a.elapsed_time(b)
+    d_solo = [sv.diagnostics().as_dict() for sv in solo]
+    same = all(json.dumps(x, sort_keys=True) == json.dumps(y, sort_keys=True) for x, y in zip(d_ens, d_solo))
+    return {
+        "workload": f"c4_ensemble_{len(tanks)}_tanks", "tanks": len(tanks), "particles": n_total,
+        "particles_min": min(tk["n"] for tk in tanks), "particles_max": max(tk["n"] for tk in tanks),
+        "steps": steps, "value": n_total * steps / (ms_ens / 1e3 * steps) if ms_ens > 0 else None, "unit": UNIT,
+        "ms_per_step": ms_ens, "back_to_back": n_total * steps / (ms_solo / 1e3), "back_to_back_ms_per_step": ms_solo / steps,
+        "speedup": (ms_solo / steps) / ms_ens if ms_ens > 0 else None, "branches": branches,
+        "gpu_launches_per_step": launches, "diagnostics_bit_identical": bool(same),
+        "execution": "one CUDA graph launch per ensemble step (every tank's kernels as concurrent branches)",
+    }
 
 
 def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vapor, label):

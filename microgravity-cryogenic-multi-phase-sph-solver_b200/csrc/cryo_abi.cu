@@ -86,6 +86,8 @@ size_t particle_bytes(size_t cap) {
 
 }  // namespace
 
+void ensemble_detach(cryo_ensemble* e, cryo_ctx* c);
+
 struct cryo_ctx {
   cryo_config_t cfg{};
   cryo_fluid_t fluid{};
@@ -144,6 +146,13 @@ struct cryo_ctx {
   bool has_particles = false, initialized = false, has_vapor = false;
   float char_length = 0;
   float pass_dt = 0;
+
+  // batched stepping: the ensemble this tank belongs to (if any), an event
+  // for ordering its stream against the ensemble's, and a counter bumped
+  // whenever the step graphs are invalidated (the ensemble then rebuilds)
+  cryo_ensemble* ensemble = nullptr;
+  cudaEvent_t ens_ev = nullptr;
+  unsigned long long generation = 0;
 
   // execution
   bool graph_mode = true;
@@ -236,6 +245,8 @@ struct cryo_ctx {
   }
 
   ~cryo_ctx() {
+    if (ensemble) ensemble_detach(ensemble, this);
+    if (ens_ev) cudaEventDestroy(ens_ev);
     telemetry_release();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (int k = 0; k < 2; ++k)
@@ -285,6 +296,7 @@ struct cryo_ctx {
     return std::max(1, std::min(need, sm_count * (2048 / FORCES_BLOCK) * 2));
   }
   void invalidate_graphs() {
+    ++generation;
     for (int k = 0; k < 2; ++k) {
       if (graph[k]) cudaGraphExecDestroy(graph[k]);
       graph[k] = nullptr;
@@ -753,6 +765,187 @@ void cryo_ctx::run_until(double t_end) {
     for (long long s = 0; s < k; ++s) launch_step();
     check_capacity();  // pulls the clock
   }
+}
+
+// ---------------------------------------------------------------------------
+// Batched stepping of independent tanks (no counterpart in the reference).
+// Each tank keeps its own context: arena, stream, parameters and step
+// sequence.  One ensemble step is ONE graph launch that holds every tank's
+// step as a chain of that tank's own kernels, spread over `chains` concurrent
+// branches (tanks assigned longest-processing-time first by particle count;
+// one branch per tank by default).  Tanks far too small to fill the GPU alone
+// then run side by side.  Every tank runs exactly the kernels, launch shapes
+// and arguments of its own step graph, so its results are those of stepping
+// it alone, bit for bit.
+struct cryo_ensemble {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
+  std::vector<cryo_ctx*> tanks;
+  int chains = 0;  // 0: one branch per tank
+  cudaGraphExec_t exec[2] = {nullptr, nullptr};
+  std::vector<int> built_cur;  // each tank's ping-pong parity when exec[0] was built
+  std::vector<unsigned long long> built_gen;
+  int built_chains = -1;
+  int next = 0;  // exec launched by the next step
+  int step_launches = 0;
+  long long steps_run = 0;
+  std::string err;
+
+  ~cryo_ensemble() {
+    if (stream) cudaStreamSynchronize(stream);
+    drop();
+    for (cryo_ctx* c : tanks) c->ensemble = nullptr;
+    for (cudaEvent_t e : {fork, done, t0, t1})
+      if (e) cudaEventDestroy(e);
+    if (stream) cudaStreamDestroy(stream);
+  }
+  void drop() {
+    for (int k = 0; k < 2; ++k) {
+      if (exec[k]) cudaGraphExecDestroy(exec[k]);
+      exec[k] = nullptr;
+    }
+    built_chains = -1;
+  }
+  int branches() const {
+    const int t = (int)tanks.size();
+    return chains <= 0 ? t : std::min(chains, t);
+  }
+  bool valid() const {
+    if (!exec[0] || !exec[1] || built_chains != branches()) return false;
+    for (size_t t = 0; t < tanks.size(); ++t)
+      if (tanks[t]->generation != built_gen[t] || tanks[t]->cur != ((built_cur[t] + next) & 1)) return false;
+    return true;
+  }
+  // Tanks per branch: largest first, each to the least-loaded branch.
+  std::vector<std::vector<int>> plan() const {
+    const int k = branches();
+    std::vector<int> order(tanks.size());
+    for (size_t t = 0; t < tanks.size(); ++t) order[t] = (int)t;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return tanks[a]->hdyn->n > tanks[b]->hdyn->n; });
+    std::vector<std::vector<int>> out(k);
+    std::vector<long long> load(k, 0);
+    for (int t : order) {
+      int best = 0;
+      for (int b = 1; b < k; ++b)
+        if (load[b] < load[best]) best = b;
+      out[best].push_back(t);
+      load[best] += std::max(tanks[t]->hdyn->n, 1);
+    }
+    return out;
+  }
+  void capture(int q, const std::vector<std::vector<int>>& branches_plan, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+    int launches = 0;
+    try {
+      CK(cudaEventRecord(fork, stream));
+      for (const auto& br : branches_plan) {
+        cudaEvent_t prev = fork;
+        for (int t : br) {
+          cryo_ctx* c = tanks[t];
+          CK(cudaStreamWaitEvent(c->stream, prev, 0));
+          const long long c0 = c->launch_counter;
+          c->enqueue_step((built_cur[t] + q) & 1);
+          launches += (int)(c->launch_counter - c0);
+          CK(cudaEventRecord(c->ens_ev, c->stream));
+          prev = c->ens_ev;
+        }
+      }
+      for (cryo_ctx* c : tanks) CK(cudaStreamWaitEvent(stream, c->ens_ev, 0));
+    } catch (...) {
+      cudaStreamEndCapture(stream, &g);
+      if (g) cudaGraphDestroy(g);
+      throw;
+    }
+    CK(cudaStreamEndCapture(stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    CK(e);
+    step_launches = launches;
+  }
+  void build() {
+    drop();
+    leave();
+    for (cryo_ctx* c : tanks) c->pull();  // particle counts for the plan
+    enter();
+    built_cur.resize(tanks.size());
+    built_gen.resize(tanks.size());
+    for (size_t t = 0; t < tanks.size(); ++t) {
+      built_cur[t] = tanks[t]->cur;
+      built_gen[t] = tanks[t]->generation;
+    }
+    next = 0;
+    const auto pl = plan();
+    capture(0, pl, &exec[0]);
+    capture(1, pl, &exec[1]);
+    built_chains = branches();
+  }
+  // tank streams -> ensemble stream, and back
+  void enter() {
+    for (cryo_ctx* c : tanks) {
+      CK(cudaEventRecord(c->ens_ev, c->stream));
+      CK(cudaStreamWaitEvent(stream, c->ens_ev, 0));
+    }
+  }
+  void leave() {
+    CK(cudaEventRecord(done, stream));
+    for (cryo_ctx* c : tanks) CK(cudaStreamWaitEvent(c->stream, done, 0));
+  }
+  void prepare() {
+    for (cryo_ctx* c : tanks) {
+      if (c->profiling) throw std::invalid_argument("ensemble: a tank has per-kernel profiling on");
+      c->ensure_initialized();
+    }
+  }
+  void launch_one() {
+    CK(cudaGraphLaunch(exec[next], stream));
+    next ^= 1;
+    for (cryo_ctx* c : tanks) c->cur ^= 1;
+    ++steps_run;
+  }
+  // Head-room for splits, per tank, between steps (sph_solver.cu:556-560).
+  void check_capacity() {
+    leave();
+    for (cryo_ctx* c : tanks) c->check_capacity();
+  }
+  void run(long long n) {
+    if (tanks.empty() || n <= 0) return;
+    prepare();
+    enter();
+    for (long long k = 0; k < n; ++k) {
+      if (!valid()) build();
+      launch_one();
+      if ((k & 15) == 15 && k + 1 < n) {
+        check_capacity();
+        enter();
+      }
+    }
+    check_capacity();
+  }
+  // Device time of `steps` steps with the current branch count (after one
+  // untimed step that also builds the graphs).
+  float time_steps(int steps) {
+    run(1);
+    enter();
+    if (!valid()) build();
+    CK(cudaEventRecord(t0, stream));
+    for (int k = 0; k < steps; ++k) launch_one();
+    CK(cudaEventRecord(t1, stream));
+    check_capacity();
+    CK(cudaEventSynchronize(t1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, t0, t1));
+    return ms / (float)std::max(steps, 1);
+  }
+};
+
+void ensemble_detach(cryo_ensemble* e, cryo_ctx* c) {
+  cudaStreamSynchronize(e->stream);
+  e->drop();
+  e->tanks.erase(std::remove(e->tanks.begin(), e->tanks.end(), c), e->tanks.end());
+  c->ensemble = nullptr;
 }
 
 // ---------------------------------------------------------------------------
@@ -1917,5 +2110,144 @@ int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {
     c->invalidate_graphs();
   });
 }
+
+
+// ------------------------------------------------------------ ensembles
+}  // extern "C"
+namespace {
+template <class F>
+int eguard(cryo_ensemble* e, F&& f) {
+  try {
+    f();
+    return CRYO_OK;
+  } catch (const std::invalid_argument& x) {
+    if (e) e->err = x.what(); else g_create_error = x.what();
+    return CRYO_EINVAL;
+  } catch (const std::out_of_range& x) {
+    if (e) e->err = x.what(); else g_create_error = x.what();
+    return CRYO_ERANGE;
+  } catch (const CudaError& x) {
+    if (e) e->err = x.what(); else g_create_error = x.what();
+    return CRYO_ECUDA;
+  } catch (const std::exception& x) {
+    if (e) e->err = x.what(); else g_create_error = x.what();
+    return CRYO_ERUNTIME;
+  }
+}
+}  // namespace
+extern "C" {
+
+int cryo_ensemble_create(int device, cryo_ensemble** out) {
+  *out = nullptr;
+  cryo_ensemble* e = nullptr;
+  const int rc = eguard(nullptr, [&] {
+    e = new cryo_ensemble;
+    try {
+      e->device = device;
+      CK(cudaSetDevice(device));
+      CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamDefault));
+      CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+      CK(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
+      CK(cudaEventCreate(&e->t0));
+      CK(cudaEventCreate(&e->t1));
+    } catch (...) {
+      delete e;
+      e = nullptr;
+      throw;
+    }
+  });
+  *out = e;
+  return rc;
+}
+
+void cryo_ensemble_destroy(cryo_ensemble* e) { delete e; }
+
+const char* cryo_ensemble_last_error(const cryo_ensemble* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
+
+int cryo_ensemble_add(cryo_ensemble* e, cryo_ctx* c) {
+  return eguard(e, [&] {
+    if (!c) throw std::invalid_argument("ensemble: null tank");
+    if (c->ensemble) throw std::invalid_argument("ensemble: the tank already belongs to an ensemble");
+    if (c->device != e->device) throw std::invalid_argument("ensemble: the tank lives on another device");
+    if (!c->has_particles) throw std::invalid_argument("ensemble: the tank has no particles");
+    if (!c->ens_ev) CK(cudaEventCreateWithFlags(&c->ens_ev, cudaEventDisableTiming));
+    CK(cudaStreamSynchronize(e->stream));
+    e->drop();
+    e->tanks.push_back(c);
+    c->ensemble = e;
+  });
+}
+
+int cryo_ensemble_remove(cryo_ensemble* e, cryo_ctx* c) {
+  return eguard(e, [&] {
+    if (!c || c->ensemble != e) throw std::invalid_argument("ensemble: the tank is not a member");
+    ensemble_detach(e, c);
+  });
+}
+
+int cryo_ensemble_size(cryo_ensemble* e, int* tanks) {
+  return eguard(e, [&] { *tanks = (int)e->tanks.size(); });
+}
+
+int cryo_ensemble_set_chains(cryo_ensemble* e, int chains) {
+  return eguard(e, [&] {
+    if (chains < 0) throw std::invalid_argument("ensemble: chains must be >= 0");
+    e->chains = chains;
+  });
+}
+
+int cryo_ensemble_chains(cryo_ensemble* e, int* chains) {
+  return eguard(e, [&] { *chains = e->branches(); });
+}
+
+int cryo_ensemble_run_steps(cryo_ensemble* e, long long n) {
+  return eguard(e, [&] { e->run(n); });
+}
+
+int cryo_ensemble_step_time(cryo_ensemble* e, int steps, float* ms_per_step) {
+  return eguard(e, [&] {
+    if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
+    *ms_per_step = e->tanks.empty() ? 0.0f : e->time_steps(steps);
+  });
+}
+
+int cryo_ensemble_tune(cryo_ensemble* e, const int* candidates, int ncand, int steps, int* best_chains,
+                       float* best_ms) {
+  return eguard(e, [&] {
+    if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
+    const int t = (int)e->tanks.size();
+    if (t == 0) throw std::invalid_argument("ensemble: no tanks");
+    std::vector<int> cand;
+    if (candidates && ncand > 0) {
+      cand.assign(candidates, candidates + ncand);
+    } else {
+      for (int k = t; k >= 1; k /= 2) cand.push_back(k);
+    }
+    int best = -1;
+    float best_t = 0.0f;
+    for (int k : cand) {
+      if (k < 0) throw std::invalid_argument("ensemble: chain counts must be >= 0");
+      e->chains = k;
+      const float ms = e->time_steps(steps);
+      if (best < 0 || ms < best_t) {
+        best = k;
+        best_t = ms;
+      }
+    }
+    e->chains = best;
+    if (best_chains) *best_chains = best;
+    if (best_ms) *best_ms = best_t;
+  });
+}
+
+int cryo_ensemble_launches_per_step(cryo_ensemble* e, int* launches) {
+  return eguard(e, [&] { *launches = e->step_launches; });
+}
+
+int cryo_ensemble_synchronize(cryo_ensemble* e) {
+  return eguard(e, [&] { CK(cudaStreamSynchronize(e->stream)); });
+}
+
+uintptr_t cryo_ensemble_stream(const cryo_ensemble* e) { return reinterpret_cast<uintptr_t>(e->stream); }
 
 }  // extern "C"

@@ -462,4 +462,33 @@ PYBIND11_MODULE(CryoSPH, m) {
             return to_array(v);
           },
           py::arg("field"), "Raw per-particle field (cryosph_b200.h CRYO_F_*).");
+
+  // Batched stepping (B200 extension): members stay ordinary Solvers.
+  py::class_<Ensemble>(m, "Ensemble",
+                       "Independent tanks advanced together: one graph launch per ensemble step, each member's "
+                       "results identical to stepping it alone.")
+      .def(py::init<int>(), py::arg("device") = 0)
+      .def(
+          "add", [](Ensemble& e, Solver& s) { e.add(s); }, py::arg("solver"), py::keep_alive<1, 2>(),
+          "Adds a Solver with particles loaded (kept alive by the ensemble).")
+      .def("remove", &Ensemble::remove, py::arg("solver"))
+      .def("__len__", &Ensemble::size)
+      .def("run_steps", &Ensemble::run_steps, py::arg("n"), py::call_guard<py::gil_scoped_release>(),
+           "Advances every member by n of its own steps.")
+      .def_property("chains", &Ensemble::chains, &Ensemble::set_chains,
+                    "Concurrent branches the members are spread over (0 = one per member).")
+      .def(
+          "tune",
+          [](Ensemble& e, std::vector<int> candidates, int steps) {
+            py::gil_scoped_release nogil;
+            return e.tune(candidates, steps);
+          },
+          py::arg("candidates") = std::vector<int>{}, py::arg("steps") = 3,
+          "Autotunes the branch count by timing `steps` steps per candidate (these steps advance the members); "
+          "returns (branches, ms per step).")
+      .def("step_time", &Ensemble::step_time, py::arg("steps"), py::call_guard<py::gil_scoped_release>(),
+           "Device ms per ensemble step over `steps` steps (which advance the members).")
+      .def_property_readonly("launches_per_step", &Ensemble::launches_per_step)
+      .def_property_readonly("stream_handle", &Ensemble::stream_handle)
+      .def("diagnostics", &Ensemble::diagnostics, "Diagnostics of every member, in insertion order.");
 }

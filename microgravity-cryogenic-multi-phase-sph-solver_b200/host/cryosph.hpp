@@ -365,6 +365,36 @@ class Solver {
   cryo_ctx* ctx_ = nullptr;
 };
 
+// Batched stepping of independent tanks (no counterpart in the reference):
+// one ensemble step advances every member Solver by one of its own steps in a
+// single graph launch; each member's results equal stepping it alone.
+class Ensemble {
+ public:
+  explicit Ensemble(int device = 0);
+  ~Ensemble();
+  Ensemble(const Ensemble&) = delete;
+  Ensemble& operator=(const Ensemble&) = delete;
+
+  void add(Solver& tank);
+  void remove(Solver& tank);
+  std::size_t size() const;
+  void run_steps(long long n);
+  void set_chains(int chains);  // concurrent branches; 0 = one per member
+  int chains() const;
+  // Times `steps` steps per candidate branch count and keeps the fastest;
+  // returns (branches, ms per step).  The timed steps advance the members.
+  std::pair<int, float> tune(const std::vector<int>& candidates, int steps);
+  float step_time(int steps);
+  int launches_per_step() const;
+  std::uintptr_t stream_handle() const;
+  std::vector<Diagnostics> diagnostics();
+
+ private:
+  void check(int rc) const;
+  cryo_ensemble* e_ = nullptr;
+  std::vector<Solver*> tanks_;
+};
+
 std::string device_name(int device = 0);
 int device_count();
 

@@ -340,6 +340,56 @@ void Solver::load_state(const std::vector<std::uint8_t>& blob) {
   check(cryo_load_state(ctx_, blob.data(), blob.size()));
 }
 
+// ------------------------------------------------------------------ Ensemble
+Ensemble::Ensemble(int device) {
+  const int rc = cryo_ensemble_create(device, &e_);
+  if (rc) raise(rc, cryo_ensemble_last_error(nullptr));
+}
+Ensemble::~Ensemble() { cryo_ensemble_destroy(e_); }
+void Ensemble::check(int rc) const {
+  if (rc) raise(rc, cryo_ensemble_last_error(e_));
+}
+void Ensemble::add(Solver& tank) {
+  check(cryo_ensemble_add(e_, tank.handle()));
+  tanks_.push_back(&tank);
+}
+void Ensemble::remove(Solver& tank) {
+  check(cryo_ensemble_remove(e_, tank.handle()));
+  tanks_.erase(std::remove(tanks_.begin(), tanks_.end(), &tank), tanks_.end());
+}
+std::size_t Ensemble::size() const { return tanks_.size(); }
+void Ensemble::run_steps(long long n) { check(cryo_ensemble_run_steps(e_, n)); }
+void Ensemble::set_chains(int chains) { check(cryo_ensemble_set_chains(e_, chains)); }
+int Ensemble::chains() const {
+  int k = 0;
+  check(cryo_ensemble_chains(e_, &k));
+  return k;
+}
+std::pair<int, float> Ensemble::tune(const std::vector<int>& candidates, int steps) {
+  int best = 0;
+  float ms = 0.0f;
+  check(cryo_ensemble_tune(e_, candidates.empty() ? nullptr : candidates.data(), static_cast<int>(candidates.size()),
+                           steps, &best, &ms));
+  return {best, ms};
+}
+float Ensemble::step_time(int steps) {
+  float ms = 0.0f;
+  check(cryo_ensemble_step_time(e_, steps, &ms));
+  return ms;
+}
+int Ensemble::launches_per_step() const {
+  int k = 0;
+  check(cryo_ensemble_launches_per_step(e_, &k));
+  return k;
+}
+std::uintptr_t Ensemble::stream_handle() const { return cryo_ensemble_stream(e_); }
+std::vector<Diagnostics> Ensemble::diagnostics() {
+  std::vector<Diagnostics> out;
+  out.reserve(tanks_.size());
+  for (Solver* t : tanks_) out.push_back(t->diagnostics());
+  return out;
+}
+
 std::string device_name(int device) {
   char buf[256] = {0};
   if (cryo_device_name(device, buf, sizeof(buf)) != CRYO_OK) return "no CUDA device";
