@@ -73,7 +73,7 @@ size_t particle_bytes(size_t cap) {
   auto r = [&](size_t b) { return (b + a - 1) / a * a; };
   size_t t = 0;
   for (int s = 0; s < 2; ++s) t += 5 * r(cap * 16) + r(cap * 4);    // persistent sets
-  t += 7 * r(cap * 16) + 4 * r(cap * 4);                            // scratch
+  t += 8 * r(cap * 16) + 4 * r(cap * 4);                            // scratch
   t += 5 * r(cap * 4);                                              // sort keys/vals, split flags
   const size_t tiles = (cap + RS_TILE - 1) / RS_TILE + 1;
   t += r((tiles + 1) * RS_BINS * 4);                                // radix histogram + digit totals
@@ -103,7 +103,7 @@ struct cryo_ctx {
   Persist set[2];
   int cur = 0;
   float4 *a4 = nullptr, *ab4 = nullptr, *fw = nullptr, *mw = nullptr, *vwp = nullptr, *ns4 = nullptr,
-         *pc = nullptr;
+         *pc = nullptr, *aux = nullptr;
   float *rmin = nullptr, *wall_w = nullptr, *heat_w = nullptr, *nu_t = nullptr;
   uint32_t *keys_a = nullptr, *keys_b = nullptr, *vals_a = nullptr, *vals_b = nullptr, *split_flag = nullptr;
   uint32_t* hist = nullptr;
@@ -273,6 +273,7 @@ struct cryo_ctx {
     V.id = set[s].id;
     V.a4 = a4; V.ab4 = ab4; V.fw = fw; V.mw = mw; V.vwp = vwp; V.ns4 = ns4; V.pc = pc;
     V.rmin = rmin; V.wall_w = wall_w; V.heat_w = heat_w; V.nu_t = nu_t;
+    V.aux = aux;
     V.cell_begin = cell_begin;
     V.dyn = dyn;
     V.man_t = man_t; V.man_acc = man_acc; V.man_omega = man_omega;
@@ -341,6 +342,7 @@ struct cryo_ctx {
     float4* na4 = a.take<float4>(cap); float4* nab4 = a.take<float4>(cap); float4* nfw = a.take<float4>(cap);
     float4* nmw = a.take<float4>(cap); float4* nvwp = a.take<float4>(cap); float4* nns4 = a.take<float4>(cap);
     float4* npc = a.take<float4>(cap);
+    float4* naux = a.take<float4>(cap);
     float* nrmin = a.take<float>(cap); float* nwall = a.take<float>(cap); float* nheat = a.take<float>(cap);
     float* nnut = a.take<float>(cap);
     uint32_t* nka = a.take<uint32_t>(cap); uint32_t* nkb = a.take<uint32_t>(cap);
@@ -370,13 +372,13 @@ struct cryo_ctx {
         cp(ns[s].nrm, set[s].nrm, 16); cp(ns[s].mrps, set[s].mrps, 16); cp(ns[s].id, set[s].id, 4);
       }
       cp(na4, a4, 16); cp(nab4, ab4, 16); cp(nfw, fw, 16); cp(nmw, mw, 16); cp(nvwp, vwp, 16); cp(nns4, ns4, 16);
-      cp(npc, pc, 16); cp(nrmin, rmin, 4); cp(nwall, wall_w, 4); cp(nheat, heat_w, 4); cp(nnut, nu_t, 4);
+      cp(npc, pc, 16); cp(naux, aux, 16); cp(nrmin, rmin, 4); cp(nwall, wall_w, 4); cp(nheat, heat_w, 4); cp(nnut, nu_t, 4);
       sync();
     }
     arena.release();
     arena = a;
     set[0] = ns[0]; set[1] = ns[1];
-    a4 = na4; ab4 = nab4; fw = nfw; mw = nmw; vwp = nvwp; ns4 = nns4; pc = npc;
+    a4 = na4; ab4 = nab4; fw = nfw; mw = nmw; vwp = nvwp; ns4 = nns4; pc = npc; aux = naux;
     rmin = nrmin; wall_w = nwall; heat_w = nheat; nu_t = nnut;
     keys_a = nka; keys_b = nkb; vals_a = nva; vals_b = nvb; split_flag = nsf;
     hist = nhist; partials = npart; max_chunks = nchunks; diag_out = ndiag; ticket = ntick;
@@ -1734,6 +1736,14 @@ int cryo_pass(cryo_ctx* c, int pass) {
     const Reduce R = c->reduce();
     cudaStream_t st = c->stream;
     const Params& P = c->P;
+    switch (pass) {  // passes that read View::aux get it from the current fields
+      case CRYO_PASS_INTERFACE: case CRYO_PASS_TRANSPORT: case CRYO_PASS_SPS: case CRYO_PASS_MOMENTUM:
+      case CRYO_PASS_CSF: case CRYO_PASS_AKINCI: case CRYO_PASS_DENSITY_RATE: case CRYO_PASS_THERMAL:
+        k_aux<<<G, kBlock, 0, st>>>(P, V);
+        LAUNCH_CHECK();
+        break;
+      default: break;
+    }
     switch (pass) {
       case CRYO_PASS_KICK_DRIFT:
         k_kick_drift<<<G, kBlock, 0, st>>>(P, V, P.density_mode == CRYO_DENSITY_CONTINUITY, P.tvf);

@@ -121,6 +121,7 @@ struct Params {
 // Capacity of the per-particle neighbour list; a particle with more
 // in-support neighbours falls back to the 27-cell scan.
 constexpr int kMaxNbr = 128;
+constexpr int kNbrChunk = 8;  // list entries per 32-byte chunk (kMaxNbr is a multiple)
 
 // Device-resident scalar block: everything the host used to keep between
 // kernel launches (dt, frame state, maxima, FP64 bookkeeping, counts).
@@ -195,6 +196,10 @@ struct View {
   uint32_t* id;
   float4 *a4, *ab4, *fw, *mw, *vwp, *ns4, *pc;
   float *rmin, *wall_w, *heat_w, *nu_t;
+  // per fluid particle {m/rho, 1/sigma, sound speed, 0}: the neighbour
+  // passes' per-pair volume factors, evaluated once per particle with the
+  // same operations (written by the density pass, valid until the kick)
+  float4* aux;
   const int* cell_begin;  // dense cell prefix table, num_cells + 1 entries
   DynState* dyn;
   // maneuver table
@@ -205,8 +210,10 @@ struct View {
   double* partials;   // per-chunk FP64 partials
   unsigned* counters; // last-block tickets
   int capacity;
-  // neighbour lists: nbr[k * capacity + i] = k-th in-support neighbour of i
-  // (reference iteration order), nbr_cnt[i] = count (> kMaxNbr: overflow)
+  // neighbour lists, in chunks of kNbrChunk: the k-th in-support neighbour
+  // of i (reference iteration order) is nbr[((k / 8) * capacity + i) * 8 +
+  // k % 8], so one particle's chunk is one 32-byte sector and a warp's
+  // chunks are contiguous; nbr_cnt[i] = count (> kMaxNbr: overflow)
   int* nbr;
   int* nbr_cnt;
   // ordered phase index lists (built after each reorder)
@@ -308,24 +315,63 @@ __device__ inline int cell_index(const Params& P, V3 p) {
   return (cz * P.ny + cy) * P.nx + cx;
 }
 
+// The 27-cell visit of particle position xi, narrowed without changing what
+// it finds: a (y, z) row of cells whose slab lies beyond the support radius
+// is skipped, and a row's side cells (x -+ 1) are dropped likewise.  Gaps
+// are measured to the faces of xi's own cell, pulled in by a margin that
+// covers the rounding of the cell index (1e-3 of a cell plus 1e-6 per cell
+// of grid extent), so every particle within the support is still visited;
+// particles clamped into a boundary cell from outside the grid lie beyond
+// the face too.  Visit order and accepted set equal the full scan's.
+struct CellWindow {
+  int cx, cy, cz, x0, x1, y0, y1, z0, z1;
+  float glo[3], ghi[3];  // gaps from xi to its own cell's faces, less the margin
+  __device__ CellWindow(const Params& P, V3 xi) {
+    cell_coords(P, xi, cx, cy, cz);
+    z0 = cz > 0 ? cz - 1 : 0; z1 = cz < P.nz - 1 ? cz + 1 : cz;
+    y0 = cy > 0 ? cy - 1 : 0; y1 = cy < P.ny - 1 ? cy + 1 : cy;
+    x0 = cx > 0 ? cx - 1 : 0; x1 = cx < P.nx - 1 ? cx + 1 : cx;
+    const float eps = P.cell * (1e-3f + 1e-6f * (float)(P.nx + P.ny + P.nz));
+    const float o[3] = {P.ox, P.oy, P.oz}, x[3] = {xi.x, xi.y, xi.z};
+    const int c[3] = {cx, cy, cz};
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float face = o[a] + (float)c[a] * P.cell;
+      glo[a] = fmaxf(x[a] - face - eps, 0.0f);
+      ghi[a] = fmaxf(face + P.cell - x[a] - eps, 0.0f);
+    }
+  }
+  // Cells [xs, xe] of row (y, z) that can hold a neighbour; false: none.
+  __device__ bool row(const Params& P, int y, int z, int& xs, int& xe) const {
+    const float gy = y < cy ? glo[1] : (y > cy ? ghi[1] : 0.0f);
+    const float gz = z < cz ? glo[2] : (z > cz ? ghi[2] : 0.0f);
+    const float g2 = gy * gy + gz * gz;
+    if (g2 >= P.support2) return false;
+    xs = x0;
+    xe = x1;
+    if (x0 < cx && glo[0] * glo[0] + g2 >= P.support2) xs = cx;
+    if (x1 > cx && ghi[0] * ghi[0] + g2 >= P.support2) xe = cx;
+    return true;
+  }
+};
+
 // Neighbour iteration (spatial_hash.hpp:37-56).  Cells are key-sorted, so the
 // three x-neighbouring cells of one (y, z) row are one contiguous index range;
-// the 27-cell visit becomes 9 ranges in the reference's z, y, x, j order.
+// the 27-cell visit becomes at most 9 ranges in the reference's z, y, x, j
+// order (CellWindow drops the parts that cannot hold a neighbour).
 // f(j, xj, rij, r2) is called for every j with r2 < support^2 (self included),
 // r2 evaluated as ((dx*dx + dy*dy) + dz*dz) exactly as norm2() does.
 template <class F>
 __device__ inline void for_each_neighbor(const Params& P, const int* __restrict__ cell_begin,
                                          const float4* __restrict__ xp, V3 xi, F&& f) {
-  int cx, cy, cz;
-  cell_coords(P, xi, cx, cy, cz);
-  const int z0 = cz > 0 ? cz - 1 : 0, z1 = cz < P.nz - 1 ? cz + 1 : cz;
-  const int y0 = cy > 0 ? cy - 1 : 0, y1 = cy < P.ny - 1 ? cy + 1 : cy;
-  const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < P.nx - 1 ? cx + 1 : cx;
-  for (int z = z0; z <= z1; ++z) {
-    for (int y = y0; y <= y1; ++y) {
+  const CellWindow W(P, xi);
+  for (int z = W.z0; z <= W.z1; ++z) {
+    for (int y = W.y0; y <= W.y1; ++y) {
+      int xs, xe;
+      if (!W.row(P, y, z, xs, xe)) continue;
       const int row = (z * P.ny + y) * P.nx;
-      const int s = __ldg(cell_begin + row + x0);
-      const int e = __ldg(cell_begin + row + x1 + 1);
+      const int s = __ldg(cell_begin + row + xs);
+      const int e = __ldg(cell_begin + row + xe + 1);
       for (int j = s; j < e; ++j) {
         const float4 xj = __ldg(xp + j);
         const V3 rij = xi - xyz(xj);
@@ -344,19 +390,28 @@ template <class F>
 __device__ inline void for_each_nbr(const Params& P, const View& V, int i, V3 xi, F&& f) {
   const int c = P.use_lists ? __ldg(V.nbr_cnt + i) : kMaxNbr + 1;
   if (c <= kMaxNbr) {
-    const int* __restrict__ list = V.nbr + i;
-    const size_t stride = (size_t)V.capacity;
-    // software pipeline: the next index and position are in flight while the
-    // current neighbour is processed
-    int jn = c > 0 ? __ldg(list) : 0;
+    // the list is read 4 indices (16 bytes) at a time, the next 4 already in
+    // flight; the next neighbour's position is in flight while the current
+    // one is processed
+    const int4* __restrict__ base = reinterpret_cast<const int4*>(V.nbr + (size_t)i * kNbrChunk);
+    const size_t cstride = (size_t)V.capacity * (kNbrChunk / 4);  // chunk stride in int4
+    auto quad = [&](int q) { return __ldg(base + (size_t)(q >> 1) * cstride + (q & 1)); };
+    int4 cur = c > 0 ? quad(0) : make_int4(0, 0, 0, 0);
+    int4 nxt = c > 4 ? quad(1) : make_int4(0, 0, 0, 0);
+    int jn = cur.x;
     float4 xn = c > 0 ? __ldg(V.xp + jn) : make_float4(0, 0, 0, 0);
-    int jnn = c > 1 ? __ldg(list + stride) : 0;
     for (int k = 0; k < c; ++k) {
       const int j = jn;
       const float4 xj = xn;
-      jn = jnn;
-      if (k + 1 < c) xn = __ldg(V.xp + jn);
-      if (k + 2 < c) jnn = __ldg(list + (size_t)(k + 2) * stride);
+      cur.x = cur.y; cur.y = cur.z; cur.z = cur.w;
+      if (((k + 1) & 3) == 0) {
+        cur = nxt;
+        if (k + 5 < c) nxt = quad(((k + 1) >> 2) + 1);
+      }
+      if (k + 1 < c) {
+        jn = cur.x;
+        xn = __ldg(V.xp + jn);
+      }
       const V3 rij = xi - xyz(xj);
       const float r2 = norm2(rij);
       f(j, xj, rij, r2);

@@ -221,10 +221,14 @@ __global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uin
 // the ordered fluid / wall index lists from the gather's chunk offsets.
 __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params P, View V, Reduce R, int mode) {
   __shared__ int wcnt[2][kBlock / 32];
+  // each thread gathers a chunk of kNbrChunk entries here and stores it as
+  // one full 32-byte sector (column per thread: no bank conflicts)
+  __shared__ int stage[kNbrChunk][kBlock];
+#pragma unroll
+  for (int q = 0; q < kNbrChunk; ++q) stage[q][threadIdx.x] = 0;  // the unused tail of a last chunk
   DynState* dyn = V.dyn;
   const int n = dyn->n;
   const int nch = num_chunks(n);
-  const size_t stride = (size_t)V.capacity;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   unsigned overflow = 0;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
@@ -254,25 +258,34 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
     if (!valid) continue;
     const V3 xi = xyz(xpi);
     int cnt = 0;
-    int* list = V.nbr + i;
-    int cx, cy, cz;
-    cell_coords(P, xi, cx, cy, cz);
-    const int z0 = cz > 0 ? cz - 1 : 0, z1 = cz < P.nz - 1 ? cz + 1 : cz;
-    const int y0 = cy > 0 ? cy - 1 : 0, y1 = cy < P.ny - 1 ? cy + 1 : cy;
-    const int x0 = cx > 0 ? cx - 1 : 0, x1 = cx < P.nx - 1 ? cx + 1 : cx;
-    for (int z = z0; z <= z1; ++z) {
-      for (int y = y0; y <= y1; ++y) {
+    const int t = threadIdx.x;
+    int4* chunk = reinterpret_cast<int4*>(V.nbr + (size_t)i * kNbrChunk);
+    const size_t cstride = (size_t)V.capacity * (kNbrChunk / 4);  // in int4
+    auto store_chunk = [&](int q) {
+      int4* dst = chunk + (size_t)q * cstride;
+      dst[0] = make_int4(stage[0][t], stage[1][t], stage[2][t], stage[3][t]);
+      dst[1] = make_int4(stage[4][t], stage[5][t], stage[6][t], stage[7][t]);
+    };
+    const CellWindow W(P, xi);
+    for (int z = W.z0; z <= W.z1; ++z) {
+      for (int y = W.y0; y <= W.y1; ++y) {
+        int xs, xe;
+        if (!W.row(P, y, z, xs, xe)) continue;
         const int row = (z * P.ny + y) * P.nx;
-        const int s = __ldg(V.cell_begin + row + x0);
-        const int e = __ldg(V.cell_begin + row + x1 + 1);
+        const int s = __ldg(V.cell_begin + row + xs);
+        const int e = __ldg(V.cell_begin + row + xe + 1);
         // candidates in groups of LIST_GROUP: all loads issued before the
         // tests, so a thread has that many positions in flight
         auto test = [&](const float4& xj, int j) {
           const V3 rij = xi - xyz(xj);
           const float r2 = norm2(rij);
-          const bool in = r2 < P.support2;
-          if (in && cnt < kMaxNbr) list[(size_t)cnt * stride] = j;
-          cnt += in ? 1 : 0;
+          if (r2 < P.support2) {
+            if (cnt < kMaxNbr) {
+              stage[cnt & (kNbrChunk - 1)][t] = j;
+              if ((cnt & (kNbrChunk - 1)) == kNbrChunk - 1) store_chunk(cnt / kNbrChunk);
+            }
+            ++cnt;
+          }
         };
         int j = s;
         for (; j + LIST_GROUP <= e; j += LIST_GROUP) {
@@ -285,6 +298,7 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
         for (; j < e; ++j) test(__ldg(V.xp + j), j);
       }
     }
+    if (cnt < kMaxNbr && (cnt & (kNbrChunk - 1)) != 0) store_chunk(cnt / kNbrChunk);  // partial last chunk
     V.nbr_cnt[i] = cnt;
     if (cnt > kMaxNbr) overflow = CRYO_DEV_NBR_OVERFLOW;
   }

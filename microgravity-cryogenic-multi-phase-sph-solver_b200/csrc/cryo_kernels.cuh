@@ -121,6 +121,7 @@ __global__ void k_nbr_fill(Params P, View V, const long long* offsets, int* list
 
 // physics (cryo_physics.cu)
 __global__ void k_density(Params P, View V, int fuse_eos);
+__global__ void k_aux(Params P, View V);
 __global__ void k_normalize_masses(Params P, View V);
 __global__ void k_eos(Params P, View V);
 __global__ void k_wall(Params P, View V);
@@ -136,23 +137,24 @@ __global__ void k_forces_t(Params P, View V, int what_rt);
 constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
 // Block shape of the force pass.  The pass is bound by the latency of each
 // particle's neighbour chain, so what matters is how many particles are in
-// flight at once: 64-thread blocks under a 112-register cap (9 per SM) keep
-// 18 warps per SM resident, which covers the 82k fluid particles of the dam
-// break in one wave (256-thread blocks at 117 registers held 16 warps and
-// needed two).
-// Neighbour-list build: candidate positions loaded per group, and the block
-// count per SM the register cap keeps resident.
-#ifndef LIST_GROUP
-#define LIST_GROUP 8
-#endif
-#ifndef LIST_MIN_BLOCKS
-#define LIST_MIN_BLOCKS 4
-#endif
+// flight at once.  Asking for 9 resident 64-thread blocks per SM makes the
+// compiler fit 5 warps in each SM sub-partition's register file (96
+// registers), 20 warps per SM: the 82k fluid particles of the dam break run
+// in one wave.  A 112-register cap fits only 4 warps per sub-partition (16
+// per SM) and needs two waves, 30 % slower there.
 #ifndef FORCES_BLOCK
 #define FORCES_BLOCK 64
 #endif
 #ifndef FORCES_MIN_BLOCKS
 #define FORCES_MIN_BLOCKS 9
+#endif
+// Neighbour-list build: candidate positions loaded per group, and the block
+// count per SM the register cap keeps resident.
+#ifndef LIST_GROUP
+#define LIST_GROUP 4
+#endif
+#ifndef LIST_MIN_BLOCKS
+#define LIST_MIN_BLOCKS 4
 #endif
 __global__ void k_shift_compute(Params P, View V);
 __global__ void k_shift_apply(Params P, View V);

@@ -35,7 +35,21 @@ __global__ void __launch_bounds__(kBlock) k_density(Params P, View V, int fuse_e
       rho = (ph == kLiquid ? V.vt[i].w : mr[0]) * sum;
       mr[1] = rho;
     }
-    if (fuse_eos) mr[2] = eos_pressure(P, ph, rho, V.vT[i].w);
+    const float Ti = V.vT[i].w;
+    if (fuse_eos) mr[2] = eos_pressure(P, ph, rho, Ti);
+    V.aux[i] = make_float4(mr[0] / rho, 1.0f / sum, sound_speed(P, ph, Ti), 0.0f);
+  }
+}
+
+// The per-particle factors of View::aux from the current fields (for
+// operator-level passes run on fields set from outside).
+__global__ void __launch_bounds__(kBlock) k_aux(Params P, View V) {
+  const int n = V.dyn->n;
+  PARTICLE_LOOP(i, n) {
+    const int ph = ph_of(V.xp[i]);
+    if (!is_fluid(ph)) continue;
+    const float4 mr = V.mrps[i];
+    V.aux[i] = make_float4(mr.x / mr.y, 1.0f / mr.w, sound_speed(P, ph, V.vT[i].w), 0.0f);
   }
 }
 
@@ -156,8 +170,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
             if (P.wall_colour) gradc += kernel_gradW(P, rij, r) * (P.vol0 * (nj.w - ci));
             return;
           }
-          const float4 mr = __ldg(V.mrps + j);
-          const float Vj = mr.x / mr.y;
+          const float Vj = __ldg(V.aux + j).x;  // m_j / rho_j
           s_all += Vj * w;
           if (phj != ph) s_other += Vj * w;
           if (j == i) return;
@@ -248,8 +261,7 @@ __global__ void __launch_bounds__(kBlock) k_sps(Params P, View V) {
         Vj = P.vol0;
       } else {
         vj = xyz(__ldg(V.vT + j));
-        const float4 mr = __ldg(V.mrps + j);
-        Vj = mr.x / mr.y;
+        Vj = __ldg(V.aux + j).x;  // m_j / rho_j
       }
       const V3 dv = (vj - vi) * Vj;
       const float dvc[3] = {dv.x, dv.y, dv.z};
@@ -366,6 +378,19 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
     const float ci = sound_speed(P, ph, Ti);
     const float etai = P.mu[pi_idx] + (P.sps ? rhoi * V.nu_t[i] : 0.0f);
     const float alpha_i = ph == kVapor ? P.alpha_av_vap : P.alpha_av;
+    // harmonic viscosity per neighbour phase (navier_stokes.cu:190-196),
+    // evaluated once per particle when it does not vary per neighbour
+    // (0 where eta_i + eta_j = 0: that term is skipped, and a zero term
+    // added to a sum leaves it unchanged)
+    float eta_pair[2] = {0.0f, 0.0f};
+    if (!P.sps) {
+#pragma unroll
+      for (int q = 0; q < 2; ++q) {
+        const float etaj = P.mu[q] + 0.0f;
+        const float eta_sum = etai + etaj;
+        eta_pair[q] = eta_sum > 0.0f ? 2.0f * etai * etaj / eta_sum : 0.0f;
+      }
+    }
 
     // transport (SPH_kernels.cu:61-74)
     const bool do_T = (what & FORCE_TRANSPORT) && P.tvf && !(sigmai < P.tvf_sigma_min) &&
@@ -462,12 +487,13 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
       // fluid neighbour
       const float4 mrj = __ldg(V.mrps + j);
       const float4 vTj = __ldg(V.vT + j);
+      const float4 axj = __ldg(V.aux + j);  // {m_j / rho_j, 1 / sigma_j, c_j}
       const float mj = mrj.x, rhoj = mrj.y;
       if (do_T) {
-        const float Vj = 1.0f / mrj.w;
+        const float Vj = axj.y;
         sumT += gw * (VT_i2 + Vj * Vj);
       }
-      const float Vj = mj / rhoj;
+      const float Vj = axj.x;
       if (what & FORCE_MOMENTUM) {
         const float vsum = Vi2 + Vj * Vj;
         const float pt = (rhoj * pi + rhoi * mrj.z) / (rhoi + rhoj);
@@ -478,16 +504,20 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
           force += Ag * (0.5f * vsum);
         }
         const V3 vij = vi - xyz(vTj);
-        const float etaj = P.mu[phase_index(phj)] + (P.sps ? rhoj * V.nu_t[j] : 0.0f);
-        const float eta_sum = etai + etaj;
-        if (eta_sum > 0.0f && separated) {
-          const float eta_ij = 2.0f * etai * etaj / eta_sum;
-          force += vij * (vsum * eta_ij * dW / r);
+        if (P.sps) {
+          const float etaj = P.mu[phase_index(phj)] + rhoj * V.nu_t[j];
+          const float eta_sum = etai + etaj;
+          if (eta_sum > 0.0f && separated) {
+            const float eta_ij = 2.0f * etai * etaj / eta_sum;
+            force += vij * (vsum * eta_ij * dW / r);
+          }
+        } else if (eta_pair[phase_index(phj)] != 0.0f && separated) {
+          force += vij * (vsum * eta_pair[phase_index(phj)] * dW / r);
         }
         if (alpha_i > 0.0f && phj == ph) {
           const float vr = dot(vij, rij);
           if (vr < 0.0f) {
-            const float cj = sound_speed(P, phj, vTj.w);
+            const float cj = axj.z;
             const float mu_ij = h * vr / (r2 + eta2);
             const float Pi = -alpha_i * 0.5f * (ci + cj) * mu_ij / (0.5f * (rhoi + rhoj));
             acc_av -= gw * (mj * Pi);
