@@ -37,61 +37,79 @@ __device__ inline void neumaier(double& s, double& c, double x) {
   c += fabs(s) >= fabs(x) ? (s - t) + x : (x - t) + s;
   s = t;
 }
+// (s, c) += (s2, c2) for compensated pairs: two-sum of the heads, the
+// rounding error and both tails into the tail.
+__device__ inline void neumaier_pair(double& s, double& c, double s2, double c2) {
+  const double t = s + s2;
+  c += (fabs(s) >= fabs(s2) ? (s - t) + s2 : (s2 - t) + s) + c2;
+  s = t;
+}
 // Sum of value v over chunks [0, nchunks), computed by the whole (last) block
-// in a fixed order: thread t sums chunks t, t + blockDim, ... (compensated),
-// then thread 0 combines the per-thread sums in thread order (compensated).
-// Every thread of the block must call it; the result is valid in thread 0.
+// in a fixed order that depends on nothing but nchunks: thread t sums chunks
+// t, t + blockDim, ... (compensated), the 32 lanes of a warp combine in a
+// fixed down-shift tree, and thread 0 combines the warps in order.  Every
+// thread of the block must call it; the result is valid in thread 0.
 __device__ inline double block_sum_partials(const Reduce& R, int v, int nchunks) {
-  __shared__ double hs[kBlock], hc[kBlock];
+  __shared__ double ws[kBlock / 32], wc[kBlock / 32];
   double s = 0, c = 0;
   const double* p = R.partials + (size_t)v * R.max_chunks;
   for (int k = threadIdx.x; k < nchunks; k += blockDim.x) neumaier(s, c, __ldcg(p + k));
-  hs[threadIdx.x] = s;
-  hc[threadIdx.x] = c;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double s2 = __shfl_down_sync(0xffffffffu, s, o), c2 = __shfl_down_sync(0xffffffffu, c, o);
+    neumaier_pair(s, c, s2, c2);  // lanes >= 32 - o combine garbage that lane 0 never sees
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    ws[warp] = s;
+    wc[warp] = c;
+  }
   __syncthreads();
   double r = 0;
   if (threadIdx.x == 0) {
-    double S = 0, Cc = 0;
-    for (int t = 0; t < (int)blockDim.x; ++t) {
-      neumaier(S, Cc, hs[t]);
-      neumaier(S, Cc, hc[t]);
-    }
-    r = S + Cc;
+    double S = ws[0], C = wc[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) neumaier_pair(S, C, ws[w], wc[w]);
+    r = S + C;
   }
   __syncthreads();
   return r;
 }
 // In-place exclusive scan of the (integral) chunk values of row v by the whole
-// block; returns the total (all threads).
+// block; returns the total (all threads).  Integral doubles add exactly, so
+// the parallel order gives the serial result.
 __device__ inline double block_exclusive_scan(const Reduce& R, int v, int nchunks) {
-  __shared__ double seg[kBlock];
+  __shared__ double wtot[kBlock / 32];
+  __shared__ double total;
   double* p = R.partials + (size_t)v * R.max_chunks;
   const int per = (nchunks + blockDim.x - 1) / blockDim.x;
   const int lo = threadIdx.x * per, hi = min(lo + per, nchunks);
-  double s = 0;
-  for (int k = lo; k < hi; ++k) s += __ldcg(p + k);
-  seg[threadIdx.x] = s;
+  double seg = 0;
+  for (int k = lo; k < hi; ++k) seg += __ldcg(p + k);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  double x = seg;  // inclusive scan over the warp
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const double y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wtot[warp] = x;
   __syncthreads();
   if (threadIdx.x == 0) {
     double run = 0;
-    for (int t = 0; t < (int)blockDim.x; ++t) {
-      const double x = seg[t];
-      seg[t] = run;
-      run += x;
+    for (int w = 0; w < nw; ++w) {
+      const double t = wtot[w];
+      wtot[w] = run;
+      run += t;
     }
+    total = run;
   }
   __syncthreads();
-  double run = seg[threadIdx.x];
+  double run = wtot[warp] + (x - seg);
   for (int k = lo; k < hi; ++k) {
-    const double x = __ldcg(p + k);
+    const double y = __ldcg(p + k);
     p[k] = run;
-    run += x;
+    run += y;
   }
-  __syncthreads();
-  // total = last segment's exclusive prefix + its sum
-  __shared__ double total;
-  if (threadIdx.x == blockDim.x - 1) total = run;
-  __syncthreads();
   const double t = total;
   __syncthreads();
   return t;
