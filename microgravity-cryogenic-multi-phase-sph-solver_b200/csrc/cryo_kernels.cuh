@@ -166,6 +166,14 @@ constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
 #ifndef FORCES_MIN_BLOCKS
 #define FORCES_MIN_BLOCKS 9
 #endif
+// The sub-pass sets with surface tension or heat need ~125 registers; at
+// 8 blocks per SM (4 warps per sub-partition) they run without spilling.
+#ifndef FORCES_MIN_BLOCKS_HEAVY
+#define FORCES_MIN_BLOCKS_HEAVY 8
+#endif
+constexpr int forces_min_blocks(int what) {
+  return (what >= 0 && (what & (FORCE_CSF | FORCE_THERMAL))) ? FORCES_MIN_BLOCKS_HEAVY : FORCES_MIN_BLOCKS;
+}
 // Neighbour-list build: candidate positions loaded per group, and the block
 // count per SM the register cap keeps resident.
 #ifndef LIST_GROUP

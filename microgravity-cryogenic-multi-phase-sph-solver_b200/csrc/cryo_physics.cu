@@ -323,7 +323,7 @@ __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
 // in one neighbour loop.  Each sub-pass reads only what the previous passes
 // wrote, never what this pass writes, so fusing keeps the reference's values.
 template <int WHAT>
-__global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Params P, View V, int what_rt) {
+__global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_forces_t(Params P, View V, int what_rt) {
   // WHAT >= 0: the sub-pass set is a compile-time constant (the step path);
   // -1: read at run time (operator-level calls)
   const int what = WHAT >= 0 ? WHAT : what_rt;
@@ -422,8 +422,12 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
     const bool do_D = (what & FORCE_DRHO) != 0;
     const V3 veli = P.tvf ? xyz(vti4) : vi;
     float div = 0.0f, diff = 0.0f;
-    // thermal
+    // thermal: the harmonic conductivity per neighbour phase
+    // (phase_change.cu:57-61), evaluated once per particle
     const float ki = P.k[pi_idx];
+    float k_pair[2];
+#pragma unroll
+    for (int qq = 0; qq < 2; ++qq) k_pair[qq] = 4.0f * ki * P.k[qq] / (ki + P.k[qq]);
     float q = 0.0f;
 
     for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
@@ -525,7 +529,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
         }
       }
       if (do_C) {
-        const V3 gwC = rij * (dW / r);
+        const V3 gwC = separated ? gw : rij * (dW / r);  // the same product where gw is not zeroed
         const V3 nj = xyz(__ldg(V.ns4 + j));
         if (norm2(nj) > 0.25f) {
           num += Vj * dot(ni - nj, gwC);
@@ -549,8 +553,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, FORCES_MIN_BLOCKS) k_forces_t(Pa
         if (phj == ph) diff += Vj * 2.0f * (rhoj - rhoi) * dot(-rij, gw) / (r2 + eta2);
       }
       if (thermal) {
-        const float kj = P.k[phase_index(phj)];
-        const float kij = 4.0f * ki * kj / (ki + kj);
+        const float kij = k_pair[phase_index(phj)];
         const float rgw = r * dW;
         q += Vi * Vj * kij * (Ti - vTj.w) * rgw / (r2 + eta2);
       }
