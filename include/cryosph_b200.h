@@ -338,13 +338,14 @@ int cryo_set_neighbor_mode(cryo_ctx* ctx, int use_lists);
 /* ------------------------------------------------------------ ensembles
  * Batched stepping of independent tanks; no counterpart in the reference
  * (its perf_scaling.cpp steps one Solver at a time).  Each member keeps its
- * own context; one ensemble step advances every member by one of its own
- * steps in ONE graph launch, with the members spread over `chains`
- * concurrent branches (0 = one branch per member).  A member's results are
- * bit-identical to stepping it alone with cryo_run_steps.  Members must live
- * on the ensemble's device and belong to one ensemble at a time; destroying
- * a member removes it.  The member's own entry points stay usable between
- * ensemble calls (the ensemble orders its stream against theirs). */
+ * own context; an ensemble step advances every member by one of its own
+ * steps.  One graph launch holds `steps_per_launch` such steps, the members
+ * spread over `chains` concurrent branches (0 = one branch per member).  A
+ * member's results are bit-identical to stepping it alone with
+ * cryo_run_steps.  Members must live on the ensemble's device and belong to
+ * one ensemble at a time; destroying a member removes it.  The member's own
+ * entry points stay usable between ensemble calls (the ensemble orders its
+ * stream against theirs). */
 int cryo_ensemble_create(int device, cryo_ensemble** out);
 void cryo_ensemble_destroy(cryo_ensemble* ens);
 const char* cryo_ensemble_last_error(const cryo_ensemble* ens);
@@ -354,17 +355,24 @@ int cryo_ensemble_size(cryo_ensemble* ens, int* tanks);
 int cryo_ensemble_set_chains(cryo_ensemble* ens, int chains);
 /* Branches in use (chains clipped to the member count). */
 int cryo_ensemble_chains(cryo_ensemble* ens, int* chains);
+/* Steps per graph launch: 1, 2, 4, 8 or 16 (runs of other lengths end with
+ * single-step launches). */
+int cryo_ensemble_set_steps_per_launch(cryo_ensemble* ens, int steps);
+int cryo_ensemble_steps_per_launch(cryo_ensemble* ens, int* steps);
 /* n ensemble steps (Solver::run_steps of every member, sph_solver.cu:535-538). */
 int cryo_ensemble_run_steps(cryo_ensemble* ens, long long n);
-/* Device time per ensemble step over `steps` steps (after one untimed step);
- * the steps advance the members. */
+/* Device time per ensemble step over `steps` steps rounded up to whole
+ * launches, after one untimed launch; all of these steps advance the members
+ * (their step counters tell how many). */
 int cryo_ensemble_step_time(cryo_ensemble* ens, int steps, float* ms_per_step);
-/* Autotuner: times `steps` steps for each branch count in candidates[0..n)
- * (NULL: the member count, halved down to 1) and keeps the fastest.  The
- * timed steps advance the members ((steps + 1) per candidate). */
-int cryo_ensemble_tune(cryo_ensemble* ens, const int* candidates, int ncand, int steps, int* best_chains,
+/* Autotuner: times every pair of branch count (chain_candidates; NULL: the
+ * member count halved down to 1) and steps per launch (launch_candidates;
+ * NULL: the current one) with cryo_ensemble_step_time and keeps the
+ * fastest.  The timed steps advance the members. */
+int cryo_ensemble_tune(cryo_ensemble* ens, const int* chain_candidates, int nchain, const int* launch_candidates,
+                       int nlaunch, int steps, int* best_chains, int* best_steps_per_launch,
                        float* best_ms_per_step);
-/* Kernel launches inside one ensemble step graph. */
+/* Kernel launches per ensemble step inside the step graphs. */
 int cryo_ensemble_launches_per_step(cryo_ensemble* ens, int* launches);
 int cryo_ensemble_synchronize(cryo_ensemble* ens);
 uintptr_t cryo_ensemble_stream(const cryo_ensemble* ens);

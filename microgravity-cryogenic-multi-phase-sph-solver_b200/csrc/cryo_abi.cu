@@ -772,24 +772,37 @@ void cryo_ctx::run_until(double t_end) {
 // ---------------------------------------------------------------------------
 // Batched stepping of independent tanks (no counterpart in the reference).
 // Each tank keeps its own context: arena, stream, parameters and step
-// sequence.  One ensemble step is ONE graph launch that holds every tank's
-// step as a chain of that tank's own kernels, spread over `chains` concurrent
-// branches (tanks assigned longest-processing-time first by particle count;
-// one branch per tank by default).  Tanks far too small to fill the GPU alone
-// then run side by side.  Every tank runs exactly the kernels, launch shapes
-// and arguments of its own step graph, so its results are those of stepping
-// it alone, bit for bit.
+// sequence.  A graph launch holds `per_launch` consecutive steps of every
+// tank, each tank's steps a chain of that tank's own kernels, spread over
+// `chains` concurrent branches (tanks assigned longest-processing-time first
+// by particle count; one branch per tank by default).  Tanks far too small
+// to fill the GPU alone then run side by side, and several steps per launch
+// spare the drain at every launch boundary.  Every tank runs exactly the
+// kernels, launch shapes and arguments of its own step graph, so its results
+// are those of stepping it alone, bit for bit.
 struct cryo_ensemble {
+  struct Graphs {  // one launch shape: `steps` steps from either parity
+    cudaGraphExec_t exec[2] = {nullptr, nullptr};
+    int steps = 0;
+    void drop() {
+      for (int k = 0; k < 2; ++k) {
+        if (exec[k]) cudaGraphExecDestroy(exec[k]);
+        exec[k] = nullptr;
+      }
+      steps = 0;
+    }
+  };
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
   std::vector<cryo_ctx*> tanks;
-  int chains = 0;  // 0: one branch per tank
-  cudaGraphExec_t exec[2] = {nullptr, nullptr};
-  std::vector<int> built_cur;  // each tank's ping-pong parity when exec[0] was built
+  int chains = 0;      // 0: one branch per tank
+  int per_launch = 1;  // steps per graph launch (divides 16)
+  Graphs multi, single;
+  std::vector<int> built_cur;  // each tank's ping-pong parity when the graphs were built
   std::vector<unsigned long long> built_gen;
   int built_chains = -1;
-  int next = 0;  // exec launched by the next step
+  int phase = 0;  // steps taken since the build, mod 2
   int step_launches = 0;
   long long steps_run = 0;
   std::string err;
@@ -803,10 +816,8 @@ struct cryo_ensemble {
     if (stream) cudaStreamDestroy(stream);
   }
   void drop() {
-    for (int k = 0; k < 2; ++k) {
-      if (exec[k]) cudaGraphExecDestroy(exec[k]);
-      exec[k] = nullptr;
-    }
+    multi.drop();
+    single.drop();
     built_chains = -1;
   }
   int branches() const {
@@ -814,9 +825,9 @@ struct cryo_ensemble {
     return chains <= 0 ? t : std::min(chains, t);
   }
   bool valid() const {
-    if (!exec[0] || !exec[1] || built_chains != branches()) return false;
+    if (built_chains != branches() || multi.steps != per_launch) return false;
     for (size_t t = 0; t < tanks.size(); ++t)
-      if (tanks[t]->generation != built_gen[t] || tanks[t]->cur != ((built_cur[t] + next) & 1)) return false;
+      if (tanks[t]->generation != built_gen[t] || tanks[t]->cur != ((built_cur[t] + phase) & 1)) return false;
     return true;
   }
   // Tanks per branch: largest first, each to the least-loaded branch.
@@ -837,7 +848,8 @@ struct cryo_ensemble {
     }
     return out;
   }
-  void capture(int q, const std::vector<std::vector<int>>& branches_plan, cudaGraphExec_t* out) {
+  // `steps` steps of every tank starting at parity offset q, as one graph.
+  void capture(int q, int steps, const std::vector<std::vector<int>>& branches_plan, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
     int launches = 0;
@@ -848,9 +860,11 @@ struct cryo_ensemble {
         for (int t : br) {
           cryo_ctx* c = tanks[t];
           CK(cudaStreamWaitEvent(c->stream, prev, 0));
-          const long long c0 = c->launch_counter;
-          c->enqueue_step((built_cur[t] + q) & 1);
-          launches += (int)(c->launch_counter - c0);
+          for (int k = 0; k < steps; ++k) {
+            const long long c0 = c->launch_counter;
+            c->enqueue_step((built_cur[t] + q + k) & 1);
+            launches += (int)(c->launch_counter - c0);
+          }
           CK(cudaEventRecord(c->ens_ev, c->stream));
           prev = c->ens_ev;
         }
@@ -865,7 +879,13 @@ struct cryo_ensemble {
     const cudaError_t e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
     CK(e);
-    step_launches = launches;
+    step_launches = launches / std::max(steps, 1);
+  }
+  void build_shape(Graphs& gr, int steps, const std::vector<std::vector<int>>& pl) {
+    gr.drop();
+    capture(0, steps, pl, &gr.exec[0]);
+    if (steps & 1) capture(1, steps, pl, &gr.exec[1]);  // an even count returns to the start parity
+    gr.steps = steps;
   }
   void build() {
     drop();
@@ -878,10 +898,10 @@ struct cryo_ensemble {
       built_cur[t] = tanks[t]->cur;
       built_gen[t] = tanks[t]->generation;
     }
-    next = 0;
+    phase = 0;
     const auto pl = plan();
-    capture(0, pl, &exec[0]);
-    capture(1, pl, &exec[1]);
+    build_shape(multi, per_launch, pl);
+    if (per_launch > 1) build_shape(single, 1, pl);
     built_chains = branches();
   }
   // tank streams -> ensemble stream, and back
@@ -901,11 +921,13 @@ struct cryo_ensemble {
       c->ensure_initialized();
     }
   }
-  void launch_one() {
-    CK(cudaGraphLaunch(exec[next], stream));
-    next ^= 1;
-    for (cryo_ctx* c : tanks) c->cur ^= 1;
-    ++steps_run;
+  // One launch of `steps` (per_launch or 1) steps of every tank.
+  void launch(int steps) {
+    const Graphs& gr = (steps == per_launch) ? multi : single;
+    CK(cudaGraphLaunch(gr.exec[(steps & 1) ? phase : 0], stream));
+    phase = (phase + steps) & 1;
+    for (cryo_ctx* c : tanks) c->cur = (c->cur + steps) & 1;
+    steps_run += steps;
   }
   // Head-room for splits, per tank, between steps (sph_solver.cu:556-560).
   void check_capacity() {
@@ -916,30 +938,36 @@ struct cryo_ensemble {
     if (tanks.empty() || n <= 0) return;
     prepare();
     enter();
-    for (long long k = 0; k < n; ++k) {
+    long long since_check = 0;
+    while (n > 0) {
       if (!valid()) build();
-      launch_one();
-      if ((k & 15) == 15 && k + 1 < n) {
+      const int k = n >= per_launch ? per_launch : 1;
+      launch(k);
+      n -= k;
+      since_check += k;
+      if (since_check >= 16 && n > 0) {
         check_capacity();
         enter();
+        since_check = 0;
       }
     }
     check_capacity();
   }
-  // Device time of `steps` steps with the current branch count (after one
-  // untimed step that also builds the graphs).
+  // Device time per step over `steps` steps (rounded up to whole launches)
+  // with the current shape, after one untimed launch that also builds it.
   float time_steps(int steps) {
-    run(1);
+    run(per_launch);
     enter();
     if (!valid()) build();
+    const int launches = std::max(1, (steps + per_launch - 1) / per_launch);
     CK(cudaEventRecord(t0, stream));
-    for (int k = 0; k < steps; ++k) launch_one();
+    for (int k = 0; k < launches; ++k) launch(per_launch);
     CK(cudaEventRecord(t1, stream));
     check_capacity();
     CK(cudaEventSynchronize(t1));
     float ms = 0.0f;
     CK(cudaEventElapsedTime(&ms, t0, t1));
-    return ms / (float)std::max(steps, 1);
+    return ms / (float)(launches * per_launch);
   }
 };
 
@@ -2210,6 +2238,18 @@ int cryo_ensemble_chains(cryo_ensemble* e, int* chains) {
   return eguard(e, [&] { *chains = e->branches(); });
 }
 
+int cryo_ensemble_set_steps_per_launch(cryo_ensemble* e, int steps) {
+  return eguard(e, [&] {
+    if (steps < 1 || steps > 16 || (16 % steps) != 0)
+      throw std::invalid_argument("ensemble: steps per launch must be 1, 2, 4, 8 or 16");
+    e->per_launch = steps;
+  });
+}
+
+int cryo_ensemble_steps_per_launch(cryo_ensemble* e, int* steps) {
+  return eguard(e, [&] { *steps = e->per_launch; });
+}
+
 int cryo_ensemble_run_steps(cryo_ensemble* e, long long n) {
   return eguard(e, [&] { e->run(n); });
 }
@@ -2221,31 +2261,39 @@ int cryo_ensemble_step_time(cryo_ensemble* e, int steps, float* ms_per_step) {
   });
 }
 
-int cryo_ensemble_tune(cryo_ensemble* e, const int* candidates, int ncand, int steps, int* best_chains,
-                       float* best_ms) {
+int cryo_ensemble_tune(cryo_ensemble* e, const int* chain_candidates, int nchain, const int* launch_candidates,
+                       int nlaunch, int steps, int* best_chains, int* best_steps_per_launch, float* best_ms) {
   return eguard(e, [&] {
     if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
     const int t = (int)e->tanks.size();
     if (t == 0) throw std::invalid_argument("ensemble: no tanks");
-    std::vector<int> cand;
-    if (candidates && ncand > 0) {
-      cand.assign(candidates, candidates + ncand);
-    } else {
-      for (int k = t; k >= 1; k /= 2) cand.push_back(k);
-    }
-    int best = -1;
-    float best_t = 0.0f;
-    for (int k : cand) {
+    std::vector<int> cc, lc;
+    if (chain_candidates && nchain > 0) cc.assign(chain_candidates, chain_candidates + nchain);
+    else for (int k = t; k >= 1; k /= 2) cc.push_back(k);
+    if (launch_candidates && nlaunch > 0) lc.assign(launch_candidates, launch_candidates + nlaunch);
+    else lc.push_back(e->per_launch);
+    for (int k : cc)
       if (k < 0) throw std::invalid_argument("ensemble: chain counts must be >= 0");
-      e->chains = k;
-      const float ms = e->time_steps(steps);
-      if (best < 0 || ms < best_t) {
-        best = k;
-        best_t = ms;
+    for (int k : lc)
+      if (k < 1 || k > 16 || (16 % k) != 0)
+        throw std::invalid_argument("ensemble: steps per launch must be 1, 2, 4, 8 or 16");
+    int best_c = -1, best_l = 1;
+    float best_t = 0.0f;
+    for (int l : lc)
+      for (int k : cc) {
+        e->chains = k;
+        e->per_launch = l;
+        const float ms = e->time_steps(steps);
+        if (best_c < 0 || ms < best_t) {
+          best_c = k;
+          best_l = l;
+          best_t = ms;
+        }
       }
-    }
-    e->chains = best;
-    if (best_chains) *best_chains = best;
+    e->chains = best_c;
+    e->per_launch = best_l;
+    if (best_chains) *best_chains = best_c;
+    if (best_steps_per_launch) *best_steps_per_launch = best_l;
     if (best_ms) *best_ms = best_t;
   });
 }

@@ -214,7 +214,9 @@ __global__ void __launch_bounds__(kBlock) k_pc_apply(Params P, View V, int gated
     float in_m = 0.0f, in_H = 0.0f;
     if (!(fl & kDying)) {
       for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
-        if (j == i) return;
+        // only flagged sources carry out_m > 0 (pc_source_one), so the
+        // others are passed over without reading their pc record
+        if (j == i || !(fl_of(xj) & kSource)) return;
         const float4 pcj = __ldg(V.pc + j);
         const float om = pcj.x;
         if (!(om > 0.0f)) return;

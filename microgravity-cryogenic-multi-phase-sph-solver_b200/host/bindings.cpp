@@ -477,15 +477,18 @@ PYBIND11_MODULE(CryoSPH, m) {
            "Advances every member by n of its own steps.")
       .def_property("chains", &Ensemble::chains, &Ensemble::set_chains,
                     "Concurrent branches the members are spread over (0 = one per member).")
+      .def_property("steps_per_launch", &Ensemble::steps_per_launch, &Ensemble::set_steps_per_launch,
+                    "Ensemble steps per graph launch (1, 2, 4, 8 or 16).")
       .def(
           "tune",
-          [](Ensemble& e, std::vector<int> candidates, int steps) {
+          [](Ensemble& e, std::vector<int> chains, std::vector<int> steps_per_launch, int steps) {
             py::gil_scoped_release nogil;
-            return e.tune(candidates, steps);
+            return e.tune(chains, steps_per_launch, steps);
           },
-          py::arg("candidates") = std::vector<int>{}, py::arg("steps") = 3,
-          "Autotunes the branch count by timing `steps` steps per candidate (these steps advance the members); "
-          "returns (branches, ms per step).")
+          py::arg("chains") = std::vector<int>{}, py::arg("steps_per_launch") = std::vector<int>{},
+          py::arg("steps") = 3,
+          "Autotunes branch count and steps per launch by timing `steps` steps per candidate pair (these steps "
+          "advance the members); returns (branches, steps per launch, ms per step).")
       .def("step_time", &Ensemble::step_time, py::arg("steps"), py::call_guard<py::gil_scoped_release>(),
            "Device ms per ensemble step over `steps` steps (which advance the members).")
       .def_property_readonly("launches_per_step", &Ensemble::launches_per_step)

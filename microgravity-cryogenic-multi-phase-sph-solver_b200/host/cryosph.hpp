@@ -9,6 +9,7 @@
 #include <limits>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "cryosph_b200.h"
@@ -381,9 +382,13 @@ class Ensemble {
   void run_steps(long long n);
   void set_chains(int chains);  // concurrent branches; 0 = one per member
   int chains() const;
-  // Times `steps` steps per candidate branch count and keeps the fastest;
-  // returns (branches, ms per step).  The timed steps advance the members.
-  std::pair<int, float> tune(const std::vector<int>& candidates, int steps);
+  void set_steps_per_launch(int steps);  // 1, 2, 4, 8 or 16
+  int steps_per_launch() const;
+  // Times `steps` steps per (branch count, steps per launch) candidate and
+  // keeps the fastest; returns (branches, steps per launch, ms per step).
+  // The timed steps advance the members.
+  std::tuple<int, int, float> tune(const std::vector<int>& chain_candidates, const std::vector<int>& launch_candidates,
+                                   int steps);
   float step_time(int steps);
   int launches_per_step() const;
   std::uintptr_t stream_handle() const;

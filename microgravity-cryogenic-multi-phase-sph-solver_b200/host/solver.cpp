@@ -365,12 +365,21 @@ int Ensemble::chains() const {
   check(cryo_ensemble_chains(e_, &k));
   return k;
 }
-std::pair<int, float> Ensemble::tune(const std::vector<int>& candidates, int steps) {
-  int best = 0;
+void Ensemble::set_steps_per_launch(int steps) { check(cryo_ensemble_set_steps_per_launch(e_, steps)); }
+int Ensemble::steps_per_launch() const {
+  int k = 0;
+  check(cryo_ensemble_steps_per_launch(e_, &k));
+  return k;
+}
+std::tuple<int, int, float> Ensemble::tune(const std::vector<int>& chain_candidates,
+                                           const std::vector<int>& launch_candidates, int steps) {
+  int best = 0, per = 0;
   float ms = 0.0f;
-  check(cryo_ensemble_tune(e_, candidates.empty() ? nullptr : candidates.data(), static_cast<int>(candidates.size()),
-                           steps, &best, &ms));
-  return {best, ms};
+  check(cryo_ensemble_tune(e_, chain_candidates.empty() ? nullptr : chain_candidates.data(),
+                           static_cast<int>(chain_candidates.size()),
+                           launch_candidates.empty() ? nullptr : launch_candidates.data(),
+                           static_cast<int>(launch_candidates.size()), steps, &best, &per, &ms));
+  return {best, per, ms};
 }
 float Ensemble::step_time(int steps) {
   float ms = 0.0f;

@@ -68,11 +68,14 @@ def test_branch_counts_and_tuning_keep_bit_identity(cuda_device, tanks, chains):
         ens.add(s)
     ens.chains = chains
     ens.run_steps(4)
-    best, ms = ens.tune([len(tanks), 3, 1], 2)  # 3 x (2 + 1) steps
-    assert best in (len(tanks), 3, 1) and ms > 0
-    ens.run_steps(3)
+    best, per, ms = ens.tune([len(tanks), 3, 1], [1, 2], 2)
+    assert best in (len(tanks), 3, 1) and per in (1, 2) and ms > 0
+    ens.steps_per_launch = 4
+    ens.run_steps(7)  # one 4-step launch, then single steps
+    total = ens_s[0].step_count
+    assert all(s.step_count == total for s in ens_s)
     for s in solo:
-        s.run_steps(4 + 9 + 3)
+        s.run_steps(total)
     for k, (a, b) in enumerate(zip(ens_s, solo)):
         assert same_state(a, b) is None, (k, same_state(a, b))
 
@@ -115,3 +118,5 @@ def test_bad_members_are_refused(cuda_device, tanks):
         other.add(s)  # member of another ensemble
     with pytest.raises(ValueError):
         ens.chains = -1
+    with pytest.raises(ValueError):
+        ens.steps_per_launch = 3
