@@ -53,10 +53,10 @@ SEED = 2002
 
 
 # ----------------------------------------------------------------- workloads
-def workload(name, cs):
-    """(label, SolverConfig, fluid, particle dict, domain lo, hi, config dict for the C ABI)."""
+def workload(name, cs, dx_override=None):
+    """(label, SolverConfig, fluid, particle dict, domain lo, hi)."""
     if name == "dam_break":
-        dx = 0.02
+        dx = dx_override or 0.02
         water = cs.FluidProperties.water()
         water.mu_liquid = 1.0e-3
         cfg = cs.SolverConfig()
@@ -81,16 +81,16 @@ def workload(name, cs):
         p = {k: v[keep] for k, v in p.items()}
         pad = 4 * dx
         lo, hi = (-pad, -0.5 - pad, -pad), (3.22 + pad, 0.5 + pad, 1.0 + pad)
-        label, fluid = "dam_break_spheric2_dx0.02", water
+        label, fluid = f"dam_break_spheric2_dx{dx:g}", water
     elif name in ("c1", "c3"):
         if name == "c1":
             fluid = cs.FluidProperties.liquid_nitrogen()
-            dx, geo, g = 0.004, cs.CylinderTank(0.05, 0.12), (0.0, 0.0, -9.81e-4)
-            label = "c1_ln2_cylinder_dx0.004"
+            dx, geo, g = dx_override or 0.004, cs.CylinderTank(0.05, 0.12), (0.0, 0.0, -9.81e-4)
+            label = f"c1_ln2_cylinder_dx{dx:g}"
         else:
             fluid = cs.FluidProperties.liquid_hydrogen()
-            dx, geo, g = 0.0052, cs.SphereTank(0.5), (0.0, 0.0, -9.81e-4)
-            label = "c3_lh2_sphere_dx0.0052"
+            dx, geo, g = dx_override or 0.0052, cs.SphereTank(0.5), (0.0, 0.0, -9.81e-4)
+            label = f"c3_lh2_sphere_dx{dx:g}"
         cfg = cs.SolverConfig()
         cfg.dx = dx
         cfg.gravity = g
@@ -277,7 +277,9 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=10)
-    ap.add_argument("--workload", default="dam_break")
+    ap.add_argument("--workload", default="dam_break", choices=["dam_break", "c1", "c3", "c4"],
+                    help="c4: only the batched-ensemble comparison (64 tanks), reported as the main line")
+    ap.add_argument("--dx", type=float, default=None, help="lattice spacing override (dam_break, c1, c3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=50)
@@ -296,7 +298,9 @@ def main():
 
     import CryoSPH as cs
 
-    label, cfg, fluid, p, lo, hi = workload(args.workload, cs)
+    if args.workload == "c4":
+        return batched_main(args, cs, rank, world, local)
+    label, cfg, fluid, p, lo, hi = workload(args.workload, cs, args.dx)
     n_total = int(len(p["position"]))
     n_wall = int((p["phase"] == 2).sum())
     n_fluid = n_total - n_wall
@@ -426,6 +430,49 @@ def main():
             "batched": batched,
         }
         print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def batched_main(args, cs, rank, world, local):
+    """--workload c4: the batched ensemble against back-to-back plain solves
+    as the main line (metric: batched particle-steps/s)."""
+    import torch
+    import cryo_shard
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    all_tanks = c4_tanks(cs, count=args.batched_tanks)
+    mine = cryo_shard.shard_of([tk["n"] for tk in all_tanks], rank, world)
+    if dist:
+        dist.barrier()
+    with Clocks(local) as clk:
+        b = batched_run(cs, [all_tanks[t] for t in mine], args.steps, args.warmup, local)
+    agg = torch.tensor([b["ms_per_step"], b["back_to_back_ms_per_step"], 0.0 if b["diagnostics_bit_identical"] else 1.0],
+                       dtype=torch.float64, device=local)
+    if dist:
+        dist.all_reduce(agg, op=dist.ReduceOp.MAX)
+    ms_e, ms_s, differs = (float(v) for v in agg.tolist())
+    n_all = sum(tk["n"] for tk in all_tanks)
+    if rank == 0:
+        clocks = clk.summary()
+        print(json.dumps({
+            "metric": "particle-steps/s/GPU (batched)", "value": n_all / (ms_e / 1e3), "unit": UNIT, "n_gpus": world,
+            "steps": b["steps"], "warmup": args.warmup, "ms_per_step": ms_e, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 fields, f64 reductions", "data": "synthetic",
+            "config": {"workload": b["workload"], "tanks": len(all_tanks), "particles": n_all,
+                       "parallelism": f"tanks sharded x{world}" if world > 1 else "1 GPU",
+                       "l2": "state of all tanks (GBs) exceeds L2", "execution": b["execution"], "seed": SEED},
+            "back_to_back": n_all / (ms_s / 1e3), "back_to_back_ms_per_step": ms_s, "speedup": ms_s / ms_e,
+            "branches": b["branches"], "steps_per_launch": b["steps_per_launch"],
+            "gpu_launches": b["gpu_launches_per_step"] * b["steps"], "diagnostics_bit_identical": differs == 0.0,
+            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+        }))
     if dist:
         dist.barrier()
         dist.destroy_process_group()

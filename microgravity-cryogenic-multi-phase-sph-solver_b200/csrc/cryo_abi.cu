@@ -881,10 +881,11 @@ struct cryo_ensemble {
     CK(e);
     step_launches = launches / std::max(steps, 1);
   }
+  // Graphs for both start parities (a run can reach either before a launch).
   void build_shape(Graphs& gr, int steps, const std::vector<std::vector<int>>& pl) {
     gr.drop();
     capture(0, steps, pl, &gr.exec[0]);
-    if (steps & 1) capture(1, steps, pl, &gr.exec[1]);  // an even count returns to the start parity
+    capture(1, steps, pl, &gr.exec[1]);
     gr.steps = steps;
   }
   void build() {
@@ -924,7 +925,7 @@ struct cryo_ensemble {
   // One launch of `steps` (per_launch or 1) steps of every tank.
   void launch(int steps) {
     const Graphs& gr = (steps == per_launch) ? multi : single;
-    CK(cudaGraphLaunch(gr.exec[(steps & 1) ? phase : 0], stream));
+    CK(cudaGraphLaunch(gr.exec[phase], stream));
     phase = (phase + steps) & 1;
     for (cryo_ctx* c : tanks) c->cur = (c->cur + steps) & 1;
     steps_run += steps;

@@ -80,6 +80,26 @@ def test_branch_counts_and_tuning_keep_bit_identity(cuda_device, tanks, chains):
         assert same_state(a, b) is None, (k, same_state(a, b))
 
 
+@pytest.mark.parametrize("per_launch", [2, 4])
+def test_multi_step_launches_from_either_parity(cuda_device, tanks, per_launch):
+    """Launches of several steps, entered after an odd and after an even
+    number of steps (both ping-pong parities), and a remainder of single steps."""
+    ens_s, solo = solvers(tanks), solvers(tanks)
+    ens = cs.Ensemble(0)
+    for s in ens_s:
+        ens.add(s)
+    ens.steps_per_launch = per_launch
+    ens.run_steps(1)
+    ens.run_steps(2 * per_launch + 1)
+    ens.run_steps(per_launch)
+    n = 1 + 2 * per_launch + 1 + per_launch
+    for s in solo:
+        s.run_steps(n)
+    for k, (a, b) in enumerate(zip(ens_s, solo)):
+        assert a.step_count == n
+        assert same_state(a, b) is None, (k, same_state(a, b))
+
+
 def test_member_stepped_alone_and_removed(cuda_device, tanks):
     ens_s, solo = solvers(tanks), solvers(tanks)
     ens = cs.Ensemble(0)
