@@ -112,8 +112,37 @@ def options():
     return cfg, fl, parts, lo, hi
 
 
+def lh2_sphere():
+    """C3's physics on a small sphere: closed LH2 tank R 0.05 m, fill 0.5,
+    1e-4 g (the BASELINE C3 configuration at R 0.5 m, scaled to a test size)."""
+    fl = cabi.py_fluid(cabi.FLUID_LH2)
+    cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1)
+    parts, lo, hi = tank([(refpy.SPHERE, 0, 0, (0.05, 0, 0))], fl, 0.004, refpy.make_fill(fill_fraction=0.5))
+    return cfg, fl, parts, lo, hi
+
+
+def ln2_boiloff():
+    """C5's physics on a small cylinder: closed LN2 tank R 0.03 m, H 0.075 m,
+    fill 0.5, 2 K superheat, Lee coefficient 5, 20 W heater, 1e-4 g."""
+    fl = cabi.py_fluid(cabi.FLUID_LN2)
+    cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1, lee_evaporation=5, heater_power=20.0)
+    parts, lo, hi = tank([(refpy.CYLINDER, 0, 0, (0.03, 0.075, 0))], fl, 0.004,
+                         refpy.make_fill(fill_fraction=0.5, T_liquid=fl.T_sat + 2))
+    return cfg, fl, parts, lo, hi
+
+
+def lch4_box():
+    """A closed methane tank with superheated liquid (one of the C4 presets)."""
+    fl = cabi.py_fluid(cabi.FLUID_LCH4)
+    cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1, lee_evaporation=2, lee_condensation=2,
+                         velocity_scale=1, contact_angle_deg=20)
+    parts, lo, hi = tank([(refpy.BOX, 0, 0, (0.04, 0.04, 0.04))], fl, 0.004,
+                         refpy.make_fill(fill_fraction=0.3, T_liquid=fl.T_sat + 2))
+    return cfg, fl, parts, lo, hi
+
+
 SCENARIOS = {"c1": c1, "box_split": box_split, "vented": vented, "dam_break": dam_break, "akinci": akinci,
-             "options": options}
+             "options": options, "lh2_sphere": lh2_sphere, "ln2_boiloff": ln2_boiloff, "lch4_box": lch4_box}
 
 
 def normwise(a, b):

@@ -62,7 +62,7 @@ def resync(g, o, fields):
         g.set_field(f, o.field(f))
 
 
-SCEN = ["c1", "box_split", "vented", "dam_break", "akinci", "options"]
+SCEN = ["c1", "box_split", "vented", "dam_break", "akinci", "options", "lh2_sphere", "ln2_boiloff", "lch4_box"]
 
 
 @pytest.mark.parametrize("name", SCEN)
@@ -143,7 +143,7 @@ def test_pass_parity(cuda_device, name):
           max(report, key=lambda r: r[3]) if report else None)
 
 
-@pytest.mark.parametrize("name", ["c1", "box_split", "dam_break", "options"])
+@pytest.mark.parametrize("name", ["c1", "box_split", "dam_break", "options", "lh2_sphere", "ln2_boiloff", "lch4_box"])
 def test_step_parity(cuda_device, name):
     """Whole Solver::step sequences (adaptive dt, graphs) from identical inputs."""
     cfg, g, o = make_pair(name)

@@ -81,7 +81,8 @@ def test_cloud_neighbor_counts_match_brute_force_and_golden():
 
 @needs_ref
 @pytest.mark.parametrize("name,steps", [("c1", 3), ("box_split", 60), ("vented", 20), ("dam_break", 5),
-                                        ("akinci", 10), ("options", 10)])
+                                        ("akinci", 10), ("options", 10), ("lh2_sphere", 5), ("ln2_boiloff", 5),
+                                        ("lch4_box", 20)])
 def test_oracle_bit_identical_to_reference(name, steps):
     cfg, fl, parts, lo, hi = S.SCENARIOS[name]()
     r = refpy.Ref(cfg, fl)
