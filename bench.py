@@ -245,15 +245,17 @@ class Clocks:
 
 
 # ------------------------------------------------------------- reference arm
-def reference_rate(cs_cfg, fluid, p, lo, hi, steps, warmup, budget_s=60.0):
-    """The reference's CPU implementation (oracle/_ref, built from its own
-    sources) on the same workload, all host threads; returns (rate, threads,
-    steps timed, seconds)."""
+def reference_rate(cs_cfg, fluid, p, lo, hi, steps, warmup, budget_s=60.0, cuda=False):
+    """The reference's own implementation (oracle/_ref, built from its own
+    sources) on the same workload: its CPU/OpenMP backend with all host
+    threads, or (cuda=True) its CUDA backend built for sm_100a, wall clock as
+    its perf_scaling.cpp times it; returns (rate, threads, steps timed,
+    seconds)."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import refpy
-    if not refpy.ref_available():
+    if not refpy.ref_available(cuda=cuda):
         return None
-    ref = refpy.Ref(c_config(cs_cfg), c_fluid(fluid))
+    ref = refpy.Ref(c_config(cs_cfg), c_fluid(fluid), cuda=cuda)
     threads = os.cpu_count() or 1
     ref.set_threads(threads)
     arrays = {"x": p["position"], "m": p["mass"], "rho": p["density"], "T": p["temperature"], "phase": p["phase"],
@@ -404,6 +406,14 @@ def main():
             "sharding": "tanks split over ranks longest-processing-time first by particle count" if world > 1 else None,
         })
 
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
+        r = reference_rate(cfg, fluid, p, lo, hi, 2000, 3, budget_s=10.0, cuda=True)
+        if r is not None:
+            rate, _, k, el = r
+            ref_gpu = {"value": rate, "unit": UNIT, "kind": "reference CUDA backend (its own sources, sm_100a)",
+                       "sample": f"{k} steps of {label} after 3 warm-up steps ({el:.1f} s wall clock)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
         r = reference_rate(cfg, fluid, p, lo, hi, 200, 2, budget_s=20.0)
@@ -427,6 +437,7 @@ def main():
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
+            "reference_gpu": ref_gpu,
             "batched": batched,
         }
         print(json.dumps(line))

@@ -25,6 +25,7 @@ import cryo_cabi as cabi  # noqa: E402  (struct layouts of include/cryosph_b200.
 
 REF_LIB = os.path.join(HERE, "_ref", "libcryoref.so")
 REF_LIB64 = os.path.join(HERE, "_ref", "libcryoref64.so")
+REF_LIB_CUDA = os.path.join(HERE, "_ref", "libcryoref_cuda.so")  # make refcuda: the reference's CUDA backend
 ORACLE_LIB = os.path.join(HERE, "libcryo_oracle.so")
 
 # geometry node kinds (ref_driver.h)
@@ -267,8 +268,8 @@ class Ref(_Checker):
     prefix = "ref_"
     has_tank = True
 
-    def __init__(self, cfg, fluid, fp64=False):
-        super().__init__(REF_LIB64 if fp64 else REF_LIB, cfg, fluid)
+    def __init__(self, cfg, fluid, fp64=False, cuda=False):
+        super().__init__(REF_LIB_CUDA if cuda else (REF_LIB64 if fp64 else REF_LIB), cfg, fluid)
 
     def build_tank(self, nodes, fill):
         g = geom(nodes)
@@ -283,8 +284,8 @@ class Ref(_Checker):
         return c, s
 
 
-def ref_available(fp64=False):
-    return os.path.exists(REF_LIB64 if fp64 else REF_LIB)
+def ref_available(fp64=False, cuda=False):
+    return os.path.exists(REF_LIB_CUDA if cuda else (REF_LIB64 if fp64 else REF_LIB))
 
 
 def oracle_available():
