@@ -190,6 +190,31 @@ enum {
 typedef struct cryo_ctx cryo_ctx;
 typedef struct cryo_ensemble cryo_ensemble;
 
+/* Tank geometry for the device lattice generator (geometry.hpp:22-130):
+ * a tree of nodes, children before parents, the last node the root.
+ *   CYLINDER p = {R, H}  CAPSULE p = {R, L}  SPHERE p = {R}  BOX p = {lx, ly, lz}
+ *   TRANSLATED a = child, p = offset   DIFFERENCE / UNION a, b = children
+ * (mesh tanks have no device form: the host generator builds them). */
+enum { CRYO_GEOM_CYLINDER = 0, CRYO_GEOM_CAPSULE = 1, CRYO_GEOM_SPHERE = 2, CRYO_GEOM_BOX = 3,
+       CRYO_GEOM_TRANSLATED = 4, CRYO_GEOM_DIFFERENCE = 5, CRYO_GEOM_UNION = 6 };
+#define CRYO_GEOM_MAX_NODES 32
+typedef struct cryo_geom_node {
+  int kind, a, b;
+  double p[3];
+} cryo_geom_node_t;
+/* FillSpec (geometry.hpp:162-176); NaN temperatures mean T_sat. */
+enum { CRYO_FILL_SETTLED = 0, CRYO_FILL_CENTRAL_BUBBLE = 1, CRYO_FILL_FULL = 2 };
+typedef struct cryo_fill {
+  int mode;
+  double fill_fraction;
+  float settle_direction[3];
+  float bubble_center[3];
+  int include_vapor;
+  int wall_layers;
+  float T_liquid, T_vapor, T_wall;
+  double heater_zmin, heater_zmax;
+} cryo_fill_t;
+
 /* ----------------------------------------------------------- defaults */
 /* Default SolverConfig values (sph_solver.hpp:20-91). */
 void cryo_config_default(cryo_config_t* cfg);
@@ -215,6 +240,17 @@ uintptr_t cryo_stream(const cryo_ctx* ctx);
 /* Solver::set_particles (sph_solver.cu:407-428).  domain_lo/hi: float[3]. */
 int cryo_set_particles(cryo_ctx* ctx, const cryo_host_particles_t* p, const float* domain_lo,
                        const float* domain_hi);
+
+/* Solver::build_tank (sph_solver.cu:430-437) with the lattice generated on
+ * the device: build_tank_particles (geometry.cpp:242-330) evaluated per
+ * lattice node (signed distances in double, the host generator's operations
+ * in its order, so the particles are identical), ordered compaction of walls
+ * and fluid, the liquid/vapour split at an order statistic of the fill key,
+ * and the particles written straight into the solver's arrays.  bounds_lo/hi:
+ * the geometry's AABB (Geometry::bounds); the domain is padded by
+ * (wall_layers + 1) dx as build_tank does. */
+int cryo_build_tank(cryo_ctx* ctx, const cryo_geom_node_t* nodes, int n_nodes, const cryo_fill_t* fill,
+                    const float* bounds_lo, const float* bounds_hi);
 
 /* Solver::step / run_steps / run_until / relax / next_dt (sph_solver.cu:506-543,707-736). */
 int cryo_step(cryo_ctx* ctx);

@@ -396,6 +396,8 @@ struct cryo_ctx {
   // --------------------------------------------------- parameter lowering
   void init_params();
   void configure_grid(const float* lo, const float* hi);
+  void begin_load(int n, bool vapor, const float* lo, const float* hi);
+  void finish_load(int n, uint32_t next_id);
 
   // ------------------------------------------------------ step pieces
   void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
@@ -1186,36 +1188,86 @@ uintptr_t cryo_stream(const cryo_ctx* ctx) { return reinterpret_cast<uintptr_t>(
 
 // Solver::set_particles (sph_solver.cu:407-428) + ParticleSystem::upload
 // (particle_system.cpp:73-93) + SpatialHash::configure.
+// Set-up shared by set_particles and build_tank (sph_solver.cu:407-428 and
+// ParticleSystem::upload, particle_system.cpp:73-93): checks, parameters,
+// capacity and grid for n particles, then (finish_load) the clean scratch and
+// the reset scalar block once the particles are in set[0].
+void cryo_ctx::begin_load(int n, bool vap, const float* lo, const float* hi) {
+  if (vap && cfg.surface_tension == CRYO_ST_AKINCI)
+    throw std::invalid_argument(
+        "Solver: the Akinci surface-tension model is a free-surface (liquid-only) model; use CSF when vapour "
+        "particles are present (FillSpec.include_vapor = false for Akinci runs)");
+  sync();
+  has_vapor = vap;
+  const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
+  float cl = ex;
+  if (cl < ey) cl = ey;
+  if (cl < ez) cl = ez;
+  this->char_length = cl;
+  this->init_params();
+  {
+    const long long cap2 = (long long)((double)n * 2.0);
+    const long long cap = std::max(cap2, (long long)n + 1024);
+    if (cap > (long long)std::numeric_limits<int>::max() / 2) throw std::out_of_range("particle count too large");
+    if (cap > this->capacity) {
+      this->arena.release();
+      this->capacity = 0;
+      this->allocate((int)cap);
+    }
+  }
+  this->configure_grid(lo, hi);
+  this->invalidate_graphs();
+  cur = 0;
+}
+
+void cryo_ctx::finish_load(int n, uint32_t next_id) {
+  cryo_ctx* c = this;
+  // scratch fields start clean (particle_system.cpp:85-88)
+  const size_t cap = (size_t)c->capacity;
+  for (float4* a : {c->a4, c->ab4, c->fw, c->mw, c->vwp, c->ns4, c->pc})
+    CK(cudaMemsetAsync(a, 0, cap * 16, c->stream));
+  for (float* a : {c->wall_w, c->heat_w, c->nu_t}) CK(cudaMemsetAsync(a, 0, cap * 4, c->stream));
+  // scalar block: keep the frame state, reset the rest (sph_solver.cu:419-427)
+  c->pull();
+  DynState& d = *c->hdyn;
+  d.n = n;
+  d.n_alive = n;
+  d.capacity = c->capacity;
+  d.next_id = next_id;
+  d.time = 0;
+  d.last_dt = 0;
+  d.step = 0;
+  d.dt = 0;
+  DynState::Frame& f = c->man_active ? d.fr : c->hframe;
+  set3(f.cfg_gravity, c->cfg.gravity);
+  for (int k = 0; k < 3; ++k) f.gravity[k] = c->cfg.gravity[k] - f.frame_acc[k];
+  d.T_sat = c->fluid.T_sat;
+  d.heat_inv_norm = 0;
+  d.p_ullage = c->fluid.p_sat;
+  d.fluid_volume0 = 0;
+  d.heat_input = 0;
+  d.v_max = d.a_max = d.Tv_max = d.nu_t_max = 0;
+  d.spacing_ratio = 1.0f;
+  d.evaporated = d.condensed = d.vented = d.vented_h = 0;
+  d.merges = d.splits = 0;
+  d.status = 0;
+  d.split_requested = 0;
+  d.damp_after_step = 0;
+  d.damping = 1.0f;
+  d.thermal_on = c->P.thermal;
+  d.phase_change_on = c->cfg.phase_change ? 1 : 0;
+  c->push();
+  c->has_particles = true;
+  c->initialized = false;
+}
+
 int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float* lo, const float* hi) {
   return guard(c, [&] {
     const int n = p->n;
     if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
     bool vap = false;
     for (int i = 0; i < n; ++i) vap |= p->phase[i] == CRYO_VAPOR;
-    if (vap && c->cfg.surface_tension == CRYO_ST_AKINCI)
-      throw std::invalid_argument(
-          "Solver: the Akinci surface-tension model is a free-surface (liquid-only) model; use CSF when vapour "
-          "particles are present (FillSpec.include_vapor = false for Akinci runs)");
-    c->sync();
-    c->has_vapor = vap;
-    const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
-    float cl = ex;
-    if (cl < ey) cl = ey;
-    if (cl < ez) cl = ez;
-    c->char_length = cl;
-    c->init_params();
-    {
-      const long long cap2 = (long long)((double)n * 2.0);
-      const long long cap = std::max(cap2, (long long)n + 1024);
-      if (cap > (long long)std::numeric_limits<int>::max() / 2) throw std::out_of_range("particle count too large");
-      if (cap > c->capacity) {
-        c->arena.release();
-        c->capacity = 0;
-        c->allocate((int)cap);
-      }
-    }
-    c->configure_grid(lo, hi);
-    c->invalidate_graphs();
+    c->begin_load(n, vap, lo, hi);
     // pack the host arrays into the device layout
     std::vector<float4> xp(n), vT(n), vt(n), nrm(n), mrps(n);
     std::vector<uint32_t> id(n);
@@ -1232,7 +1284,6 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
       id[i] = p->id ? p->id[i] : (uint32_t)i;
       next_id = std::max(next_id, id[i] + 1);
     }
-    c->cur = 0;
     const Persist& s = c->set[0];
     CK(cudaMemcpyAsync(s.xp, xp.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(s.vT, vT.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
@@ -1240,43 +1291,203 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
     CK(cudaMemcpyAsync(s.nrm, nrm.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(s.mrps, mrps.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemcpyAsync(s.id, id.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
-    // scratch fields start clean (particle_system.cpp:85-88)
-    const size_t cap = (size_t)c->capacity;
-    for (float4* a : {c->a4, c->ab4, c->fw, c->mw, c->vwp, c->ns4, c->pc})
-      CK(cudaMemsetAsync(a, 0, cap * 16, c->stream));
-    for (float* a : {c->wall_w, c->heat_w, c->nu_t}) CK(cudaMemsetAsync(a, 0, cap * 4, c->stream));
-    // scalar block: keep the frame state, reset the rest (sph_solver.cu:419-427)
-    c->pull();
-    DynState& d = *c->hdyn;
-    d.n = n;
-    d.n_alive = n;
-    d.capacity = c->capacity;
-    d.next_id = next_id;
-    d.time = 0;
-    d.last_dt = 0;
-    d.step = 0;
-    d.dt = 0;
-    DynState::Frame& f = c->man_active ? d.fr : c->hframe;
-    set3(f.cfg_gravity, c->cfg.gravity);
-    for (int k = 0; k < 3; ++k) f.gravity[k] = c->cfg.gravity[k] - f.frame_acc[k];
-    d.T_sat = c->fluid.T_sat;
-    d.heat_inv_norm = 0;
-    d.p_ullage = c->fluid.p_sat;
-    d.fluid_volume0 = 0;
-    d.heat_input = 0;
-    d.v_max = d.a_max = d.Tv_max = d.nu_t_max = 0;
-    d.spacing_ratio = 1.0f;
-    d.evaporated = d.condensed = d.vented = d.vented_h = 0;
-    d.merges = d.splits = 0;
-    d.status = 0;
-    d.split_requested = 0;
-    d.damp_after_step = 0;
-    d.damping = 1.0f;
-    d.thermal_on = c->P.thermal;
-    d.phase_change_on = c->cfg.phase_change ? 1 : 0;
-    c->push();
-    c->has_particles = true;
-    c->initialized = false;
+    c->finish_load(n, next_id);
+  });
+}
+
+// Solver::build_tank with the lattice generated on the device (see
+// cryo_setup.cu).  The lattice range, the liquid cut and the particle
+// constants follow build_tank_particles (geometry.cpp:242-330) operation for
+// operation; the domain is build_tank's (sph_solver.cu:430-437).
+int cryo_build_tank(cryo_ctx* c, const cryo_geom_node_t* nodes, int n_nodes, const cryo_fill_t* fill,
+                    const float* blo, const float* bhi) {
+  return guard(c, [&] {
+    const float dxf = c->cfg.dx;
+    if (!(dxf > 0)) throw std::invalid_argument("build_tank_particles: dx must be > 0");
+    if (fill->wall_layers < 1) throw std::invalid_argument("build_tank_particles: wall_layers must be >= 1");
+    if (fill->fill_fraction < 0 || fill->fill_fraction > 1)
+      throw std::invalid_argument("build_tank_particles: fill_fraction must be in [0, 1]");
+    if (n_nodes < 1 || n_nodes > kGeomNodes)
+      throw std::invalid_argument("build_tank: geometry needs 1 to " + std::to_string(kGeomNodes) + " nodes");
+    // the node tree: children before parents, one parent each, root last
+    std::vector<int> parent(n_nodes, -1);
+    for (int k = 0; k < n_nodes; ++k) {
+      const cryo_geom_node_t& g = nodes[k];
+      if (g.kind < CRYO_GEOM_CYLINDER || g.kind > CRYO_GEOM_UNION) throw std::invalid_argument("build_tank: bad node");
+      const int nch = g.kind == CRYO_GEOM_TRANSLATED ? 1 : (g.kind >= CRYO_GEOM_DIFFERENCE ? 2 : 0);
+      for (int q = 0; q < nch; ++q) {
+        const int ch = q == 0 ? g.a : g.b;
+        if (ch < 0 || ch >= k || parent[ch] >= 0) throw std::invalid_argument("build_tank: the nodes are not a tree");
+        parent[ch] = k;
+      }
+    }
+    for (int k = 0; k + 1 < n_nodes; ++k)
+      if (parent[k] < 0) throw std::invalid_argument("build_tank: every node but the last needs a parent");
+    std::vector<GeomNode> prog(n_nodes);
+    for (int k = 0; k < n_nodes; ++k) {
+      GeomNode& g = prog[k];
+      std::memset(&g, 0, sizeof(g));
+      g.kind = nodes[k].kind;
+      g.a = nodes[k].a;
+      g.b = nodes[k].b;
+      for (int q = 0; q < 3; ++q) g.p[q] = nodes[k].p[q];
+      std::vector<int> chain;  // Translated ancestors, nearest first
+      for (int u = parent[k]; u >= 0; u = parent[u])
+        if (nodes[u].kind == CRYO_GEOM_TRANSLATED) chain.push_back(u);
+      g.nofs = (int)chain.size();
+      for (int f = 0; f < g.nofs; ++f)  // root first
+        for (int q = 0; q < 3; ++q) g.ofs[f][q] = nodes[chain[g.nofs - 1 - f]].p[q];
+    }
+    // lattice (geometry.cpp:255-271)
+    const double h = dxf;
+    const double band = fill->wall_layers * h;
+    Lattice L{};
+    L.i0 = static_cast<int>(std::floor((blo[0] - band) / h)) - 1;
+    L.j0 = static_cast<int>(std::floor((blo[1] - band) / h)) - 1;
+    L.k0 = static_cast<int>(std::floor((blo[2] - band) / h)) - 1;
+    const int i1 = static_cast<int>(std::ceil((bhi[0] + band) / h)) + 1;
+    const int j1 = static_cast<int>(std::ceil((bhi[1] + band) / h)) + 1;
+    const int k1 = static_cast<int>(std::ceil((bhi[2] + band) / h)) + 1;
+    L.nx = i1 - L.i0;
+    L.ny = j1 - L.j0;
+    L.nz = k1 - L.k0;
+    L.total = static_cast<long long>(L.nx) * L.ny * L.nz;
+    L.h = h;
+    L.band = band;
+    if (L.total > 400'000'000LL) throw std::runtime_error("build_tank_particles: lattice too large, increase dx");
+    // particle constants (geometry.cpp:281-285)
+    const cryo_fluid_t& fl = c->fluid;
+    const float vol = dxf * dxf * dxf;
+    FillDev F{};
+    F.mode = fill->mode;
+    F.include_vapor = fill->include_vapor ? 1 : 0;
+    F.m_liq = fl.rho_liquid * vol;
+    F.m_vap = fl.rho_vapor * vol;
+    F.rho_liq = fl.rho_liquid;
+    F.rho_vap = fl.rho_vapor;
+    F.T_liq = std::isnan(fill->T_liquid) ? fl.T_sat : fill->T_liquid;
+    F.T_vap = std::isnan(fill->T_vapor) ? fl.T_sat : fill->T_vapor;
+    F.T_wall = std::isnan(fill->T_wall) ? fl.T_sat : fill->T_wall;
+    F.heater_zmin = fill->heater_zmin;
+    F.heater_zmax = fill->heater_zmax;
+    {  // normalized(settle_direction) (geometry.cpp:17-21, eps 1e-20)
+      const float* d = fill->settle_direction;
+      const float nn = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      for (int q = 0; q < 3; ++q) F.g[q] = nn > 1e-20f ? d[q] / nn : 0.0f;
+      for (int q = 0; q < 3; ++q) F.c[q] = fill->bubble_center[q];
+    }
+    c->sync();
+    cudaStream_t st = c->stream;
+    const long long nb_ll = (L.total + kBlock - 1) / kBlock;
+    const int nb = (int)nb_ll;
+    // device scratch of the set-up (freed at the end of the call)
+    std::vector<void*> tmp;
+    auto take = [&](size_t bytes) {
+      void* q = nullptr;
+      CK(cudaMallocAsync(&q, std::max<size_t>(bytes, 16), st));
+      tmp.push_back(q);
+      return q;
+    };
+    auto release = [&] {
+      for (void* q : tmp) cudaFreeAsync(q, st);
+      tmp.clear();
+    };
+    try {
+      GeomNode* dG = static_cast<GeomNode*>(take(sizeof(GeomNode) * n_nodes));
+      uint8_t* cls = static_cast<uint8_t*>(take((size_t)L.total));
+      uint32_t* cnt_f = static_cast<uint32_t*>(take(sizeof(uint32_t) * nb));
+      uint32_t* cnt_w = static_cast<uint32_t*>(take(sizeof(uint32_t) * nb));
+      unsigned long long* tot = static_cast<unsigned long long*>(take(4 * sizeof(unsigned long long)));
+      unsigned long long htot[4] = {0, 0, 0, 0};
+      CK(cudaMemcpyAsync(dG, prog.data(), sizeof(GeomNode) * n_nodes, cudaMemcpyHostToDevice, st));
+      k_lattice_classify<<<nb, kBlock, 0, st>>>(dG, n_nodes, L, cls, cnt_f, cnt_w);
+      LAUNCH_CHECK();
+      k_scan_counts<<<1, 1024, 0, st>>>(cnt_f, nb, tot);
+      LAUNCH_CHECK();
+      k_scan_counts<<<1, 1024, 0, st>>>(cnt_w, nb, tot + 1);
+      LAUNCH_CHECK();
+      CK(cudaMemcpyAsync(htot, tot, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      c->sync();
+      const long long nf = (long long)htot[0], nw = (long long)htot[1];
+      if (nf == 0) throw std::runtime_error("build_tank_particles: no fluid particles; dx too large?");
+      if (nf + nw > (long long)std::numeric_limits<int>::max() / 4) throw std::out_of_range("particle count too large");
+      long long* fluid_nodes = static_cast<long long*>(take(sizeof(long long) * nf));
+      long long* wall_nodes = static_cast<long long*>(take(sizeof(long long) * std::max(nw, 1LL)));
+      k_lattice_scatter<<<nb, kBlock, 0, st>>>(L, cls, cnt_f, cnt_w, fluid_nodes, wall_nodes);
+      LAUNCH_CHECK();
+      // liquid cut: the n_liq-th largest fill key (geometry.cpp:308-323)
+      const int nfi = (int)nf;
+      const int gb = std::max(1, std::min((nfi + kBlock - 1) / kBlock, c->sm_count * 8));
+      F.any_liquid = 1;
+      if (fill->mode != CRYO_FILL_FULL) {
+        const long long n_liq = std::llround(fill->fill_fraction * static_cast<double>(nf));
+        if (n_liq <= 0) {
+          F.any_liquid = 0;
+        } else {
+          uint32_t* keys = static_cast<uint32_t*>(take(sizeof(uint32_t) * nf));
+          unsigned int* hist = static_cast<unsigned int*>(take(256 * sizeof(unsigned int)));
+          k_fill_keys<<<gb, kBlock, 0, st>>>(L, F, fluid_nodes, nfi, keys);
+          LAUNCH_CHECK();
+          long long r = nf - n_liq;  // rank from the smallest
+          uint32_t prefix = 0, mask = 0;
+          unsigned int hh[256];
+          for (int shift = 24; shift >= 0; shift -= 8) {
+            CK(cudaMemsetAsync(hist, 0, 256 * sizeof(unsigned int), st));
+            k_key_digits<<<gb, kBlock, 0, st>>>(keys, nfi, prefix, mask, shift, hist);
+            LAUNCH_CHECK();
+            CK(cudaMemcpyAsync(hh, hist, sizeof(hh), cudaMemcpyDeviceToHost, st));
+            c->sync();
+            int d = 0;
+            for (; d < 255; ++d) {
+              if (r < (long long)hh[d]) break;
+              r -= hh[d];
+            }
+            prefix |= (uint32_t)d << shift;
+            mask |= 0xffu << shift;
+          }
+          const uint32_t bits = (prefix & 0x80000000u) ? (prefix & 0x7fffffffu) : ~prefix;
+          float kf;
+          std::memcpy(&kf, &bits, sizeof(kf));
+          F.cut = static_cast<double>(kf) - 1e-6 * h;
+        }
+      }
+      uint8_t* liquid = static_cast<uint8_t*>(take((size_t)nf));
+      const int nbf = (nfi + kBlock - 1) / kBlock;
+      uint32_t* cnt_keep = static_cast<uint32_t*>(take(sizeof(uint32_t) * nbf));
+      uint32_t* cnt_liq = static_cast<uint32_t*>(take(sizeof(uint32_t) * nbf));
+      k_fill_split<<<nbf, kBlock, 0, st>>>(L, F, fluid_nodes, nfi, liquid, cnt_keep, cnt_liq);
+      LAUNCH_CHECK();
+      k_scan_counts<<<1, 1024, 0, st>>>(cnt_keep, nbf, tot + 2);
+      LAUNCH_CHECK();
+      k_scan_counts<<<1, 1024, 0, st>>>(cnt_liq, nbf, tot + 3);
+      LAUNCH_CHECK();
+      CK(cudaMemcpyAsync(htot, tot, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+      c->sync();
+      const int kept = (int)htot[2], n_liquid = (int)htot[3];
+      const int n = (int)nw + kept;
+      const bool vapor = kept > n_liquid;
+      float lo[3], hi[3];  // build_tank's domain (sph_solver.cu:433-435)
+      const float pad = (fill->wall_layers + 1) * dxf;
+      for (int q = 0; q < 3; ++q) {
+        lo[q] = blo[q] - pad;
+        hi[q] = bhi[q] + pad;
+      }
+      c->begin_load(n, vapor, lo, hi);
+      const View V = c->view(0);
+      const int gw = std::max(1, std::min((int)((nw + kBlock - 1) / kBlock), c->sm_count * 8));
+      if (nw > 0) {
+        k_emit_walls<<<gw, kBlock, 0, st>>>(dG, n_nodes, L, F, wall_nodes, (int)nw, V);
+        LAUNCH_CHECK();
+      }
+      k_emit_fluid<<<nbf, kBlock, 0, st>>>(L, F, fluid_nodes, nfi, liquid, cnt_keep, (int)nw, V);
+      LAUNCH_CHECK();
+      c->finish_load(n, (uint32_t)n);
+      release();
+      c->sync();
+    } catch (...) {
+      release();
+      throw;
+    }
   });
 }
 

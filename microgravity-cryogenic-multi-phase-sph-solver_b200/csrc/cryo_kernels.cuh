@@ -218,4 +218,43 @@ __global__ void k_telemetry_pack(View V, TelemetryRecord* out);
 // Number of FP64 values per chunk of the diagnostics reduction.
 constexpr int kDiagValues = 30;
 
+// tank lattice generator (cryo_setup.cu)
+constexpr int kGeomNodes = CRYO_GEOM_MAX_NODES;
+// One geometry node with the offsets of its Translated ancestors, root first
+// (applied to the query point in that order, as the nested sdf calls do).
+struct GeomNode {
+  int kind, a, b, nofs;
+  double p[3];
+  double ofs[kGeomNodes][3];
+};
+// Lattice nodes at ((i0 + i + 1/2) h, ...), i < nx, ...; band = wall_layers h.
+struct Lattice {
+  int i0, j0, k0, nx, ny, nz;
+  long long total;
+  double h, band;
+};
+// Fill of the generated tank: key direction or centre, the liquid cut, the
+// per-phase mass, density and temperature, the heater band.
+struct FillDev {
+  int mode, include_vapor, any_liquid;
+  float g[3], c[3];
+  double cut;
+  float m_liq, m_vap, rho_liq, rho_vap, T_liq, T_vap, T_wall;
+  double heater_zmin, heater_zmax;
+};
+__global__ void k_lattice_classify(const GeomNode* G, int ng, Lattice L, uint8_t* cls, uint32_t* cnt_f,
+                                   uint32_t* cnt_w);
+__global__ void k_scan_counts(uint32_t* cnt, int n, unsigned long long* total);
+__global__ void k_lattice_scatter(Lattice L, const uint8_t* cls, const uint32_t* off_f, const uint32_t* off_w,
+                                  long long* fluid_nodes, long long* wall_nodes);
+__global__ void k_fill_keys(Lattice L, FillDev F, const long long* fluid_nodes, int nf, uint32_t* keys);
+__global__ void k_key_digits(const uint32_t* keys, int n, uint32_t prefix, uint32_t mask, int shift,
+                             unsigned int* hist);
+__global__ void k_fill_split(Lattice L, FillDev F, const long long* fluid_nodes, int nf, uint8_t* liquid,
+                             uint32_t* cnt_keep, uint32_t* cnt_liq);
+__global__ void k_emit_walls(const GeomNode* G, int ng, Lattice L, FillDev F, const long long* wall_nodes, int nw,
+                             View V);
+__global__ void k_emit_fluid(Lattice L, FillDev F, const long long* fluid_nodes, int nf, const uint8_t* liquid,
+                             const uint32_t* off_keep, int nw, View V);
+
 }  // namespace cryo

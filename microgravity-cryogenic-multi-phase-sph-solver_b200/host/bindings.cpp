@@ -351,8 +351,9 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def(py::init<const SolverConfig&, const FluidProperties&, int>(), py::arg("config"), py::arg("fluid"),
            py::arg("device") = 0)
       .def(
-          "build_tank", [](Solver& s, const Geometry& g, const FillSpec& f) { s.build_tank(g, f); }, py::arg("geometry"),
-          py::arg("fill") = FillSpec{}, "Generates wall/liquid/vapour particles for a tank.")
+          "build_tank", [](Solver& s, const Geometry& g, const FillSpec& f, bool on_device) { s.build_tank(g, f, on_device); },
+          py::arg("geometry"), py::arg("fill") = FillSpec{}, py::arg("on_device") = true,
+          "Generates wall/liquid/vapour particles for a tank (on the GPU for analytic and CSG tanks).")
       .def(
           "set_particles",
           [](Solver& s, DArr position, DArr mass, DArr density, DArr temperature, U8Arr phase, const Tuple3& domain_lo,

@@ -165,10 +165,14 @@ class Geometry {
   virtual std::string name() const = 0;
   virtual double volume() const { return -1.0; }
   Vec3 outward_normal(double x, double y, double z, double eps) const;
+  // Appends this geometry's node tree for the device lattice generator
+  // (children first) and returns the root's index; -1: no device form.
+  virtual int emit_nodes(std::vector<cryo_geom_node_t>& out) const { (void)out; return -1; }
 };
 
 class CylinderTank final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   CylinderTank(double radius, double height);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -183,6 +187,7 @@ class CylinderTank final : public Geometry {
 
 class CapsuleTank final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   CapsuleTank(double radius, double length);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -195,6 +200,7 @@ class CapsuleTank final : public Geometry {
 
 class SphereTank final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   explicit SphereTank(double radius);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -207,6 +213,7 @@ class SphereTank final : public Geometry {
 
 class BoxTank final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   BoxTank(double lx, double ly, double lz);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -219,6 +226,7 @@ class BoxTank final : public Geometry {
 
 class Translated final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   Translated(std::shared_ptr<const Geometry> g, Vec3 offset);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -232,6 +240,7 @@ class Translated final : public Geometry {
 
 class Difference final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   Difference(std::shared_ptr<const Geometry> a, std::shared_ptr<const Geometry> b);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override { return a_->bounds(); }
@@ -243,6 +252,7 @@ class Difference final : public Geometry {
 
 class Union final : public Geometry {
  public:
+  int emit_nodes(std::vector<cryo_geom_node_t>& out) const override;
   Union(std::shared_ptr<const Geometry> a, std::shared_ptr<const Geometry> b);
   double sdf(double x, double y, double z) const override;
   AABB bounds() const override;
@@ -309,7 +319,9 @@ class Solver {
   Solver& operator=(const Solver&) = delete;
 
   void set_particles(const HostParticles& particles, const AABB& domain);
-  void build_tank(const Geometry& geometry, const FillSpec& fill);
+  // on_device: generate the lattice on the GPU where the geometry has a
+  // device form (the particles are the same as the host generator's)
+  void build_tank(const Geometry& geometry, const FillSpec& fill, bool on_device = true);
 
   void step();
   void run_steps(long long n);

@@ -148,6 +148,48 @@ AABB Union::bounds() const {
           Vec3{std::max(p.hi.x, q.hi.x), std::max(p.hi.y, q.hi.y), std::max(p.hi.z, q.hi.z)}};
 }
 
+// Device forms of the analytic shapes (cryo_geom_node_t); the same doubles
+// the shapes evaluate with (a box by its full side lengths).
+namespace {
+int push_node(std::vector<cryo_geom_node_t>& out, int kind, int a, int b, double p0, double p1, double p2) {
+  cryo_geom_node_t n{};
+  n.kind = kind;
+  n.a = a;
+  n.b = b;
+  n.p[0] = p0;
+  n.p[1] = p1;
+  n.p[2] = p2;
+  out.push_back(n);
+  return static_cast<int>(out.size()) - 1;
+}
+}  // namespace
+int CylinderTank::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  return push_node(out, CRYO_GEOM_CYLINDER, -1, -1, R_, H_, 0.0);
+}
+int CapsuleTank::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  return push_node(out, CRYO_GEOM_CAPSULE, -1, -1, R_, L_, 0.0);
+}
+int SphereTank::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  return push_node(out, CRYO_GEOM_SPHERE, -1, -1, R_, 0.0, 0.0);
+}
+int BoxTank::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  return push_node(out, CRYO_GEOM_BOX, -1, -1, 2.0 * hx_, 2.0 * hy_, 2.0 * hz_);
+}
+int Translated::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  const int a = g_->emit_nodes(out);
+  return a < 0 ? -1 : push_node(out, CRYO_GEOM_TRANSLATED, a, -1, ox_, oy_, oz_);
+}
+int Difference::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  const int a = a_->emit_nodes(out);
+  const int b = a < 0 ? -1 : b_->emit_nodes(out);
+  return b < 0 ? -1 : push_node(out, CRYO_GEOM_DIFFERENCE, a, b, 0.0, 0.0, 0.0);
+}
+int Union::emit_nodes(std::vector<cryo_geom_node_t>& out) const {
+  const int a = a_->emit_nodes(out);
+  const int b = a < 0 ? -1 : b_->emit_nodes(out);
+  return b < 0 ? -1 : push_node(out, CRYO_GEOM_UNION, a, b, 0.0, 0.0, 0.0);
+}
+
 // Wavefront OBJ: "v x y z" and "f a b c ..." records (polygons fanned from the
 // first vertex; "i/t/n" forms and negative relative indices accepted).
 void load_obj(const std::string& path, std::vector<std::array<double, 3>>& vertices,

@@ -143,7 +143,30 @@ void Solver::set_particles(const HostParticles& hp, const AABB& domain) {
 }
 
 // Solver::build_tank (sph_solver.cu:430-437)
-void Solver::build_tank(const Geometry& geometry, const FillSpec& fill) {
+void Solver::build_tank(const Geometry& geometry, const FillSpec& fill, bool on_device) {
+  std::vector<cryo_geom_node_t> nodes;
+  if (on_device && geometry.emit_nodes(nodes) >= 0 && nodes.size() <= CRYO_GEOM_MAX_NODES) {
+    // the lattice generated on the GPU (identical particles; mesh tanks and
+    // larger trees take the host generator below)
+    cryo_fill_t f{};
+    f.mode = static_cast<int>(fill.mode);
+    f.fill_fraction = fill.fill_fraction;
+    put3(f.settle_direction, fill.settle_direction);
+    put3(f.bubble_center, fill.bubble_center);
+    f.include_vapor = fill.include_vapor ? 1 : 0;
+    f.wall_layers = fill.wall_layers;
+    f.T_liquid = fill.T_liquid;
+    f.T_vapor = fill.T_vapor;
+    f.T_wall = fill.T_wall;
+    f.heater_zmin = fill.heater_zmin;
+    f.heater_zmax = fill.heater_zmax;
+    const AABB b = geometry.bounds();
+    float lo[3], hi[3];
+    put3(lo, b.lo);
+    put3(hi, b.hi);
+    check(cryo_build_tank(ctx_, nodes.data(), static_cast<int>(nodes.size()), &f, lo, hi));
+    return;
+  }
   const HostParticles hp = build_tank_particles(geometry, fluid_, cfg_.dx, fill);
   AABB dom = geometry.bounds();
   const real pad = (fill.wall_layers + 1) * cfg_.dx;
