@@ -222,6 +222,24 @@ struct View {
 };
 
 // --------------------------------------------------------- SPH kernels
+// Single-precision pow, cos, sin and cbrt as the reference's CPU build gets
+// them: from the C library, which returns the correctly rounded value for
+// nearly every argument (all but ~2e-4 of the powf and ~1e-2 of the cosf /
+// sinf arguments these passes see; cbrtf misses more often).  The device
+// takes the correctly rounded value from the double-precision function,
+// which matches the library far more often than CUDA's single-precision
+// versions (2 ulp); a mismatch moves one result by one ulp.
+__host__ __device__ inline float pow_cr(float x, float y) {
+#ifdef __CUDA_ARCH__
+  return (float)pow((double)x, (double)y);
+#else
+  return powf(x, y);
+#endif
+}
+__device__ inline float cos_cr(float x) { return (float)cos((double)x); }
+__device__ inline float sin_cr(float x) { return (float)sin((double)x); }
+__device__ inline float cbrt_cr(float x) { return (float)cbrt((double)x); }
+
 // kernel_W / kernel_dWdr / kernel_gradW (SPH_kernels.cuh:34-64)
 __host__ __device__ inline float kernel_W(const Params& P, float r) {
   const float q = r * P.inv_h;
@@ -265,7 +283,7 @@ __host__ __device__ inline float akinci_adhesion(float r, float c) {
   if (r >= c || 2.0f * r <= c) return 0.0f;
   const float arg = -4.0f * r * r / c + 6.0f * r - 2.0f * c;
   if (arg <= 0.0f) return 0.0f;
-  return 0.007f / powf(c, 3.25f) * powf(arg, 0.25f);
+  return 0.007f / pow_cr(c, 3.25f) * pow_cr(arg, 0.25f);
 }
 
 // EOS and enthalpy (sim_params.cuh:100-135)
@@ -280,7 +298,7 @@ __device__ inline float eos_pressure(const Params& P, int ph, float rho, float T
       const float r2 = ratio * ratio;
       r_g = r2 * r2 * r2 * ratio;
     } else {
-      r_g = powf(ratio, P.tait_gamma);
+      r_g = pow_cr(ratio, P.tait_gamma);
     }
     p = P.tait_B * (r_g - 1.0f) + P.p_bg;
   }

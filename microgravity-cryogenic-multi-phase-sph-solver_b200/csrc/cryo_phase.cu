@@ -349,7 +349,7 @@ __device__ inline V3 random_direction(uint32_t id, uint32_t seed) {  // phase_ch
   const float u = 2.0f * hash_unit(id * 2654435761u ^ seed) - 1.0f;
   const float phi = 2.0f * kPi * hash_unit(hash_u32(id + 0x9e3779b9u) ^ (seed * 747796405u));
   const float s = sqrtf(1.0f - u * u > 0.0f ? 1.0f - u * u : 0.0f);
-  return V3{s * cosf(phi), s * sinf(phi), u};
+  return V3{s * cos_cr(phi), s * sin_cr(phi), u};
 }
 
 __global__ void __launch_bounds__(kBlock) k_split(Params P, View V, Reduce R, const uint32_t* __restrict__ flag,
@@ -398,9 +398,9 @@ __global__ void __launch_bounds__(kBlock) k_split(Params P, View V, Reduce R, co
       const V3 nn = gc / gm;
       const V3 t = e - nn * dot(e, nn);
       e = normalized(t - nn * 0.5f);
-      xd = xi + e * (0.5f * cbrtf(vol));
+      xd = xi + e * (0.5f * cbrt_cr(vol));
     } else {
-      const float delta = 0.25f * cbrtf(vol);
+      const float delta = 0.25f * cbrt_cr(vol);
       xd = xi + e * delta;
       const V3 xn = xi - e * delta;
       xp.x = xn.x;
