@@ -636,7 +636,8 @@ def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vap
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic(top[0], label)
     return {"kernel": top[0], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "algorithmic_bytes": alg, "avg_launch_ms": avg_ms,
+            "frac": achieved / peak, "traffic": traffic, "ncu_utilisation": ncu_utilisation(top[0], label),
+            "algorithmic_bytes": alg, "avg_launch_ms": avg_ms,
             "share": top[1] / total if total else None, "peak_source": "measured" if peaks else "fallback",
             "kernels": {r[0]: {"ms_per_step": r[1] / steps, "launches": r[2]} for r in sorted(rows, key=lambda r: -r[1])}}
 
@@ -648,6 +649,17 @@ def cfg_dict(cfg):
         v = getattr(cfg, k)
         out[k] = int(v.value) if hasattr(v, "value") else int(v)
     return out
+
+
+def ncu_utilisation(kernel, label):
+    """Issue-slot, FMA-pipe, L1 and DRAM utilisation of `kernel` from the
+    committed ncu capture (the neighbour passes are bound by issue and
+    latency, not HBM; null if absent)."""
+    try:
+        with open(os.path.join(REPO, "profiles", "ncu_dram.json")) as fh:
+            return json.load(fh).get("utilisation", {}).get(label, {}).get(kernel)
+    except (OSError, ValueError):
+        return None
 
 
 def ncu_traffic(kernel, label):
