@@ -225,10 +225,12 @@ struct View {
 // Single-precision pow, cos, sin and cbrt as the reference's CPU build gets
 // them: from the C library, which returns the correctly rounded value for
 // nearly every argument (all but ~2e-4 of the powf and ~1e-2 of the cosf /
-// sinf arguments these passes see; cbrtf misses more often).  The device
-// takes the correctly rounded value from the double-precision function,
-// which matches the library far more often than CUDA's single-precision
-// versions (2 ulp); a mismatch moves one result by one ulp.
+// sinf arguments these passes see; cbrtf misses more often).  These device
+// versions take the correctly rounded value from the double-precision
+// function (CUDA's single-precision versions are within 2 ulp).  The force
+// pass keeps CUDA's powf for the transport-velocity wall volume: the double
+// code inlined there cost the whole pass 20 % (registers), and that path
+// matched the library no less often in the runs compared.
 __host__ __device__ inline float pow_cr(float x, float y) {
 #ifdef __CUDA_ARCH__
   return (float)pow((double)x, (double)y);

@@ -7,7 +7,10 @@
 namespace cryo {
 
 constexpr int RS_THREADS = 256;
-constexpr int RS_TILE = 4096;  // keys per radix tile (16 per thread)
+#ifndef RS_TILE_KEYS
+#define RS_TILE_KEYS 1024
+#endif
+constexpr int RS_TILE = RS_TILE_KEYS;  // keys per radix tile (RS_TILE / RS_THREADS per thread)
 constexpr int RS_BITS = 8;
 constexpr int RS_BINS = 1 << RS_BITS;
 constexpr int RS_SCAN_THREADS = 256;

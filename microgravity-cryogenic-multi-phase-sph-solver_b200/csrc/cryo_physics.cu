@@ -446,7 +446,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
             rho_w = (vwj.w - (P.p_bg - P.vapor_K)) / (P.gas_R * Ti);
           } else {
             const float ratio = (mrj.z - P.p_bg) / P.tait_B + 1.0f;
-            rho_w = P.rho0[0] * pow_cr(ratio > 0.5f ? ratio : 0.5f, inv_gamma);
+            rho_w = P.rho0[0] * powf(ratio > 0.5f ? ratio : 0.5f, inv_gamma);
           }
           const float Vj = rho_w > 0.0f ? VT_i * rhoi / rho_w : VT_i;
           sumT += gw * (VT_i2 + Vj * Vj);
