@@ -612,7 +612,8 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
   }
   sorted_keys = kin;
   sorted_perm = vin;
-  LAUNCH(k_cells, G, kBlock, P, kin, dyn, cell_begin);
+  const int GC = std::max(1, std::min((P.num_cells + 1 + kBlock - 1) / kBlock, sm_count * 16));
+  LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
   LAUNCH(k_gather, G, kBlock, view(src), view(1 - src), vin, reduce());
   if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
 }

@@ -166,13 +166,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
 // Dense cell table: cell_begin[c] = first sorted index with key >= c, for
 // c in [0, num_cells]; cell_begin[num_cells] = number of live particles.
 __global__ void k_cells(Params P, const uint32_t* __restrict__ keys, DynState* dyn, int* __restrict__ cell_begin) {
+  // cell_begin[c] = first sorted index whose key is >= c (lower_bound), one
+  // thread per cell, so long runs of empty cells (the padding layers) cost no
+  // more than occupied ones; cell_begin[num_cells] = the live count.
   const int n = dyn->n;
   const int nc = P.num_cells;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
-    const int prev = i == 0 ? -1 : (int)min(keys[i - 1], (uint32_t)nc);
-    const int cur = i < n ? (int)min(keys[i], (uint32_t)nc) : nc;
-    for (int c = prev + 1; c <= cur; ++c) cell_begin[c] = i;
-    if (prev < nc && cur >= nc) dyn->n_alive = i;
+  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= nc; c += gridDim.x * blockDim.x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((int)min(__ldg(keys + mid), (uint32_t)nc) < c) lo = mid + 1;
+      else hi = mid;
+    }
+    cell_begin[c] = lo;
+    if (c == nc) dyn->n_alive = lo;
   }
 }
 
