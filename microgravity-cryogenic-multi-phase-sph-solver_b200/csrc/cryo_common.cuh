@@ -441,6 +441,45 @@ __device__ inline void for_each_nbr(const Params& P, const View& V, int i, V3 xi
   }
 }
 
+// for_each_nbr that also brings each neighbour's record of `A` (one float4
+// per particle) along with its position, one neighbour ahead, so that load
+// is in flight while the previous neighbour is processed: f(j, xj, rij, r2, aj).
+template <class F>
+__device__ inline void for_each_nbr_pf(const Params& P, const View& V, int i, V3 xi,
+                                       const float4* __restrict__ A, F&& f) {
+  const int c = P.use_lists ? __ldg(V.nbr_cnt + i) : kMaxNbr + 1;
+  if (c <= kMaxNbr) {
+    const int4* __restrict__ base = reinterpret_cast<const int4*>(V.nbr + (size_t)i * kNbrChunk);
+    const size_t cstride = (size_t)V.capacity * (kNbrChunk / 4);
+    auto quad = [&](int q) { return __ldg(base + (size_t)(q >> 1) * cstride + (q & 1)); };
+    int4 cur = c > 0 ? quad(0) : make_int4(0, 0, 0, 0);
+    int4 nxt = c > 4 ? quad(1) : make_int4(0, 0, 0, 0);
+    int jn = cur.x;
+    float4 xn = c > 0 ? __ldg(V.xp + jn) : make_float4(0, 0, 0, 0);
+    float4 an = c > 0 ? __ldg(A + jn) : make_float4(0, 0, 0, 0);
+    for (int k = 0; k < c; ++k) {
+      const int j = jn;
+      const float4 xj = xn, aj = an;
+      cur.x = cur.y; cur.y = cur.z; cur.z = cur.w;
+      if (((k + 1) & 3) == 0) {
+        cur = nxt;
+        if (k + 5 < c) nxt = quad(((k + 1) >> 2) + 1);
+      }
+      if (k + 1 < c) {
+        jn = cur.x;
+        xn = __ldg(V.xp + jn);
+        an = __ldg(A + jn);
+      }
+      const V3 rij = xi - xyz(xj);
+      const float r2 = norm2(rij);
+      f(j, xj, rij, r2, aj);
+    }
+  } else {
+    for_each_neighbor(P, V.cell_begin, V.xp, xi,
+                      [&](int j, float4 xj, V3 rij, float r2) { f(j, xj, rij, r2, __ldg(A + j)); });
+  }
+}
+
 // The particles a pass visits: with lists, an ordered phase index list
 // (fluid or wall); otherwise every particle (the pass filters by phase).
 struct Range {

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
         const float ci = ph == kLiquid ? 1.0f : 0.0f;
         V3 gradc{0, 0, 0}, wall_n{0, 0, 0}, akn{0, 0, 0}, gradphi{0, 0, 0};
         float s_all = 0, s_other = 0, ww = 0, hw = 0;
-        for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
+        for_each_nbr_pf(P, V, i, xi, V.aux, [&](int j, float4 xj, V3 rij, float r2, const float4& auxj) {
           const float r = sqrtf(r2);
           const float w = kernel_W(P, r);
           const int phj = ph_of(xj);
@@ -170,7 +170,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
             if (P.wall_colour) gradc += kernel_gradW(P, rij, r) * (P.vol0 * (nj.w - ci));
             return;
           }
-          const float Vj = __ldg(V.aux + j).x;  // m_j / rho_j
+          const float Vj = auxj.x;  // m_j / rho_j
           s_all += Vj * w;
           if (phj != ph) s_other += Vj * w;
           if (j == i) return;
