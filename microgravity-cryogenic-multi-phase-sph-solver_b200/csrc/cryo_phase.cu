@@ -266,9 +266,9 @@ __global__ void __launch_bounds__(kBlock) k_rebalance1(Params P, View V, int gat
     const V3 vi = xyz(vTi);
     float dm = 0.0f, dH = 0.0f;
     V3 dP{0, 0, 0};
-    for_each_nbr(P, V, i, xyz(xpi), [&](int j, float4 xj, V3, float r2) {
+    for_each_nbr_pf(P, V, i, xyz(xpi), V.mrps, [&](int j, float4 xj, V3, float r2, const float4& mrj) {
       if (j == i || ph_of(xj) != kVapor) return;
-      const float mj = __ldg(V.mrps + j).x;
+      const float mj = mrj.x;
       const float flow = beta * P.vol0 * kernel_W(P, sqrtf(r2)) * (mj - mi);
       const bool from_j = flow > 0.0f;
       dm += flow;
