@@ -413,6 +413,47 @@ int cryo_ensemble_launches_per_step(cryo_ensemble* ens, int* launches);
 int cryo_ensemble_synchronize(cryo_ensemble* ens);
 uintptr_t cryo_ensemble_stream(const cryo_ensemble* ens);
 
+/* ------------------------------------------------------------------------
+ * Differentiated window (no counterpart in the reference).  cryo_adj_forward
+ * runs `steps` ordinary steps from the current state, keeps a state
+ * checkpoint every `checkpoint_every` steps and returns the objectives
+ *   objectives[0..2] = sum over the steps of dt * slosh_force
+ *                      (slosh_force = -sum fw, sph_solver.cu:219-232, 640)
+ *   objectives[3..5] = sum over the steps of dt * slosh_moment (-sum mw)
+ *   objectives[6]    = p_ullage after the last step (sph_solver.cu:586-607).
+ * cryo_adj_backward takes seed[7] = d(loss)/d(objectives) and returns the
+ * gradients of that loss, computed by the hand-written reverse passes of
+ * every step (segments recomputed from the checkpoints):
+ *   grads[0] surface tension coefficient (FluidProperties::sigma)
+ *   grads[1] contact angle, per degree (SolverConfig::contact_angle_deg)
+ *   grads[2] lee_evaporation, grads[3] lee_condensation, grads[4] heater_power
+ *   frame_acc_grads[3 * k + c] (optional) = d(loss)/d(frame acceleration c
+ *   of step k), the acceleration the manoeuvre gives at the end of step k.
+ * The neighbour sets, phases and branch decisions of each step are held
+ * fixed (the derivative of the step as it ran); particles may not split,
+ * merge or die inside the window.  The solver's state after the backward is
+ * the window's final state.  Requires fixed_dt, a pinned sound speed
+ * (sound_speed or velocity_scale > 0), summation density, the default
+ * CSF/normal-rotation surface tension or none, adiabatic walls, a closed tank
+ * when phase change has vapour, no SPS, shifting or transport stress; other
+ * configurations return CRYO_EINVAL. */
+#define CRYO_ADJ_OBJECTIVES 7
+#define CRYO_ADJ_PARAMS 5
+int cryo_adj_forward(cryo_ctx* ctx, long long steps, int checkpoint_every, double* objectives);
+int cryo_adj_backward(cryo_ctx* ctx, const double* seed, double* grads, double* frame_acc_grads);
+/* Final-state adjoint seeds and initial-state adjoints (verification hooks):
+ * which 0 x, 1 v, 2 T, 3 m, 4 a, 5 ab; 3 or 1 floats per particle, in the
+ * window's final (seed) or initial (gradient) particle order. */
+int cryo_adj_seed_state(cryo_ctx* ctx, int which, const float* data, size_t count);
+int cryo_adj_state_gradient(cryo_ctx* ctx, int which, float* out, size_t count);
+/* Device bytes held by the window (checkpoints, tape, adjoints). */
+int cryo_adj_memory(cryo_ctx* ctx, size_t* bytes);
+int cryo_adj_release(cryo_ctx* ctx);
+/* Parameter setters for differentiated runs (the reference fixes these at
+ * construction: FluidProperties::sigma, SolverConfig::lee_*). */
+int cryo_set_surface_tension(cryo_ctx* ctx, float sigma);
+int cryo_set_lee_coefficients(cryo_ctx* ctx, float evaporation, float condensation);
+
 #ifdef __cplusplus
 }
 #endif

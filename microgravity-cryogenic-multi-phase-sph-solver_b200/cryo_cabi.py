@@ -282,6 +282,14 @@ def load(path=None):
         "cryo_load_state": (i, [vp, vp, C.c_size_t]),
         "cryo_set_graph_mode": (i, [vp, i]),
         "cryo_set_neighbor_mode": (i, [vp, i]),
+        "cryo_adj_forward": (i, [vp, C.c_longlong, i, vp]),
+        "cryo_adj_backward": (i, [vp, vp, vp, vp]),
+        "cryo_adj_seed_state": (i, [vp, i, vp, C.c_size_t]),
+        "cryo_adj_state_gradient": (i, [vp, i, vp, C.c_size_t]),
+        "cryo_adj_memory": (i, [vp, C.POINTER(C.c_size_t)]),
+        "cryo_adj_release": (i, [vp]),
+        "cryo_set_surface_tension": (i, [vp, f]),
+        "cryo_set_lee_coefficients": (i, [vp, f, f]),
     }
     for name, (res, args) in decl.items():
         fn = getattr(L, name)
@@ -424,3 +432,51 @@ class Context:
         lst = np.empty(max(total.value, 1), np.int32)
         self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), _ptr(lst), total.value, C.byref(total)))
         return counts, lst[: total.value]
+
+    # ---------------------------------------------- differentiated window
+    ADJ_STATE = {"x": 0, "v": 1, "T": 2, "m": 3, "a": 4, "ab": 5}
+
+    def set_surface_tension(self, sigma):
+        self.check(self.L.cryo_set_surface_tension(self.h, float(sigma)))
+
+    def set_lee_coefficients(self, evaporation, condensation):
+        self.check(self.L.cryo_set_lee_coefficients(self.h, float(evaporation), float(condensation)))
+
+    def set_contact_angle(self, degrees):
+        self.check(self.L.cryo_set_contact_angle(self.h, float(degrees)))
+
+    def set_heater_power(self, watts):
+        self.check(self.L.cryo_set_heater_power(self.h, float(watts)))
+
+    def adj_forward(self, steps, checkpoint_every=20):
+        """Runs the window; returns [int F (3), int M (3), p_ullage]."""
+        out = np.zeros(7, np.float64)
+        self.check(self.L.cryo_adj_forward(self.h, int(steps), int(checkpoint_every), _ptr(out)))
+        self._adj_steps = int(steps)
+        return out
+
+    def adj_seed_state(self, name, data):
+        comps = 1 if name in ("T", "m") else 3
+        a = np.ascontiguousarray(data, np.float32).reshape(-1)
+        self.check(self.L.cryo_adj_seed_state(self.h, self.ADJ_STATE[name], _ptr(a), a.size))
+
+    def adj_backward(self, seed):
+        """Returns (grads[5]: sigma, contact angle (deg), lee_evap, lee_cond,
+        heater power; frame acceleration gradient per step (steps, 3))."""
+        sd = np.ascontiguousarray(seed, np.float64).reshape(7)
+        g = np.zeros(5, np.float64)
+        fg = np.zeros((self._adj_steps, 3), np.float64)
+        self.check(self.L.cryo_adj_backward(self.h, _ptr(sd), _ptr(g), _ptr(fg)))
+        return g, fg
+
+    def adj_state_gradient(self, name):
+        comps = 1 if name in ("T", "m") else 3
+        n = self.num_particles()
+        out = np.empty(n * comps, np.float32)
+        self.check(self.L.cryo_adj_state_gradient(self.h, self.ADJ_STATE[name], _ptr(out), out.size))
+        return out if comps == 1 else out.reshape(n, 3)
+
+    def adj_memory(self):
+        b = C.c_size_t()
+        self.check(self.L.cryo_adj_memory(self.h, C.byref(b)))
+        return b.value

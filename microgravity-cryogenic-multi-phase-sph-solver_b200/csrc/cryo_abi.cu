@@ -16,7 +16,7 @@
 #include <string>
 #include <vector>
 
-#include "cryo_kernels.cuh"
+#include "cryo_adjoint.cuh"
 
 using namespace cryo;
 
@@ -87,6 +87,16 @@ size_t particle_bytes(size_t cap) {
 }  // namespace
 
 void ensemble_detach(cryo_ensemble* e, cryo_ctx* c);
+struct AdjWindow;
+void adj_free(AdjWindow* w);
+
+// Where a step recomputed for the reverse sweep leaves the values its later
+// stages overwrite (cryo_adjoint.cuh, Adj).
+struct StepTape {
+  float4 *vT1, *ns1, *pc2, *vT2;
+  float *m1, *m2;
+  DynState* dyn1;
+};
 
 struct cryo_ctx {
   cryo_config_t cfg{};
@@ -186,6 +196,9 @@ struct cryo_ctx {
   long long tele_step = 0;
   int tele_n = 0;
 
+  // differentiated window (cryo_adj_*)
+  AdjWindow* adj = nullptr;
+
   cudaEvent_t next_event() {
     if (event_used == event_pool.size()) {
       cudaEvent_t e;
@@ -246,6 +259,10 @@ struct cryo_ctx {
 
   ~cryo_ctx() {
     if (ensemble) ensemble_detach(ensemble, this);
+    if (adj) {
+      if (stream) cudaStreamSynchronize(stream);
+      adj_free(adj);
+    }
     if (ens_ev) cudaEventDestroy(ens_ev);
     telemetry_release();
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
@@ -403,7 +420,7 @@ struct cryo_ctx {
   void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
   void sort_and_gather(int src, int list_mode);  // after keys_a holds the keys
   void evaluate_rates(int s, bool maxima_reset, bool density_done);
-  void enqueue_step(int s);
+  void enqueue_step(int s, const StepTape* tape = nullptr);
   void launch_step();
   void ensure_initialized();
   void check_capacity();
@@ -655,8 +672,10 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
   }
 }
 
-// One Solver::step (sph_solver.cu:511-533) starting from set s; all device side.
-void cryo_ctx::enqueue_step(int s) {
+// One Solver::step (sph_solver.cu:511-533) starting from set s; all device
+// side.  With a tape (the reverse sweep's recomputation) the values the later
+// stages overwrite are copied out as they are produced.
+void cryo_ctx::enqueue_step(int s, const StepTape* tape) {
   const int G = grid_blocks();
   LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
   LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
@@ -664,6 +683,11 @@ void cryo_ctx::enqueue_step(int s) {
   const int d = 1 - s;
   const View V = view(d);
   evaluate_rates(d, false, false);
+  if (tape) {
+    LAUNCH(k_adj_copy4, G, kBlock, V.vT, tape->vT1, tape->m1, V.mrps, dyn);
+    LAUNCH(k_adj_copy4, G, kBlock, V.ns4, tape->ns1, nullptr, nullptr, dyn);
+    CK(cudaMemcpyAsync(tape->dyn1, dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, stream));
+  }
   LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   if (P.shift_strength > 0.0f) {
     LAUNCH(k_shift_compute, G, kBlock, P, V);
@@ -675,7 +699,9 @@ void cryo_ctx::enqueue_step(int s) {
   if (P.cfg_phase_change) {
     const Reduce R = reduce();
     LAUNCH(k_pc_normalize, G, kBlock, P, V, R, 1);
+    if (tape) LAUNCH(k_adj_copy4, G, kBlock, V.pc, tape->pc2, nullptr, nullptr, dyn);
     LAUNCH(k_pc_apply, G, kBlock, P, V, 1);
+    if (tape) LAUNCH(k_adj_copy4, G, kBlock, V.vT, tape->vT2, tape->m2, V.mrps, dyn);
     const bool reb = P.vapor_rebalance > 0.0f && has_vapor;
     if (reb) {
       LAUNCH(k_rebalance1, G, kBlock, P, V, 1);
@@ -2520,5 +2546,429 @@ int cryo_ensemble_synchronize(cryo_ensemble* e) {
 }
 
 uintptr_t cryo_ensemble_stream(const cryo_ensemble* e) { return reinterpret_cast<uintptr_t>(e->stream); }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Differentiated window (no counterpart in the reference).  The forward run
+// steps as usual (step graphs), keeps a state checkpoint every `every` steps
+// and integrates the slosh force and moment.  The backward sweep takes the
+// segments from the last: it restores the segment's checkpoint, re-runs the
+// segment keeping every step's start state, then for each step from the last
+// restores its start state, recomputes it eagerly with the one-step tape and
+// runs the reverse passes (cryo_adjoint.cu).  At the end the window's final
+// state is restored, so the solver continues as if only the forward had run.
+namespace {
+
+struct AdjSnap {
+  char* base = nullptr;
+  int cur = 0;
+};
+
+}  // namespace
+
+struct AdjWindow {
+  int n = 0, every = 20, cap = 0;
+  long long steps = 0;
+  bool recorded = false;
+  int splits0 = 0, merges0 = 0;
+  char* arena = nullptr;
+  size_t bytes = 0, snap_bytes = 0;
+  std::vector<AdjSnap> ckpt;  // start of every segment + the window's end
+  std::vector<AdjSnap> seg;   // start states of the steps of one segment
+  StepTape tape{};
+  float4 *cX[2]{}, *cV[2]{}, *cA[2]{}, *cB[2]{};
+  float4 *gP = nullptr, *gN = nullptr, *gG = nullptr, *gC = nullptr, *gU1 = nullptr, *gU2 = nullptr,
+         *gU3 = nullptr;
+  int* argmax = nullptr;
+  double *glob = nullptr, *partials = nullptr, *obj = nullptr, *ggrav = nullptr;
+  unsigned *ticket = nullptr, *status = nullptr;
+  int max_chunks = 0;
+  int q = 0;
+  // final-state seeds (float4 per particle, final order): x|m, v|T, a, ab
+  std::vector<float4> seed[4];
+};
+
+void adj_free(AdjWindow* w) {
+  if (!w) return;
+  if (w->arena) cudaFree(w->arena);
+  delete w;
+}
+
+namespace {
+
+constexpr int kSnap16 = 7;  // xp, vT, vt, nrm, mrps, a4, ab4
+
+size_t r256(size_t b) { return (b + 255) & ~size_t(255); }
+
+size_t snap_size(int n) { return kSnap16 * r256((size_t)n * 16) + r256((size_t)n * 4) + r256(sizeof(DynState)); }
+
+void snap_save(cryo_ctx* c, AdjWindow& W, AdjSnap& S) {
+  const size_t n = (size_t)W.n;
+  const Persist& p = c->set[c->cur];
+  const void* src[kSnap16] = {p.xp, p.vT, p.vt, p.nrm, p.mrps, c->a4, c->ab4};
+  char* q = S.base;
+  for (const void* a : src) {
+    CK(cudaMemcpyAsync(q, a, n * 16, cudaMemcpyDeviceToDevice, c->stream));
+    q += r256(n * 16);
+  }
+  CK(cudaMemcpyAsync(q, p.id, n * 4, cudaMemcpyDeviceToDevice, c->stream));
+  q += r256(n * 4);
+  CK(cudaMemcpyAsync(q, c->dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
+  S.cur = c->cur;
+}
+
+void snap_load(cryo_ctx* c, AdjWindow& W, const AdjSnap& S) {
+  const size_t n = (size_t)W.n;
+  c->cur = S.cur;
+  const Persist& p = c->set[c->cur];
+  void* dst[kSnap16] = {p.xp, p.vT, p.vt, p.nrm, p.mrps, c->a4, c->ab4};
+  const char* q = S.base;
+  for (void* a : dst) {
+    CK(cudaMemcpyAsync(a, q, n * 16, cudaMemcpyDeviceToDevice, c->stream));
+    q += r256(n * 16);
+  }
+  CK(cudaMemcpyAsync(p.id, q, n * 4, cudaMemcpyDeviceToDevice, c->stream));
+  q += r256(n * 4);
+  CK(cudaMemcpyAsync(c->dyn, q, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// The configurations the reverse passes cover.
+void adj_check_config(const cryo_ctx* c) {
+  const cryo_config_t& g = c->cfg;
+  const Params& P = c->P;
+  auto no = [](const char* what) { throw std::invalid_argument(std::string("adjoint: not supported: ") + what); };
+  if (!(P.fixed_dt > 0.0f)) no("adaptive time step (set fixed_dt)");
+  if (!(g.sound_speed > 0 || g.velocity_scale > 0)) no("sound speed derived from the surface tension (set sound_speed)");
+  if (P.density_mode != CRYO_DENSITY_SUMMATION) no("continuity density");
+  if (P.sps) no("SPS turbulence");
+  if (P.shift_strength > 0.0f) no("particle shifting");
+  if (P.tvf_stress) no("transport-velocity stress");
+  if (P.st_model == CRYO_ST_AKINCI) no("Akinci surface tension");
+  if (P.csf_smooth || P.csf_balanced) no("smoothed or balanced CSF");
+  if (P.wetting_model != 0) no("contact-line force wetting");
+  if (P.wall_bc != CRYO_WALL_ADIABATIC) no("isothermal walls");
+  if (P.clamp_neg) no("negative-pressure clamp");
+  if (g.thermo_mode == CRYO_THERMO_VENTED && c->has_vapor && P.cfg_phase_change) no("vented tank");
+}
+
+void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
+  // snapshots hold the window's n particles; the tape and the adjoints are
+  // sized by the capacity, which every kernel's particle count stays within
+  const int n = W.cap;
+  const long long nck = (steps + every - 1) / every + 1;
+  const int nseg = (int)std::min<long long>(every, steps);
+  W.snap_bytes = snap_size(W.n);
+  const size_t n16 = r256((size_t)n * 16), n4 = r256((size_t)n * 4);
+  W.max_chunks = n / kChunk + 2;
+  size_t t = (size_t)(nck + nseg) * W.snap_bytes;
+  t += 4 * n16 + 2 * n4 + r256(sizeof(DynState));            // tape
+  t += 8 * n16 + 7 * n16 + n4;                                // adjoints
+  t += r256(AG_COUNT * 8) + r256((size_t)AR_COUNT * W.max_chunks * 8) + r256(8 * 8) + r256((size_t)steps * 3 * 8);
+  t += r256(64) + r256(64);
+  if (W.arena && W.bytes >= t) {
+    // reuse
+  } else {
+    if (W.arena) CK(cudaFree(W.arena));
+    W.arena = nullptr;
+    CK(cudaMalloc(&W.arena, t));
+    W.bytes = t;
+  }
+  char* p = W.arena;
+  auto take = [&](size_t b) {
+    char* r = p;
+    p += r256(b);
+    return r;
+  };
+  W.ckpt.assign((size_t)nck, AdjSnap{});
+  for (auto& s : W.ckpt) s.base = take(W.snap_bytes);
+  W.seg.assign((size_t)nseg, AdjSnap{});
+  for (auto& s : W.seg) s.base = take(W.snap_bytes);
+  W.tape.vT1 = (float4*)take(n16);
+  W.tape.ns1 = (float4*)take(n16);
+  W.tape.pc2 = (float4*)take(n16);
+  W.tape.vT2 = (float4*)take(n16);
+  W.tape.m1 = (float*)take(n4);
+  W.tape.m2 = (float*)take(n4);
+  W.tape.dyn1 = (DynState*)take(sizeof(DynState));
+  for (int k = 0; k < 2; ++k) {
+    W.cX[k] = (float4*)take(n16);
+    W.cV[k] = (float4*)take(n16);
+    W.cA[k] = (float4*)take(n16);
+    W.cB[k] = (float4*)take(n16);
+  }
+  W.gP = (float4*)take(n16);
+  W.gN = (float4*)take(n16);
+  W.gG = (float4*)take(n16);
+  W.gC = (float4*)take(n16);
+  W.gU1 = (float4*)take(n16);
+  W.gU2 = (float4*)take(n16);
+  W.gU3 = (float4*)take(n16);
+  W.argmax = (int*)take(n4);
+  W.glob = (double*)take(AG_COUNT * 8);
+  W.partials = (double*)take((size_t)AR_COUNT * W.max_chunks * 8);
+  W.obj = (double*)take(8 * 8);
+  W.ggrav = (double*)take((size_t)steps * 3 * 8);
+  W.ticket = (unsigned*)take(64);
+  W.status = (unsigned*)take(64);
+  if ((size_t)(p - W.arena) > W.bytes) throw std::runtime_error("internal: adjoint arena overflow");
+  CK(cudaMemsetAsync(W.ticket, 0, 64, c->stream));
+  CK(cudaMemsetAsync(W.status, 0, 64, c->stream));
+  W.steps = steps;
+  W.every = every;
+}
+
+#define ALAUNCH(c, K, G, B, ...)                      \
+  do {                                                \
+    ++(c)->launch_counter;                            \
+    K<<<(G), (B), 0, (c)->stream>>>(__VA_ARGS__);     \
+    LAUNCH_CHECK();                                   \
+  } while (0)
+
+void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k) {
+  const Params& P = c->P;
+  const int d = c->cur;
+  Adj A{};
+  A.V = c->view(d);
+  A.vT1 = W.tape.vT1;
+  A.m1 = W.tape.m1;
+  A.ns1 = W.tape.ns1;
+  A.pc2 = W.tape.pc2;
+  A.vT2 = W.tape.vT2;
+  A.m2 = W.tape.m2;
+  A.dyn1 = W.tape.dyn1;
+  A.gX = W.cX[W.q];
+  A.gV = W.cV[W.q];
+  A.gA = W.cA[W.q];
+  A.gB = W.cB[W.q];
+  A.prevX = W.cX[1 - W.q];
+  A.prevV = W.cV[1 - W.q];
+  A.prevA = W.cA[1 - W.q];
+  A.prevB = W.cB[1 - W.q];
+  A.gP = W.gP;
+  A.gN = W.gN;
+  A.gG = W.gG;
+  A.gC = W.gC;
+  A.gU1 = W.gU1;
+  A.gU2 = W.gU2;
+  A.gU3 = W.gU3;
+  A.argmax = W.argmax;
+  A.perm = c->sorted_perm;
+  A.glob = W.glob;
+  A.partials = W.partials;
+  A.ticket = W.ticket;
+  A.max_chunks = W.max_chunks;
+  A.status = W.status;
+  const size_t n16 = (size_t)W.n * 16;
+  for (float4* a : {W.gP, W.gN, W.gG, W.gC, W.gU1, W.gU2, W.gU3}) CK(cudaMemsetAsync(a, 0, n16, c->stream));
+  const int G = c->grid_blocks();
+  const int GF = std::max(1, std::min((W.n + 127) / 128, c->sm_count * 16));
+  ALAUNCH(c, k_adj_saturation_sums, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_rebalance_local, G, kBlock, P, A);
+  if (P.cfg_phase_change) {
+    ALAUNCH(c, k_adj_rebalance_gather, G, kBlock, P, A);
+    ALAUNCH(c, k_adj_apply_local, G, kBlock, P, A);
+    ALAUNCH(c, k_adj_apply_gather, G, kBlock, P, A);
+    ALAUNCH(c, k_adj_normalize_local, G, kBlock, P, A);
+    ALAUNCH(c, k_adj_normalize_gather, G, kBlock, P, A);
+  }
+  ALAUNCH(c, k_adj_kick_sources, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_forces_local, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE, 4, AG_HINV, 0);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE + 4, 1, AG_SIGMA, 1);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE + 5, 1, AG_HEAT, 1);
+  ALAUNCH(c, k_adj_forces_gather, GF, 128, P, A);
+  ALAUNCH(c, k_adj_interface_local, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_interface_gather, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_wall_local, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_wall_gather, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_density_gather, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_SRC, 1, AG_TSAT_IN, 0);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_SRC + 1, 2, AG_LEE_E, 1);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_IFACE, 2, AG_COS, 1);
+  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_WALL, 3, AG_GRAV, 1);
+  ALAUNCH(c, k_adj_drift_scatter, G, kBlock, P, A);
+  ALAUNCH(c, k_adj_step_end, 1, 32, W.glob, W.ggrav + 3 * k);
+  W.q = 1 - W.q;
+}
+
+AdjWindow& adj_window(cryo_ctx* c) {
+  if (!c->adj || !c->adj->recorded) throw std::runtime_error("adjoint: no recorded window (call cryo_adj_forward)");
+  return *c->adj;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cryo_set_surface_tension(cryo_ctx* c, float sigma) {
+  return guard(c, [&] {
+    if (!(sigma >= 0)) throw std::invalid_argument("surface tension must be >= 0");
+    c->sync();
+    c->fluid.sigma = sigma;
+    c->P.sigma = c->cfg.surface_tension != CRYO_ST_NONE ? sigma : 0.0f;
+    c->invalidate_graphs();
+  });
+}
+
+int cryo_set_lee_coefficients(cryo_ctx* c, float evaporation, float condensation) {
+  return guard(c, [&] {
+    if (!(evaporation >= 0 && condensation >= 0)) throw std::invalid_argument("Lee coefficients must be >= 0");
+    c->sync();
+    c->cfg.lee_evaporation = evaporation;
+    c->cfg.lee_condensation = condensation;
+    c->P.lee_evap = evaporation;
+    c->P.lee_cond = condensation;
+    c->invalidate_graphs();
+  });
+}
+
+int cryo_adj_forward(cryo_ctx* c, long long steps, int every, double* objectives) {
+  return guard(c, [&] {
+    if (steps < 1) throw std::invalid_argument("adjoint: steps must be >= 1");
+    if (every < 1) throw std::invalid_argument("adjoint: checkpoint interval must be >= 1");
+    adj_check_config(c);
+    c->ensure_initialized();
+    c->pull();
+    if (!c->adj) c->adj = new AdjWindow;
+    AdjWindow& W = *c->adj;
+    W.recorded = false;
+    W.n = c->hdyn->n;
+    W.cap = c->capacity;
+    W.splits0 = c->hdyn->splits;
+    W.merges0 = c->hdyn->merges;
+    adj_alloc(c, W, steps, every);
+    CK(cudaMemsetAsync(W.obj, 0, 8 * 8, c->stream));
+    for (long long k = 0; k < steps; ++k) {
+      if (k % every == 0) snap_save(c, W, W.ckpt[(size_t)(k / every)]);
+      c->launch_step();
+      const View V = c->view(c->cur);
+      ALAUNCH(c, k_adj_objective, c->grid_blocks(), kBlock, c->P, V, c->reduce(), W.obj);
+    }
+    snap_save(c, W, W.ckpt.back());
+    double obj[6];
+    CK(cudaMemcpyAsync(obj, W.obj, sizeof(obj), cudaMemcpyDeviceToHost, c->stream));
+    c->pull();
+    if (c->hdyn->n != W.n || c->hdyn->splits != W.splits0 || c->hdyn->merges != W.merges0)
+      throw std::runtime_error("adjoint: particles split, merged or died inside the window (topology must stay fixed)");
+    for (int k = 0; k < 6; ++k) objectives[k] = obj[k];
+    objectives[6] = c->hdyn->p_ullage;
+    for (auto& v : W.seed) v.clear();
+    W.recorded = true;
+  });
+}
+
+// Seeds of the final state's adjoint (tests): which 0 x, 1 v, 2 T, 3 m, 4 a,
+// 5 ab; 3 or 1 floats per particle in the window's final order.
+int cryo_adj_seed_state(cryo_ctx* c, int which, const float* data, size_t count) {
+  return guard(c, [&] {
+    AdjWindow& W = adj_window(c);
+    if (which < 0 || which > 5) throw std::invalid_argument("adjoint: unknown state field");
+    const int comps = (which == 2 || which == 3) ? 1 : 3;
+    if (count != (size_t)W.n * comps) throw std::invalid_argument("adjoint: seed size mismatch");
+    const int slot = which == 0 || which == 3 ? 0 : (which == 1 || which == 2 ? 1 : which - 2);
+    std::vector<float4>& s = W.seed[slot];
+    if (s.empty()) s.assign((size_t)W.n, make_float4(0, 0, 0, 0));
+    for (int i = 0; i < W.n; ++i) {
+      if (comps == 3) {
+        s[i].x = data[3 * i];
+        s[i].y = data[3 * i + 1];
+        s[i].z = data[3 * i + 2];
+      } else {
+        s[i].w = data[i];
+      }
+    }
+  });
+}
+
+int cryo_adj_backward(cryo_ctx* c, const double* seed, double* grads, double* frame_grads) {
+  return guard(c, [&] {
+    AdjWindow& W = adj_window(c);
+    double g[AG_COUNT] = {0};
+    for (int k = 0; k < 3; ++k) {
+      g[AG_FW + k] = seed[k];
+      g[AG_MW + k] = seed[3 + k];
+    }
+    g[AG_P_OBJ] = seed[6];
+    CK(cudaMemcpyAsync(W.glob, g, sizeof(g), cudaMemcpyHostToDevice, c->stream));
+    const size_t n16 = (size_t)W.n * 16;
+    for (int k = 0; k < 2; ++k)
+      for (float4* a : {W.cX[k], W.cV[k], W.cA[k], W.cB[k]}) CK(cudaMemsetAsync(a, 0, n16, c->stream));
+    W.q = 0;
+    float4* dst[4] = {W.cX[0], W.cV[0], W.cA[0], W.cB[0]};
+    for (int k = 0; k < 4; ++k)
+      if (!W.seed[k].empty()) CK(cudaMemcpyAsync(dst[k], W.seed[k].data(), n16, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemsetAsync(W.status, 0, 4, c->stream));
+    c->sync();  // the pageable sources above are free again
+    const long long nseg = (W.steps + W.every - 1) / W.every;
+    for (long long sg = nseg - 1; sg >= 0; --sg) {
+      const long long k0 = sg * W.every, k1 = std::min(W.steps, k0 + W.every);
+      snap_load(c, W, W.ckpt[(size_t)sg]);
+      for (long long k = k0; k < k1; ++k) {
+        if (k > k0) snap_save(c, W, W.seg[(size_t)(k - k0)]);
+        if (k < k1 - 1) c->launch_step();
+      }
+      for (long long k = k1 - 1; k >= k0; --k) {
+        snap_load(c, W, k == k0 ? W.ckpt[(size_t)sg] : W.seg[(size_t)(k - k0)]);
+        const int s = c->cur;
+        c->enqueue_step(s, &W.tape);
+        c->cur = 1 - s;
+        adj_reverse_step(c, W, k);
+      }
+    }
+    snap_load(c, W, W.ckpt.back());
+    unsigned status = 0;
+    std::vector<double> gg((size_t)W.steps * 3);
+    CK(cudaMemcpyAsync(g, W.glob, sizeof(g), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(&status, W.status, 4, cudaMemcpyDeviceToHost, c->stream));
+    if (frame_grads) CK(cudaMemcpyAsync(gg.data(), W.ggrav, gg.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    c->pull();
+    if (status & ADJ_TOPOLOGY) throw std::runtime_error("adjoint: a particle died inside the window");
+    const double deg = (double)kPi / 180.0;
+    grads[0] = g[AG_SIGMA];
+    grads[1] = (-(double)c->P.sin_theta * g[AG_COS] + (double)c->P.cos_theta * g[AG_SIN]) * deg;
+    grads[2] = g[AG_LEE_E];
+    grads[3] = g[AG_LEE_C];
+    grads[4] = g[AG_HEAT];
+    if (frame_grads)
+      for (size_t k = 0; k < gg.size(); ++k) frame_grads[k] = -gg[k];  // gravity = g - a_frame
+  });
+}
+
+// Adjoint of the window's initial state (after cryo_adj_backward): which as
+// in cryo_adj_seed_state, in the order of the state the window started from.
+int cryo_adj_state_gradient(cryo_ctx* c, int which, float* out, size_t count) {
+  return guard(c, [&] {
+    AdjWindow& W = adj_window(c);
+    if (which < 0 || which > 5) throw std::invalid_argument("adjoint: unknown state field");
+    const int comps = (which == 2 || which == 3) ? 1 : 3;
+    if (count != (size_t)W.n * comps) throw std::invalid_argument("adjoint: output size mismatch");
+    const float4* src[6] = {W.cX[W.q], W.cV[W.q], W.cV[W.q], W.cX[W.q], W.cA[W.q], W.cB[W.q]};
+    std::vector<float4> h((size_t)W.n);
+    CK(cudaMemcpyAsync(h.data(), src[which], (size_t)W.n * 16, cudaMemcpyDeviceToHost, c->stream));
+    c->sync();
+    for (int i = 0; i < W.n; ++i) {
+      if (comps == 3) {
+        out[3 * i] = h[i].x;
+        out[3 * i + 1] = h[i].y;
+        out[3 * i + 2] = h[i].z;
+      } else {
+        out[i] = h[i].w;
+      }
+    }
+  });
+}
+
+int cryo_adj_memory(cryo_ctx* c, size_t* bytes) {
+  return guard(c, [&] { *bytes = c->adj ? c->adj->bytes : 0; });
+}
+
+int cryo_adj_release(cryo_ctx* c) {
+  return guard(c, [&] {
+    c->sync();
+    adj_free(c->adj);
+    c->adj = nullptr;
+  });
+}
 
 }  // extern "C"

@@ -398,6 +398,48 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def("set_maneuver", &Solver::set_maneuver, py::arg("profile"))
       .def("clear_frame_motion", &Solver::clear_frame_motion)
       .def("set_contact_angle", &Solver::set_contact_angle, py::arg("degrees"))
+      .def("set_surface_tension", &Solver::set_surface_tension, py::arg("sigma"),
+           "Surface tension coefficient (FluidProperties.sigma) for the following steps.")
+      .def("set_lee_coefficients", &Solver::set_lee_coefficients, py::arg("evaporation"), py::arg("condensation"))
+      .def(
+          "adjoint_forward",
+          [](Solver& s, long long steps, int checkpoint_every) {
+            std::array<double, 7> o;
+            {
+              py::gil_scoped_release nogil;
+              o = s.adjoint_forward(steps, checkpoint_every);
+            }
+            py::array_t<double> out(7);
+            std::memcpy(out.mutable_data(), o.data(), sizeof(o));
+            return out;
+          },
+          py::arg("steps"), py::arg("checkpoint_every") = 20,
+          "Runs `steps` steps keeping checkpoints; returns [time-integrated slosh force (3), time-integrated "
+          "slosh moment (3), final ullage pressure].")
+      .def(
+          "adjoint_backward",
+          [](Solver& s, const std::array<double, 7>& seed) {
+            Solver::AdjointGradients g;
+            {
+              py::gil_scoped_release nogil;
+              g = s.adjoint_backward(seed);
+            }
+            const py::ssize_t steps = static_cast<py::ssize_t>(g.frame_acceleration.size() / 3);
+            py::array_t<double> fa({steps, py::ssize_t{3}});
+            if (steps) std::memcpy(fa.mutable_data(), g.frame_acceleration.data(), g.frame_acceleration.size() * 8);
+            py::dict d;
+            d["sigma"] = g.sigma;
+            d["contact_angle"] = g.contact_angle;
+            d["lee_evaporation"] = g.lee_evaporation;
+            d["lee_condensation"] = g.lee_condensation;
+            d["heater_power"] = g.heater_power;
+            d["frame_acceleration"] = fa;
+            return d;
+          },
+          py::arg("seed"),
+          "Gradients of seed . objectives of the last adjoint_forward window (hand-written reverse passes).")
+      .def_property_readonly("adjoint_memory", &Solver::adjoint_memory)
+      .def("adjoint_release", &Solver::adjoint_release)
       .def("damp_velocities", &Solver::damp_velocities, py::arg("factor"))
       .def(
           "configure_telemetry", [](Solver& s, TelemetryMode mode) { s.configure_telemetry(mode); }, py::arg("mode"),

@@ -371,11 +371,26 @@ class Solver {
   std::vector<std::uint8_t> save_state() const;
   void load_state(const std::vector<std::uint8_t>& blob);
 
+  // Differentiated window (cryo_adj_*): objectives of `steps` steps from the
+  // current state, then the gradients of seed . objectives by the reverse
+  // passes (include/cryosph_b200.h describes both).
+  std::array<double, 7> adjoint_forward(long long steps, int checkpoint_every = 20);
+  struct AdjointGradients {
+    double sigma = 0, contact_angle = 0, lee_evaporation = 0, lee_condensation = 0, heater_power = 0;
+    std::vector<double> frame_acceleration;  // 3 per step
+  };
+  AdjointGradients adjoint_backward(const std::array<double, 7>& seed);
+  std::size_t adjoint_memory() const;
+  void adjoint_release();
+  void set_surface_tension(real sigma);
+  void set_lee_coefficients(real evaporation, real condensation);
+
  private:
   void check(int rc) const;
   SolverConfig cfg_;
   FluidProperties fluid_;
   cryo_ctx* ctx_ = nullptr;
+  long long adj_steps_ = 0;
 };
 
 // Batched stepping of independent tanks (no counterpart in the reference):

@@ -289,6 +289,39 @@ void Solver::set_contact_angle(real degrees) {
   check(cryo_set_contact_angle(ctx_, degrees));
   cfg_.contact_angle_deg = degrees;
 }
+void Solver::set_surface_tension(real sigma) {
+  check(cryo_set_surface_tension(ctx_, sigma));
+  fluid_.sigma = sigma;
+}
+void Solver::set_lee_coefficients(real evaporation, real condensation) {
+  check(cryo_set_lee_coefficients(ctx_, evaporation, condensation));
+  cfg_.lee_evaporation = evaporation;
+  cfg_.lee_condensation = condensation;
+}
+std::array<double, 7> Solver::adjoint_forward(long long steps, int checkpoint_every) {
+  std::array<double, 7> obj{};
+  check(cryo_adj_forward(ctx_, steps, checkpoint_every, obj.data()));
+  adj_steps_ = steps;
+  return obj;
+}
+Solver::AdjointGradients Solver::adjoint_backward(const std::array<double, 7>& seed) {
+  AdjointGradients g;
+  double p[CRYO_ADJ_PARAMS] = {0};
+  g.frame_acceleration.assign(static_cast<std::size_t>(adj_steps_) * 3, 0.0);
+  check(cryo_adj_backward(ctx_, seed.data(), p, g.frame_acceleration.data()));
+  g.sigma = p[0];
+  g.contact_angle = p[1];
+  g.lee_evaporation = p[2];
+  g.lee_condensation = p[3];
+  g.heater_power = p[4];
+  return g;
+}
+std::size_t Solver::adjoint_memory() const {
+  std::size_t b = 0;
+  check(cryo_adj_memory(ctx_, &b));
+  return b;
+}
+void Solver::adjoint_release() { check(cryo_adj_release(ctx_)); }
 void Solver::damp_velocities(real factor) { check(cryo_damp_velocities(ctx_, factor)); }
 void Solver::relax(double duration, real damping) { check(cryo_relax(ctx_, duration, damping)); }
 
