@@ -288,6 +288,9 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=100,
                     help="steps of the batched-ensemble comparison (0 = skip it)")
     ap.add_argument("--batched-tanks", type=int, default=64)
+    ap.add_argument("--adjoint-steps", type=int, default=400,
+                    help="steps of the differentiated C5 window (0 = skip the adjoint leg)")
+    ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval of the adjoint window")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
     args = ap.parse_args()
@@ -406,6 +409,11 @@ def main():
             "sharding": "tanks split over ranks longest-processing-time first by particle count" if world > 1 else None,
         })
 
+    adjoint = None
+    if rank == 0 and args.adjoint_steps > 0 and not args.only_timed:
+        torch.cuda.empty_cache()
+        adjoint = adjoint_run(cs, device, args.adjoint_steps, args.adjoint_every)
+
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
         r = reference_rate(cfg, fluid, p, lo, hi, 2000, 3, budget_s=10.0, cuda=True)
@@ -439,6 +447,7 @@ def main():
             "cpu_baseline": cpu,
             "reference_gpu": ref_gpu,
             "batched": batched,
+            "adjoint": adjoint,
         }
         print(json.dumps(line))
     if dist:
@@ -533,6 +542,94 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
     return {"value": n * steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": int(state_in / steps + ctl), "d2h_bytes_per_step": int(diag + state_out / steps),
             "steps": steps, "timing": "CUDA events per step (host work inside), L2 flushed between steps"}
+
+
+def c5_solver(cs, device, dx=0.0034):
+    """BASELINE config 5 (differentiation): closed LN2 cylinder R 0.1 m, H
+    0.25 m, dx 3.4 mm, fill 0.5, 2 K superheat, Lee 5 1/s both ways, 20 W
+    heater, 1e-4 g; a fixed step of 1 ms and a pinned sound speed (0.5 m/s),
+    and no splitting or merging inside the differentiated window."""
+    fluid = cs.FluidProperties.liquid_nitrogen()
+    cfg = cs.SolverConfig()
+    cfg.dx = dx
+    cfg.gravity = (0.0, 0.0, -9.81e-4)
+    cfg.thermo_mode = cs.TankThermoMode.Closed
+    cfg.heater_power = 20.0
+    cfg.lee_evaporation = 5.0
+    cfg.lee_condensation = 5.0
+    cfg.fixed_dt = 1e-3
+    cfg.sound_speed = 0.5
+    cfg.split_ratio = 1e3
+    cfg.merge_ratio = 0.0
+    s = cs.Solver(cfg, fluid, device)
+    fill = cs.FillSpec()
+    fill.fill_fraction = 0.5
+    fill.T_liquid = fluid.T_sat + 2.0
+    s.build_tank(cs.CylinderTank(0.1, 0.25), fill)
+    return s, fluid
+
+
+def adjoint_run(cs, device, steps, every, knots=16):
+    """gradients of the time-integrated slosh force and
+    moment and the final ullage pressure with respect to the surface tension,
+    the contact angle, the Lee coefficient and 16 piecewise-constant lateral
+    frame-acceleration knots (seeded U[-0.05, 0.05] m/s^2), through the
+    torch.autograd.Function over the hand-written adjoint.  Wall-clock times
+    with the device synchronised: the plain forward (the same steps, step
+    graphs, no checkpoints), the differentiated forward (checkpoints every
+    `every` steps) and the backward (segment recomputation + reverse passes)."""
+    import torch
+    import cryo_adjoint as ca
+    free0 = torch.cuda.mem_get_info(device)[0]
+    s, fluid = c5_solver(cs, device)
+    s.run_steps(3)
+    blob = s.save_state()
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    kn = np.zeros((knots, 3))
+    kn[:, 0] = rng.uniform(-0.05, 0.05, knots)
+    dt = float(s.config.fixed_dt)
+    times, _ = ca.knot_schedule(s.time, dt, steps, knots)
+    s.set_maneuver(ca._maneuver(times, kn))
+    s.run_steps(1)  # graph capture outside the timing
+    s.load_state(blob)
+    s.set_maneuver(ca._maneuver(times, kn))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.run_steps(steps)
+    torch.cuda.synchronize()
+    t_plain = time.perf_counter() - t0
+    s.load_state(blob)
+    sigma = torch.tensor(float(fluid.sigma), dtype=torch.float64, requires_grad=True)
+    theta = torch.tensor(float(s.config.contact_angle_deg), dtype=torch.float64, requires_grad=True)
+    lee = torch.tensor(5.0, dtype=torch.float64, requires_grad=True)
+    kt = torch.tensor(kn, dtype=torch.float64, requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    out = ca.slosh_window(s, sigma, theta, lee, kt, steps, every)
+    torch.cuda.synchronize()
+    t_fwd = time.perf_counter() - t0
+    weights = torch.tensor([1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1e-4], dtype=torch.float64)
+    loss = (out * weights).sum()
+    t0 = time.perf_counter()
+    loss.backward()
+    torch.cuda.synchronize()
+    t_bwd = time.perf_counter() - t0
+    used = free0 - torch.cuda.mem_get_info(device)[0]
+    res = {
+        "workload": "c5_ln2_boiloff_cylinder_dx0.0034", "particles": int(s.num_particles), "steps": steps,
+        "checkpoint_every": every, "knots": knots,
+        "plain_forward_s": t_plain, "adjoint_forward_s": t_fwd, "backward_s": t_bwd,
+        "adjoint_forward_ratio": (t_fwd + t_bwd) / t_plain,
+        "backward_over_forward": t_bwd / t_plain,
+        "window_device_bytes": int(s.adjoint_memory), "process_device_bytes": int(used),
+        "objectives": [float(v) for v in out.detach()],
+        "grad": {"sigma": float(sigma.grad), "contact_angle_deg": float(theta.grad), "lee": float(lee.grad),
+                 "knots_x": [float(v) for v in kt.grad[:, 0]]},
+        "loss": "sum of int F, int M (N s, N m s) + 1e-4 p_ullage (Pa)",
+        "timing": "wall clock, device synchronised; plain forward = the same steps through Solver.run_steps",
+    }
+    s.adjoint_release()
+    return res
 
 
 def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
