@@ -591,6 +591,11 @@ def adjoint_run(cs, device, steps, every, knots=16):
     times, _ = ca.knot_schedule(s.time, dt, steps, knots)
     s.set_maneuver(ca._maneuver(times, kn))
     s.run_steps(1)  # graph capture outside the timing
+    # one untimed window first: the window's device arena is allocated once
+    # and reused by later windows of the same size (an optimisation loop)
+    s.load_state(blob)
+    s.adjoint_forward(steps, every)
+    s.adjoint_backward([1.0] * 7)
     s.load_state(blob)
     s.set_maneuver(ca._maneuver(times, kn))
     torch.cuda.synchronize()
@@ -626,7 +631,8 @@ def adjoint_run(cs, device, steps, every, knots=16):
         "grad": {"sigma": float(sigma.grad), "contact_angle_deg": float(theta.grad), "lee": float(lee.grad),
                  "knots_x": [float(v) for v in kt.grad[:, 0]]},
         "loss": "sum of int F, int M (N s, N m s) + 1e-4 p_ullage (Pa)",
-        "timing": "wall clock, device synchronised; plain forward = the same steps through Solver.run_steps",
+        "timing": "wall clock, device synchronised, after one untimed window (arena allocated); plain forward = "
+                  "the same steps through Solver.run_steps",
     }
     s.adjoint_release()
     return res

@@ -96,6 +96,8 @@ struct StepTape {
   float4 *vT1, *ns1, *pc2, *vT2;
   float *m1, *m2;
   DynState* dyn1;
+  float4* sums;  // View::tape for the taped force / interface variants
+  int n;
 };
 
 struct cryo_ctx {
@@ -196,8 +198,11 @@ struct cryo_ctx {
   long long tele_step = 0;
   int tele_n = 0;
 
-  // differentiated window (cryo_adj_*)
+  // differentiated window (cryo_adj_*), and the sums tape of the step being
+  // recomputed for it (View::tape; null otherwise)
   AdjWindow* adj = nullptr;
+  float4* tape_sums = nullptr;
+  int tape_n = 0;
 
   cudaEvent_t next_event() {
     if (event_used == event_pool.size()) {
@@ -301,6 +306,8 @@ struct cryo_ctx {
     V.nbr_cnt = nbr_cnt;
     V.fluid_idx = fluid_idx;
     V.wall_idx = wall_idx;
+    V.tape = tape_sums;
+    V.tape_n = tape_n;
     return V;
   }
   Reduce reduce() const { return Reduce{partials, ticket, max_chunks}; }
@@ -419,7 +426,7 @@ struct cryo_ctx {
   // ------------------------------------------------------ step pieces
   void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
   void sort_and_gather(int src, int list_mode);  // after keys_a holds the keys
-  void evaluate_rates(int s, bool maxima_reset, bool density_done);
+  void evaluate_rates(int s, bool maxima_reset, bool density_done, bool tape = false);
   void enqueue_step(int s, const StepTape* tape = nullptr);
   void launch_step();
   void ensure_initialized();
@@ -637,13 +644,14 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
 
 // Solver::evaluate_rates (sph_solver.cu:449-480) on set s.  density_done:
 // the density/EOS pass already ran inside the list build.
-void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
+void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done, bool tape) {
   const int G = grid_blocks();
   const View V = view(s);
   if (maxima_reset) LAUNCH(k_begin_step, 1, 1, P, V, BEGIN_RATES);
   if (!density_done) LAUNCH(k_density, G, kBlock, P, V, 1);
   LAUNCH(k_wall, G, kBlock, P, V);
-  LAUNCH(k_interface, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
+  if (tape) LAUNCH(k_interface<1>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
+  else LAUNCH(k_interface<0>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
   if (P.sps) LAUNCH(k_sps, G, kBlock, P, V);
   if (P.csf_active && P.csf_smooth) LAUNCH(k_smooth_normals, G, kBlock, P, V);
   const int GF = forces_blocks();
@@ -652,6 +660,20 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
   if (P.st_model == CRYO_ST_AKINCI) what |= FORCE_AKINCI;
   if (P.density_mode == CRYO_DENSITY_CONTINUITY) what |= FORCE_DRHO;
   if (P.thermal) what |= FORCE_THERMAL;
+  if (tape) {  // the recomputation of a differentiated window: variants that also store their sums
+    switch (what) {
+      case FORCE_BASE: LAUNCH(k_forces_t<FORCE_BASE | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
+      case FORCE_BASE | FORCE_THERMAL:
+        LAUNCH(k_forces_t<FORCE_BASE | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
+        break;
+      case FORCE_BASE | FORCE_CSF: LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
+      case FORCE_BASE | FORCE_CSF | FORCE_THERMAL:
+        LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
+        break;
+      default: throw std::runtime_error("internal: no taped force pass for this configuration");
+    }
+    return;
+  }
   switch (what) {
 #define FORCES_CASE(W) \
   case W: LAUNCH(k_forces_t<W>, GF, FORCES_BLOCK, P, V, W); break;
@@ -677,12 +699,26 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done) {
 // stages overwrite are copied out as they are produced.
 void cryo_ctx::enqueue_step(int s, const StepTape* tape) {
   const int G = grid_blocks();
+  // the sums tape is visible to view() for this step only, also if a launch throws
+  struct TapeScope {
+    cryo_ctx* c;
+    ~TapeScope() {
+      if (c) {
+        c->tape_sums = nullptr;
+        c->tape_n = 0;
+      }
+    }
+  } scope{tape ? this : nullptr};
+  if (tape) {
+    tape_sums = tape->sums;
+    tape_n = tape->n;
+  }
   LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
   LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
   sort_and_gather(s, LISTS_PHASE);
   const int d = 1 - s;
   const View V = view(d);
-  evaluate_rates(d, false, false);
+  evaluate_rates(d, false, false, tape != nullptr);
   if (tape) {
     LAUNCH(k_adj_copy4, G, kBlock, V.vT, tape->vT1, tape->m1, V.mrps, dyn);
     LAUNCH(k_adj_copy4, G, kBlock, V.ns4, tape->ns1, nullptr, nullptr, dyn);
@@ -2023,7 +2059,7 @@ int cryo_pass(cryo_ctx* c, int pass) {
       case CRYO_PASS_NORMALIZE_MASSES: k_normalize_masses<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_EOS: k_eos<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_WALL_BOUNDARY: k_wall<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_INTERFACE: k_interface<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
+      case CRYO_PASS_INTERFACE: k_interface<0><<<G, kBlock, 0, st>>>(P, V, R, 0); break;
       case CRYO_PASS_TRANSPORT: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_TRANSPORT); break;
       case CRYO_PASS_SPS: k_sps<<<G, kBlock, 0, st>>>(P, V); break;
       case CRYO_PASS_MOMENTUM: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_MOMENTUM); break;
@@ -2575,11 +2611,16 @@ struct AdjWindow {
   char* arena = nullptr;
   size_t bytes = 0, snap_bytes = 0;
   std::vector<AdjSnap> ckpt;  // start of every segment + the window's end
-  std::vector<AdjSnap> seg;   // start states of the steps of one segment
-  StepTape tape{};
+  // one per step of a segment: the step's tape and its end-of-step arrays
+  struct Slot {
+    StepTape tape;
+    AdjSlot end;
+  };
+  std::vector<Slot> slots;
+  size_t slot_bytes = 0;
   float4 *cX[2]{}, *cV[2]{}, *cA[2]{}, *cB[2]{};
   float4 *gP = nullptr, *gN = nullptr, *gG = nullptr, *gC = nullptr, *gU1 = nullptr, *gU2 = nullptr,
-         *gU3 = nullptr;
+         *gU3 = nullptr, *R1 = nullptr, *R2 = nullptr;
   int* argmax = nullptr;
   double *glob = nullptr, *partials = nullptr, *obj = nullptr, *ggrav = nullptr;
   unsigned *ticket = nullptr, *status = nullptr;
@@ -2652,18 +2693,30 @@ void adj_check_config(const cryo_ctx* c) {
   if (g.thermo_mode == CRYO_THERMO_VENTED && c->has_vapor && P.cfg_phase_change) no("vented tank");
 }
 
+// Device bytes of one segment slot: the tape and end-of-step arrays of one
+// step, every per-particle array sized by the capacity.
+size_t slot_size(int cap, int num_cells) {
+  const size_t c16 = r256((size_t)cap * 16), c4 = r256((size_t)cap * 4);
+  return 4 * c16 + 2 * c4 + r256(sizeof(DynState))  // mid-step tape
+         + 6 * c16                                   // force / interface sums
+         + 7 * c16 + c4                              // xp vT vt nrm mrps a4 vwp, heat_w
+         + 2 * c4                                    // perm, list counts
+         + r256((size_t)cap * 4 * kMaxNbr)           // lists
+         + r256((size_t)(num_cells + 1) * 4) + r256(sizeof(DynState));
+}
+
 void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
   // snapshots hold the window's n particles; the tape and the adjoints are
   // sized by the capacity, which every kernel's particle count stays within
   const int n = W.cap;
   const long long nck = (steps + every - 1) / every + 1;
-  const int nseg = (int)std::min<long long>(every, steps);
+  const int nslot = (int)std::min<long long>(every, steps);
   W.snap_bytes = snap_size(W.n);
+  W.slot_bytes = slot_size(n, c->P.num_cells);
   const size_t n16 = r256((size_t)n * 16), n4 = r256((size_t)n * 4);
   W.max_chunks = n / kChunk + 2;
-  size_t t = (size_t)(nck + nseg) * W.snap_bytes;
-  t += 4 * n16 + 2 * n4 + r256(sizeof(DynState));            // tape
-  t += 8 * n16 + 7 * n16 + n4;                                // adjoints
+  size_t t = (size_t)nck * W.snap_bytes + (size_t)nslot * W.slot_bytes;
+  t += 8 * n16 + 9 * n16 + n4;                                // adjoints, force-pass records
   t += r256(AG_COUNT * 8) + r256((size_t)AR_COUNT * W.max_chunks * 8) + r256(8 * 8) + r256((size_t)steps * 3 * 8);
   t += r256(64) + r256(64);
   if (W.arena && W.bytes >= t) {
@@ -2671,6 +2724,14 @@ void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
   } else {
     if (W.arena) CK(cudaFree(W.arena));
     W.arena = nullptr;
+    W.bytes = 0;
+    size_t free_b = 0, total_b = 0;
+    CK(cudaMemGetInfo(&free_b, &total_b));
+    if (t > free_b)
+      throw std::invalid_argument("adjoint: the window needs " + std::to_string(t >> 20) + " MiB of device memory, " +
+                                  std::to_string(free_b >> 20) +
+                                  " MiB are free; use a smaller checkpoint interval (one segment of steps is held "
+                                  "at a time) or a shorter window");
     CK(cudaMalloc(&W.arena, t));
     W.bytes = t;
   }
@@ -2682,15 +2743,33 @@ void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
   };
   W.ckpt.assign((size_t)nck, AdjSnap{});
   for (auto& s : W.ckpt) s.base = take(W.snap_bytes);
-  W.seg.assign((size_t)nseg, AdjSnap{});
-  for (auto& s : W.seg) s.base = take(W.snap_bytes);
-  W.tape.vT1 = (float4*)take(n16);
-  W.tape.ns1 = (float4*)take(n16);
-  W.tape.pc2 = (float4*)take(n16);
-  W.tape.vT2 = (float4*)take(n16);
-  W.tape.m1 = (float*)take(n4);
-  W.tape.m2 = (float*)take(n4);
-  W.tape.dyn1 = (DynState*)take(sizeof(DynState));
+  W.slots.assign((size_t)nslot, AdjWindow::Slot{});
+  for (auto& sl : W.slots) {
+    StepTape& tp = sl.tape;
+    tp.vT1 = (float4*)take(n16);
+    tp.ns1 = (float4*)take(n16);
+    tp.pc2 = (float4*)take(n16);
+    tp.vT2 = (float4*)take(n16);
+    tp.m1 = (float*)take(n4);
+    tp.m2 = (float*)take(n4);
+    tp.dyn1 = (DynState*)take(sizeof(DynState));
+    tp.sums = (float4*)take(6 * (size_t)n * 16);
+    tp.n = n;
+    AdjSlot& e = sl.end;
+    e.xp = (float4*)take(n16);
+    e.vT = (float4*)take(n16);
+    e.vt = (float4*)take(n16);
+    e.nrm = (float4*)take(n16);
+    e.mrps = (float4*)take(n16);
+    e.a4 = (float4*)take(n16);
+    e.vwp = (float4*)take(n16);
+    e.heat_w = (float*)take(n4);
+    e.perm = (uint32_t*)take(n4);
+    e.nbr_cnt = (int*)take(n4);
+    e.nbr = (int*)take((size_t)n * 4 * kMaxNbr);
+    e.cell_begin = (int*)take((size_t)(c->P.num_cells + 1) * 4);
+    e.dyn = (DynState*)take(sizeof(DynState));
+  }
   for (int k = 0; k < 2; ++k) {
     W.cX[k] = (float4*)take(n16);
     W.cV[k] = (float4*)take(n16);
@@ -2704,6 +2783,8 @@ void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
   W.gU1 = (float4*)take(n16);
   W.gU2 = (float4*)take(n16);
   W.gU3 = (float4*)take(n16);
+  W.R1 = (float4*)take(n16);
+  W.R2 = (float4*)take(n16);
   W.argmax = (int*)take(n4);
   W.glob = (double*)take(AG_COUNT * 8);
   W.partials = (double*)take((size_t)AR_COUNT * W.max_chunks * 8);
@@ -2725,18 +2806,57 @@ void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
     LAUNCH_CHECK();                                   \
   } while (0)
 
-void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k) {
+// End-of-step copies into a slot: the per-particle arrays by one kernel, the
+// lists (chunk rows of n entries), the cell table and the scalar block by
+// copies.
+void adj_snap_end(cryo_ctx* c, AdjWindow& W, AdjWindow::Slot& sl) {
+  const View V = c->view(c->cur);
+  ALAUNCH(c, k_adj_snap_end, c->grid_blocks(), kBlock, V, c->sorted_perm, sl.end);
+  const size_t row = (size_t)W.n * kNbrChunk * 4;  // bytes of one chunk row of the n particles
+  const size_t pitch = (size_t)c->capacity * kNbrChunk * 4, dpitch = (size_t)W.cap * kNbrChunk * 4;
+  if (W.n > 0)
+    CK(cudaMemcpy2DAsync(sl.end.nbr, dpitch, c->nbr, pitch, row, kMaxNbr / kNbrChunk, cudaMemcpyDeviceToDevice,
+                         c->stream));
+  CK(cudaMemcpyAsync(sl.end.cell_begin, c->cell_begin, (size_t)(c->P.num_cells + 1) * 4, cudaMemcpyDeviceToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync(sl.end.dyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
+}
+
+// The arrays of a recomputed step (slot) through View, as the reverse
+// kernels read them; the list chunk stride is the capacity the slot was
+// sized by.
+View slot_view(const AdjWindow& W, const AdjWindow::Slot& sl) {
+  View V{};
+  const AdjSlot& e = sl.end;
+  V.xp = e.xp;
+  V.vT = e.vT;
+  V.vt = e.vt;
+  V.nrm = e.nrm;
+  V.mrps = e.mrps;
+  V.a4 = e.a4;
+  V.vwp = e.vwp;
+  V.heat_w = e.heat_w;
+  V.cell_begin = e.cell_begin;
+  V.dyn = e.dyn;
+  V.capacity = W.cap;
+  V.nbr = e.nbr;
+  V.nbr_cnt = e.nbr_cnt;
+  return V;
+}
+
+void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k, const AdjWindow::Slot& sl) {
   const Params& P = c->P;
-  const int d = c->cur;
   Adj A{};
-  A.V = c->view(d);
-  A.vT1 = W.tape.vT1;
-  A.m1 = W.tape.m1;
-  A.ns1 = W.tape.ns1;
-  A.pc2 = W.tape.pc2;
-  A.vT2 = W.tape.vT2;
-  A.m2 = W.tape.m2;
-  A.dyn1 = W.tape.dyn1;
+  A.V = slot_view(W, sl);
+  A.vT1 = sl.tape.vT1;
+  A.m1 = sl.tape.m1;
+  A.ns1 = sl.tape.ns1;
+  A.pc2 = sl.tape.pc2;
+  A.vT2 = sl.tape.vT2;
+  A.m2 = sl.tape.m2;
+  A.dyn1 = sl.tape.dyn1;
+  A.sums = sl.tape.sums;
+  A.sums_n = sl.tape.n;
   A.gX = W.cX[W.q];
   A.gV = W.cV[W.q];
   A.gA = W.cA[W.q];
@@ -2752,8 +2872,10 @@ void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k) {
   A.gU1 = W.gU1;
   A.gU2 = W.gU2;
   A.gU3 = W.gU3;
+  A.R1 = W.R1;
+  A.R2 = W.R2;
   A.argmax = W.argmax;
-  A.perm = c->sorted_perm;
+  A.perm = sl.end.perm;
   A.glob = W.glob;
   A.partials = W.partials;
   A.ticket = W.ticket;
@@ -2903,18 +3025,16 @@ int cryo_adj_backward(cryo_ctx* c, const double* seed, double* grads, double* fr
     const long long nseg = (W.steps + W.every - 1) / W.every;
     for (long long sg = nseg - 1; sg >= 0; --sg) {
       const long long k0 = sg * W.every, k1 = std::min(W.steps, k0 + W.every);
+      // recompute the segment once, keeping what each step's reverse reads
       snap_load(c, W, W.ckpt[(size_t)sg]);
       for (long long k = k0; k < k1; ++k) {
-        if (k > k0) snap_save(c, W, W.seg[(size_t)(k - k0)]);
-        if (k < k1 - 1) c->launch_step();
-      }
-      for (long long k = k1 - 1; k >= k0; --k) {
-        snap_load(c, W, k == k0 ? W.ckpt[(size_t)sg] : W.seg[(size_t)(k - k0)]);
+        AdjWindow::Slot& sl = W.slots[(size_t)(k - k0)];
         const int s = c->cur;
-        c->enqueue_step(s, &W.tape);
+        c->enqueue_step(s, &sl.tape);
         c->cur = 1 - s;
-        adj_reverse_step(c, W, k);
+        adj_snap_end(c, W, sl);
       }
+      for (long long k = k1 - 1; k >= k0; --k) adj_reverse_step(c, W, k, W.slots[(size_t)(k - k0)]);
     }
     snap_load(c, W, W.ckpt.back());
     unsigned status = 0;

@@ -477,6 +477,152 @@ __device__ inline void forces_pair_adj(const Params& P, const FI& I, const FU& U
   else o.x -= rvb;
 }
 
+// A fluid particle's force-pass values from the records of
+// k_adj_forces_local (no divisions at the use site).
+struct FR {
+  FP f;
+  int bits;  // do_T | do_C << 1 | valid unit normal << 2
+};
+__device__ inline FR load_rec(const Adj& A, int i, float4 xpi) {
+  FR r;
+  r.f.ph = ph_of(xpi);
+  r.f.x = xyz(xpi);
+  r.f.v = xyz(__ldg(A.vT1 + i));
+  r.f.ns = xyz(__ldg(A.ns1 + i));
+  const float4 r1 = __ldg(A.R1 + i), r2 = __ldg(A.R2 + i);
+  r.f.V = r1.x;
+  r.f.VT = r1.y;
+  r.f.c = r1.z;
+  r.f.rho = r1.w;
+  r.f.p = r2.x;
+  r.f.T = r2.y;
+  r.f.m = r2.z;
+  r.f.p_wv = 0.0f;
+  r.bits = __float_as_int(r2.w);
+  return r;
+}
+// FI of a record (the fields the wall pairs use).
+__device__ inline FI fi_of(const Params& P, const FR& r) {
+  FI I;
+  I.f = r.f;
+  const int pi = phase_index(r.f.ph);
+  I.eta = P.mu[pi];
+  I.av = r.f.ph == kVapor ? P.alpha_av_vap : P.alpha_av;
+  I.ki = P.k[pi];
+  I.eta_pair[0] = I.eta_pair[1] = 0.0f;
+  I.k_pair[0] = I.k_pair[1] = 0.0f;
+  I.do_T = (r.bits & 1) != 0;
+  I.do_C = (r.bits & 2) != 0;
+  I.pb = 0.0f;
+  I.mT = 0.0f;
+  I.alpha = 0.0f;
+  return I;
+}
+
+// Both directions of a fluid pair (k, l) of the force pass at once: the
+// terms f(k, l) feeding k's outputs differentiated with respect to k's
+// inputs, and the terms f(l, k) feeding l's outputs differentiated with
+// respect to k's inputs.  The pair's pressure, viscous and conductive terms
+// are equal and opposite, so both directions share one evaluation with the
+// upstream adjoints combined (k's minus l's); artificial viscosity,
+// transport velocity and curvature carry each side's own factors.
+// eta, kc: the pair's harmonic viscosity and conductivity (symmetric).
+__device__ inline void fluid_pair_both(const Params& P, const FR& K, const FU& Uk, const FR& L, const FU& Ul, V3 rkl,
+                                       float r2, bool thermal, float eta, float kc, float av, FA& o) {
+  const FP& a = K.f;
+  const FP& b = L.f;
+  const float h = P.h;
+  const float eta2 = 0.01f * h * h;
+  const float r = sqrtf(r2);
+  if (!(r > 1e-12f * h)) return;
+  const float ir = 1.0f / r;
+  float F, dF;
+  kernel_F(P, r, F, dF);
+  const float dW = r * F;
+  const V3 gw = rkl * F;  // grad W of (k, l); (l, k) has -gw
+  V3 gwb{0, 0, 0}, rvb{0, 0, 0};
+  float Fb = 0.0f, rb = 0.0f, r2b = 0.0f;
+  // transport velocity: sumT_k += gw t (do_T_k), sumT_l -= gw t (do_T_l)
+  {
+    const bool tk = (K.bits & 1) != 0, tl = (L.bits & 1) != 0;
+    if (tk || tl) {
+      const V3 u = (tk ? Uk.sT : V3{0, 0, 0}) - (tl ? Ul.sT : V3{0, 0, 0});
+      gwb += u * (a.VT * a.VT + b.VT * b.VT);
+      o.VT += 2.0f * a.VT * dot(u, gw);
+    }
+  }
+  const float vsum = a.V * a.V + b.V * b.V;
+  const V3 du = Uk.f - Ul.f;  // force upstream, k's minus l's
+  // pressure: force_k -= gw vsum pt, force_l += gw vsum pt
+  {
+    const float iD = 1.0f / (a.rho + b.rho);
+    const float pt = (b.rho * a.p + a.rho * b.p) * iD;
+    gwb -= du * (vsum * pt);
+    const float s = -dot(du, gw);
+    o.V += 2.0f * a.V * s * pt;
+    const float ptb = s * vsum;
+    o.p += ptb * b.rho * iD;
+    o.rho += ptb * (b.p - pt) * iD;
+  }
+  const V3 vij = a.v - b.v;
+  // viscosity: force_k += vij vsum eta F, force_l -= vij vsum eta F
+  if (eta != 0.0f) {
+    const float s = dot(du, vij);
+    Fb += s * vsum * eta;
+    o.V += 2.0f * a.V * s * eta * F;
+    o.v += du * (vsum * eta * F);
+  }
+  const float iden = 1.0f / (r2 + eta2);
+  // artificial viscosity (same phase, approaching): acc_k -= gw m_l Pi, acc_l += gw m_k Pi
+  if (av > 0.0f && a.ph == b.ph) {
+    const float vr = dot(vij, rkl);
+    if (vr < 0.0f) {
+      const float mu = h * vr * iden;
+      const float cm = 0.5f * (a.c + b.c), irm = 2.0f / (a.rho + b.rho);
+      const float Pi = -av * cm * mu * irm;
+      const V3 w = Uk.av * b.m - Ul.av * a.m;
+      gwb -= w * Pi;
+      const float Pib = -dot(w, gw);
+      o.m += Pi * dot(Ul.av, gw);
+      o.c += 0.5f * Pib * (-av * mu * irm);
+      o.rho += 0.5f * Pib * (-Pi * irm);
+      const float mub = Pib * (-av * cm * irm);
+      const float vrb = mub * h * iden;
+      r2b += -mub * mu * iden;
+      rvb += vij * vrb;
+      o.v += rkl * vrb;
+    }
+  }
+  // curvature: num_k += V_l dn.gw, den_k += V_l r (-dW) (do_C_k, valid n_l);
+  //            num_l += V_k dn.gw, den_l += V_k r (-dW) (do_C_l, valid n_k)
+  {
+    const bool ck = (K.bits & 2) && (L.bits & 4), cl = (L.bits & 2) && (K.bits & 4);
+    if (ck || cl) {
+      const float an = ck ? Uk.num * b.V : 0.0f, bn = cl ? Ul.num * a.V : 0.0f;
+      const V3 dn = a.ns - b.ns;
+      gwb += dn * (an + bn);
+      o.ns += gw * (an + bn);
+      if (cl) o.V += Ul.num * dot(dn, gw) + Ul.den * r * (-dW);
+      const float dd = (ck ? Uk.den * b.V : 0.0f) + (cl ? Ul.den * a.V : 0.0f);
+      rb += dd * (-(dW + r * (F + r * dF)));
+    }
+  }
+  // conduction: q_k += V_k V_l k (T_k - T_l) G, q_l -= the same
+  if (thermal) {
+    const float qd = Uk.q - Ul.q;
+    const float G = r2 * F * iden;
+    const float dT = a.T - b.T;
+    o.V += qd * b.V * kc * dT * G;
+    o.T += qd * a.V * b.V * kc * G;
+    const float Gb = qd * a.V * b.V * kc * dT;
+    r2b += Gb * (F * iden - r2 * F * iden * iden);
+    rb += Gb * (r2 * iden) * dF;
+  }
+  rvb += gradW_vjp(rkl, r, F, dF, gwb);
+  rvb += rkl * ((Fb * dF + rb) * ir + 2.0f * r2b);
+  o.x += rvb;
+}
+
 // Rotation of the colour gradient toward the contact angle
 // (surface_tension.cu:66-84): g' = normalized(nh (1 - b) + target b) |g|.
 struct Rot {
@@ -974,12 +1120,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_forces_local(Params P, Adj A) {
   const DynState* d1 = A.dyn1;
   const int n = V.dyn->n;
   const int nch = num_chunks(n);
-  const float dt = d1->dt;
   const bool thermal = P.thermal && d1->thermal_on;
   const float csf_unit = 2.0f / (P.rho0[0] + P.rho0[1]);
   const float csf_coeff = P.sigma * csf_unit;
   const float hinv = d1->heat_inv_norm;
-  const bool iso_walls = P.wall_bc == CRYO_WALL_ISOTHERMAL;
   const Reduce R = rows(A, AR_FORCE);
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
@@ -990,57 +1134,11 @@ __global__ void __launch_bounds__(kBlock) k_adj_forces_local(Params P, Adj A) {
       if (is_fluid(ph)) {
         const FP f = load_fluid(P, A, i, xpi);
         const FI I = make_fi(P, A, i, f);
-        const float h = P.h;
-        const float eta2 = 0.01f * h * h;
-        V3 force{0, 0, 0}, sumT{0, 0, 0};
-        float num = 0.0f, den = 0.0f, q = 0.0f;
-        for_each_nbr(P, V, i, f.x, [&](int j, float4 xj, V3 rij, float r2) {
-          if (j == i) return;
-          const float r = sqrtf(r2);
-          if (!(r > 1e-12f * h)) return;
-          const float dW = kernel_dWdr(P, r);
-          const V3 gw = rij * (dW / r);
-          const int phj = ph_of(xj);
-          const float4 mrj = __ldg(V.mrps + j);
-          if (phj == kWall) {
-            const float4 vwj = __ldg(V.vwp + j);
-            if (I.do_T) {
-              float rho_w;
-              if (ph == kVapor) {
-                rho_w = (vwj.w - (P.p_bg - P.vapor_K)) / (P.gas_R * f.T);
-              } else {
-                const float ratio = (mrj.z - P.p_bg) / P.tait_B + 1.0f;
-                rho_w = P.rho0[0] * powf(ratio > 0.5f ? ratio : 0.5f, 1.0f / P.tait_gamma);
-              }
-              const float Vj = rho_w > 0.0f ? f.VT * f.rho / rho_w : f.VT;
-              sumT += gw * (f.VT * f.VT + Vj * Vj);
-            }
-            const float vsum = f.V * f.V + P.vol0 * P.vol0;
-            const float pw = ph == kVapor ? vwj.w : mrj.z;
-            force -= gw * (vsum * 0.5f * (f.p + pw));
-            if (P.no_slip) force += (f.v - xyz(vwj)) * (vsum * I.eta * dW / r);
-            if (thermal && iso_walls) q += f.V * P.vol0 * 2.0f * I.ki * (f.T - __ldg(A.vT1 + j).w) * (r * dW) / (r2 + eta2);
-            return;
-          }
-          const float mj = __ldg(A.m1 + j);
-          const float Vj = mj / mrj.y;
-          if (I.do_T) {
-            const float VTj = 1.0f / mrj.w;
-            sumT += gw * (f.VT * f.VT + VTj * VTj);
-          }
-          const float vsum = f.V * f.V + Vj * Vj;
-          force -= gw * (vsum * ((mrj.y * f.p + f.rho * mrj.z) / (f.rho + mrj.y)));
-          const float eta = I.eta_pair[phase_index(phj)];
-          if (eta != 0.0f) force += (f.v - xyz(__ldg(A.vT1 + j))) * (vsum * eta * dW / r);
-          if (I.do_C) {
-            const V3 nj = xyz(__ldg(A.ns1 + j));
-            if (norm2(nj) > 0.25f) {
-              num += Vj * dot(f.ns - nj, gw);
-              den += Vj * r * (-dW);
-            }
-          }
-          if (thermal) q += f.V * Vj * I.k_pair[phase_index(phj)] * (f.T - __ldg(A.vT1 + j).w) * (r * dW) / (r2 + eta2);
-        });
+        // the forward pass's own sums (taped when the step was recomputed)
+        const int tn = A.sums_n;
+        const float4 s0 = A.sums[i], s1 = A.sums[tn + i];
+        const V3 force = xyz(s0), sumT = xyz(s1);
+        const float q = s0.w, num = s1.w, den = A.sums[2 * tn + i].x;
         const float4 ga = A.gA[i], gb = A.gB[i];
         const V3 ab = xyz(ga);
         const V3 abb = xyz(gb);
@@ -1096,6 +1194,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_forces_local(Params P, Adj A) {
         A.gU1[i] = f4(ab, qb);
         A.gU2[i] = f4(sTb, numb);
         A.gU3[i] = make_float4(denb, 0.0f, 0.0f, 0.0f);
+        const int bits = (I.do_T ? 1 : 0) | (I.do_C ? 2 : 0) | (norm2(f.ns) > 0.25f ? 4 : 0);
+        A.R1[i] = make_float4(f.V, f.VT, f.c, f.rho);
+        A.R2[i] = make_float4(f.p, f.T, f.m, __int_as_float(bits));
         A.gG[i] = gg;
         add4(A.gX + i, xb, mb);
         add4(A.gV + i, vb, Tb);
@@ -1129,6 +1230,16 @@ __global__ void __launch_bounds__(128) k_adj_forces_gather(Params P, Adj A) {
   const float sdt = -dt;
   const V3 fwb = v3((float)A.glob[AG_FW], (float)A.glob[AG_FW + 1], (float)A.glob[AG_FW + 2]) * sdt;
   const V3 mwb = v3((float)A.glob[AG_MW], (float)A.glob[AG_MW + 1], (float)A.glob[AG_MW + 2]) * sdt;
+  // harmonic viscosity and conductivity per phase pair (symmetric: index
+  // = phase_k + phase_l), as navier_stokes.cu:190-196 and phase_change.cu:57-61
+  float etp[3], kp[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    const int pa = q > 1 ? 1 : 0, pb = q > 0 ? 1 : 0;
+    const float es = P.mu[pa] + P.mu[pb];
+    etp[q] = es > 0.0f ? 2.0f * P.mu[pa] * P.mu[pb] / es : 0.0f;
+    kp[q] = 4.0f * P.k[pa] * P.k[pb] / (P.k[pa] + P.k[pb]);
+  }
   PARTICLE_LOOP(k, n) {
     const float4 xpk = V.xp[k];
     const int phk = ph_of(xpk);
@@ -1138,9 +1249,9 @@ __global__ void __launch_bounds__(128) k_adj_forces_gather(Params P, Adj A) {
       FA o{};
       for_each_nbr(P, V, k, W.x, [&](int l, float4 xl, V3 rkl, float r2) {
         if (!is_fluid(ph_of(xl))) return;
-        const FP fl = load_fluid(P, A, l, xl);
-        const FI I = make_fi(P, A, l, fl);
-        const FU U = load_fu(A, l, fl.m);
+        const FR fl = load_rec(A, l, xl);
+        const FI I = fi_of(P, fl);
+        const FU U = load_fu(A, l, fl.f.m);
         forces_pair_adj<false>(P, I, U, W, -rkl, r2, dt, thermal, dFb, o);
       });
       float4 gp = A.gP[k];
@@ -1151,11 +1262,12 @@ __global__ void __launch_bounds__(128) k_adj_forces_gather(Params P, Adj A) {
       continue;
     }
     if (!is_fluid(phk)) continue;
-    const FP fk = load_fluid(P, A, k, xpk);
-    const FI Ik = make_fi(P, A, k, fk);
-    const FU Uk = load_fu(A, k, fk.m);
+    const FR rk = load_rec(A, k, xpk);
+    const FI Ik = fi_of(P, rk);
+    const FU Uk = load_fu(A, k, rk.f.m);
+    const int pk = phase_index(phk);
     FA o{};
-    for_each_nbr(P, V, k, fk.x, [&](int l, float4 xl, V3 rkl, float r2) {
+    for_each_nbr(P, V, k, rk.f.x, [&](int l, float4 xl, V3 rkl, float r2) {
       if (l == k) return;
       const int phl = ph_of(xl);
       if (phl == kWall) {
@@ -1165,13 +1277,15 @@ __global__ void __launch_bounds__(128) k_adj_forces_gather(Params P, Adj A) {
         return;
       }
       if (!is_fluid(phl)) return;
-      const FP fl = load_fluid(P, A, l, xl);
-      forces_pair_adj<true>(P, Ik, Uk, fl, rkl, r2, dt, thermal, V3{0, 0, 0}, o);
-      const FI Il = make_fi(P, A, l, fl);
-      const FU Ul = load_fu(A, l, fl.m);
-      forces_pair_adj<false>(P, Il, Ul, fk, -rkl, r2, dt, thermal, V3{0, 0, 0}, o);
+      const FR rl = load_rec(A, l, xl);
+      const FU Ul = load_fu(A, l, rl.f.m);
+      const int q = pk + phase_index(phl);
+      const float eta = q == 0 ? etp[0] : (q == 1 ? etp[1] : etp[2]);
+      const float kc = q == 0 ? kp[0] : (q == 1 ? kp[1] : kp[2]);
+      fluid_pair_both(P, rk, Uk, rl, Ul, rkl, r2, thermal, eta, kc, Ik.av, o);
     });
     // V = m / rho, VT = 1 / sigma, c(T)
+    const FP& fk = rk.f;
     o.m += o.V / fk.rho;
     o.rho += -o.V * fk.V / fk.rho;
     float Tb = o.T;
@@ -1210,29 +1324,11 @@ __global__ void __launch_bounds__(kBlock) k_adj_interface_local(Params P, Adj A)
       const float4 xpi = V.xp[i];
       const int ph = ph_of(xpi);
       if (is_fluid(ph)) {
-        const V3 xi = xyz(xpi);
-        const float ci = ph == kLiquid ? 1.0f : 0.0f;
-        V3 gradc{0, 0, 0}, wall_n{0, 0, 0};
-        float s_all = 0.0f, s_other = 0.0f, ww = 0.0f;
-        for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
-          const float r = sqrtf(r2);
-          const float w = kernel_W(P, r);
-          const int phj = ph_of(xj);
-          if (phj == kWall) {
-            const float vw = P.vol0 * w;
-            ww += vw;
-            const float4 nj = __ldg(V.nrm + j);
-            wall_n += xyz(nj) * vw;
-            if (P.wall_colour) gradc += kernel_gradW(P, rij, r) * (P.vol0 * (nj.w - ci));
-            return;
-          }
-          const float Vj = __ldg(A.m1 + j) / __ldg(V.mrps + j).y;
-          s_all += Vj * w;
-          if (phj != ph) s_other += Vj * w;
-          if (j == i) return;
-          const float cj = phj == kLiquid ? 1.0f : 0.0f;
-          gradc += kernel_gradW(P, rij, r) * (Vj * (cj - ci));
-        });
+        // the forward pass's sums before the rotation (taped when the step was recomputed)
+        const int tn = A.sums_n;
+        const float4 t3 = A.sums[3 * tn + i], t4 = A.sums[4 * tn + i];
+        const V3 gradc = xyz(t3), wall_n = xyz(t4);
+        const float s_all = t3.w, s_other = t4.w, ww = A.sums[5 * tn + i].x;
         const float alpha = s_all > 0.0f ? s_other / s_all : 0.0f;
         const float4 gn = A.gN[i], gg = A.gG[i];
         // colour gradient after the rotation: nrm (forces) and ns (CSF)
@@ -1566,6 +1662,22 @@ __global__ void __launch_bounds__(kBlock) k_adj_objective(Params P, View V, Redu
   for (int k = 0; k < 6; ++k) {
     const double s = block_sum_partials(R, k, nch);
     if (threadIdx.x == 0) obj[k] += dt * (-s);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_adj_snap_end(View V, const uint32_t* __restrict__ perm, AdjSlot S) {
+  const int n = V.dyn->n;
+  PARTICLE_LOOP(i, n) {
+    S.xp[i] = V.xp[i];
+    S.vT[i] = V.vT[i];
+    S.vt[i] = V.vt[i];
+    S.nrm[i] = V.nrm[i];
+    S.mrps[i] = V.mrps[i];
+    S.a4[i] = V.a4[i];
+    S.vwp[i] = V.vwp[i];
+    S.heat_w[i] = V.heat_w[i];
+    S.perm[i] = perm[i];
+    S.nbr_cnt[i] = V.nbr_cnt[i];
   }
 }
 

@@ -1,12 +1,12 @@
 // cryo_adjoint.cuh -- reverse (adjoint) passes of one Solver::step
 // (sph_solver.cu:511-533) with the neighbour topology of the step frozen.
 //
-// The reverse of a step runs after the step has been recomputed from its
-// start state.  The live arrays of the step's sorted set then still hold
-// what the rate passes read (positions and phases, density, pressure and
-// sigma, normals and colour fraction, wall fields, accelerations, heater
-// weights, the per-particle volume factors, the neighbour lists).  The few
-// values the later stages overwrite are snapshotted into a one-step tape.
+// The reverse of a step reads the step as it was recomputed from the
+// segment's checkpoint: the arrays the rate passes left (positions and
+// phases, density, pressure and sigma, normals and colour fraction, wall
+// fields, accelerations, heater weights, the neighbour lists), copied at the
+// end of the step (AdjSlot), the values the later stages overwrite, copied
+// as they were produced, and the sums of the force and interface passes.
 //
 // Every adjoint is held per particle in the step's sorted order.  A pair
 // term f(i, j) that feeds particle i's output is differentiated twice: with
@@ -50,6 +50,22 @@ enum AdjRow {
   AR_COUNT = 17
 };
 
+// The arrays of one recomputed step that the reverse sweep reads, as they
+// stand at the end of the step (positions and phase flags, v and T, m0,
+// normals and colour fraction, mass / density / pressure / sigma,
+// accelerations, wall fields, heater weights), plus the step's permutation,
+// neighbour lists (kNbrChunk-entry chunks with chunk stride n), cell table
+// and scalar block.
+struct AdjSlot {
+  float4 *xp, *vT, *vt, *nrm, *mrps, *a4, *vwp;
+  float* heat_w;
+  uint32_t* perm;
+  int* nbr_cnt;
+  int* nbr;
+  int* cell_begin;
+  DynState* dyn;
+};
+
 struct Adj {
   // forward values: the live sorted set of the recomputed step ...
   View V;
@@ -61,6 +77,8 @@ struct Adj {
   const float4* vT2;  // (v, T) after the phase-change apply
   const float* m2;    // mass after the phase-change apply
   const DynState* dyn1;  // scalar block at the rate evaluation
+  const float4* sums;    // force-pass sums (rows 0-2) and interface sums (rows 3-5), sums_n records each
+  int sums_n;
   // adjoints (sorted order of the step)
   float4* gX;  // (x, m)         carried between steps
   float4* gV;  // (v, T)         carried
@@ -73,6 +91,8 @@ struct Adj {
   float4* gU1; // per-particle upstream coefficients of the gather passes
   float4* gU2;
   float4* gU3;
+  float4* R1;  // fluid particles' force-pass values: (V, 1/sigma, c, rho)
+  float4* R2;  // ... (p, T, m, flags: do_T | do_C << 1 | valid unit normal << 2)
   int* argmax;     // sources: index of the receiver that set wr_max
   float4* prevX;   // scatter targets (the previous step's sorted order)
   float4* prevV;
@@ -110,6 +130,8 @@ __global__ void k_adj_reduce(Adj A, int row0, int nrows, int dst, int accumulate
 // dt * (-sum mw) over fluid particles (the slosh force and moment of
 // sph_solver.cu:219-232 and :640-641, integrated in time).
 __global__ void k_adj_objective(Params P, View V, Reduce R, double* obj);
+// End-of-step copy of the arrays of AdjSlot (the lists are copied apart).
+__global__ void k_adj_snap_end(View V, const uint32_t* perm, AdjSlot S);
 // End of one reverse step: the step's gravity adjoint out, the T_sat adjoint
 // carried to the previous step, the ullage-pressure seed consumed.
 __global__ void k_adj_step_end(double* glob, double* grav_out);

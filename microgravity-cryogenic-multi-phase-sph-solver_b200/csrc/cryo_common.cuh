@@ -219,6 +219,11 @@ struct View {
   // ordered phase index lists (built after each reorder)
   int* fluid_idx;
   int* wall_idx;
+  // Only while a differentiated window is recomputed (null otherwise): the
+  // force and interface sums the reverse sweep reads, 6 arrays of tape_n
+  // records (force pass: rows 0-2, interface pass: rows 3-5).
+  float4* tape;
+  int tape_n;
 };
 
 // --------------------------------------------------------- SPH kernels

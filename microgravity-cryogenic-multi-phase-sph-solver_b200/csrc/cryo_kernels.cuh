@@ -147,12 +147,15 @@ __global__ void k_normalize_masses(Params P, View V);
 __global__ void k_eos(Params P, View V);
 __global__ void k_wall(Params P, View V);
 // heat_sum: 0 none, 1 when thermal is on (step), 2 always (operator call)
+// TAPE: also store the sums into V.tape (the recomputation of a differentiated window).
+template <int TAPE>
 __global__ void k_interface(Params P, View V, Reduce R, int heat_sum);
 __global__ void k_sps(Params P, View V);
 __global__ void k_smooth_normals(Params P, View V);
 // Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
 enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8, FORCE_DRHO = 16,
-       FORCE_THERMAL = 32, FORCE_MAXIMA = 64, FORCE_THERMAL_ALWAYS = 128 };
+       FORCE_THERMAL = 32, FORCE_MAXIMA = 64, FORCE_THERMAL_ALWAYS = 128,
+       FORCE_TAPE = 256 };  // compile-time only: also store the sums into V.tape
 template <int WHAT>
 __global__ void k_forces_t(Params P, View V, int what_rt);
 constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;

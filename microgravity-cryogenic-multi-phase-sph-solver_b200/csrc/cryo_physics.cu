@@ -139,6 +139,7 @@ __global__ void __launch_bounds__(kBlock) k_wall(Params P, View V) {
 // same pass and heat_inv_norm is set (sph_solver.cu:466-472); the CSF unit
 // normal (smooth_interface_normals without smoothing, surface_tension.cu:91-101)
 // is written when the CSF model is active.
+template <int TAPE>
 __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R, int heat_sum) {
   __shared__ double sh[kBlock / 32];
   const Range rg = fluid_range(P, V);
@@ -179,6 +180,12 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
           gradc += gw * (Vj * (cj - ci));
           if (phj == kLiquid) akn += gw * Vj;
         });
+        if (TAPE) {
+          const int tn = V.tape_n;
+          V.tape[3 * tn + i] = f4(gradc, s_all);
+          V.tape[4 * tn + i] = f4(wall_n, s_other);
+          V.tape[5 * tn + i] = make_float4(ww, 0.0f, 0.0f, 0.0f);
+        }
         const float alpha = s_all > 0.0f ? s_other / s_all : 0.0f;
         V.wall_w[i] = ww;
         V.heat_w[i] = hw;
@@ -238,6 +245,9 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
     }
   }
 }
+
+template __global__ void k_interface<0>(Params, View, Reduce, int);
+template __global__ void k_interface<1>(Params, View, Reduce, int);
 
 // compute_sps_viscosity (navier_stokes.cu:71-119)
 __global__ void __launch_bounds__(kBlock) k_sps(Params P, View V) {
@@ -559,6 +569,12 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
       }
     });
 
+    if constexpr (WHAT >= 0 && (WHAT & FORCE_TAPE)) {
+      const int tn = V.tape_n;
+      V.tape[i] = f4(force, q);
+      V.tape[tn + i] = f4(sumT, num);
+      V.tape[2 * tn + i] = make_float4(den, 0.0f, 0.0f, 0.0f);
+    }
     V3 ab{0, 0, 0};
     if (what & FORCE_TRANSPORT) {
       if (do_T) ab = sumT * (-pb / mT_i);
@@ -640,6 +656,11 @@ template __global__ void k_forces_t<71>(Params, View, int);
 template __global__ void k_forces_t<103>(Params, View, int);
 template __global__ void k_forces_t<87>(Params, View, int);
 template __global__ void k_forces_t<119>(Params, View, int);
+// taped variants (FORCE_TAPE) of the sub-pass sets the adjoint covers
+template __global__ void k_forces_t<323>(Params, View, int);
+template __global__ void k_forces_t<355>(Params, View, int);
+template __global__ void k_forces_t<327>(Params, View, int);
+template __global__ void k_forces_t<359>(Params, View, int);
 
 // Maxima only (CRYO_PASS_MAXIMA; sph_solver.cu:475-479), from the stored fields.
 __global__ void __launch_bounds__(kBlock) k_maxima(Params P, View V) {
