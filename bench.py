@@ -291,6 +291,8 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=400,
                     help="steps of the differentiated C5 window (0 = skip the adjoint leg)")
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval of the adjoint window")
+    ap.add_argument("--only-adjoint", action="store_true",
+                    help="run only the adjoint leg (C5 window) and print its record; for profiler launch lists")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
     args = ap.parse_args()
@@ -303,6 +305,11 @@ def main():
 
     import CryoSPH as cs
 
+    if args.only_adjoint:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"adjoint": adjoint_run(cs, local, args.adjoint_steps, args.adjoint_every)}))
+        return 0
     if args.workload == "c4":
         return batched_main(args, cs, rank, world, local)
     label, cfg, fluid, p, lo, hi = workload(args.workload, cs, args.dx)

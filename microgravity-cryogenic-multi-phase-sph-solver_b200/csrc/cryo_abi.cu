@@ -2896,19 +2896,26 @@ void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k, const AdjWindow::S
   }
   ALAUNCH(c, k_adj_kick_sources, G, kBlock, P, A);
   ALAUNCH(c, k_adj_forces_local, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE, 4, AG_HINV, 0);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE + 4, 1, AG_SIGMA, 1);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_FORCE + 5, 1, AG_HEAT, 1);
+  {
+    // heater-norm and gravity adjoints of this step (set), sigma and heater (summed)
+    const AdjRows M{6, {AR_FORCE, AR_FORCE + 1, AR_FORCE + 2, AR_FORCE + 3, AR_FORCE + 4, AR_FORCE + 5},
+                    {AG_HINV, AG_GRAV, AG_GRAV + 1, AG_GRAV + 2, AG_SIGMA, AG_HEAT}, {0, 0, 0, 0, 1, 1}};
+    ALAUNCH(c, k_adj_reduce, M.count, kBlock, A, M);
+  }
   ALAUNCH(c, k_adj_forces_gather, GF, 128, P, A);
   ALAUNCH(c, k_adj_interface_local, G, kBlock, P, A);
   ALAUNCH(c, k_adj_interface_gather, G, kBlock, P, A);
   ALAUNCH(c, k_adj_wall_local, G, kBlock, P, A);
   ALAUNCH(c, k_adj_wall_gather, G, kBlock, P, A);
   ALAUNCH(c, k_adj_density_gather, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_SRC, 1, AG_TSAT_IN, 0);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_SRC + 1, 2, AG_LEE_E, 1);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_IFACE, 2, AG_COS, 1);
-  ALAUNCH(c, k_adj_reduce, 1, kBlock, A, AR_WALL, 3, AG_GRAV, 1);
+  {
+    // T_sat adjoint of this step's input (set); Lee, contact angle (summed); wall part of gravity (added)
+    const AdjRows M{8,
+                    {AR_SRC, AR_SRC + 1, AR_SRC + 2, AR_IFACE, AR_IFACE + 1, AR_WALL, AR_WALL + 1, AR_WALL + 2},
+                    {AG_TSAT_IN, AG_LEE_E, AG_LEE_C, AG_COS, AG_SIN, AG_GRAV, AG_GRAV + 1, AG_GRAV + 2},
+                    {0, 1, 1, 1, 1, 1, 1, 1}};
+    ALAUNCH(c, k_adj_reduce, M.count, kBlock, A, M);
+  }
   ALAUNCH(c, k_adj_drift_scatter, G, kBlock, P, A);
   ALAUNCH(c, k_adj_step_end, 1, 32, W.glob, W.ggrav + 3 * k);
   W.q = 1 - W.q;

@@ -1421,17 +1421,18 @@ __global__ void __launch_bounds__(kBlock) k_adj_interface_gather(Params P, Adj A
       const float w = kernel_W(P, r);
       const float Vl = __ldg(A.m1 + l) / __ldg(V.mrps + l).y;
       const float cl = phl == kLiquid ? 1.0f : 0.0f;
-      // k's sums over l
+      // k's sums over l (s_all, s_other: V_l W; gradc: gw V_l (c_l - c_k)) and
+      // l's sums over k (V_k W; -gw V_k (c_k - c_l)), sharing one evaluation
       const float sk = u1.w + (phl != phk ? u2.w : 0.0f);
-      xb += rkl * (sk * Vl * F);
-      xb += gradW_vjp(rkl, r, F, dF, gbk * (Vl * (cl - ck)));
-      // l's sums over k
       const float4 l1 = __ldg(A.gU1 + l);
       const float sl = l1.w + (phl != phk ? __ldg(A.gU2 + l).w : 0.0f);
-      const V3 glw = -rkl * F;  // grad W of the pair (l, k)
-      Vb += sl * w + dot(xyz(l1), glw) * (ck - cl);
-      xb += rkl * (sl * Vk * F);
-      xb -= gradW_vjp(-rkl, r, F, dF, xyz(l1) * (Vk * (ck - cl)));
+      xb += rkl * ((sk * Vl + sl * Vk) * F);
+      Vb += sl * w;
+      if (cl != ck) {
+        const V3 gl = xyz(l1);
+        Vb += dot(gl, rkl) * (F * (cl - ck));  // grad W of (l, k) is -rkl F
+        xb += gradW_vjp(rkl, r, F, dF, (gbk * Vl + gl * Vk) * (cl - ck));
+      }
     });
     add4(A.gX + k, xb, Vb / rk);
     float4 gb = A.gB[k];
@@ -1633,13 +1634,13 @@ __global__ void __launch_bounds__(kBlock) k_adj_drift_scatter(Params P, Adj A) {
   }
 }
 
-__global__ void __launch_bounds__(kBlock) k_adj_reduce(Adj A, int row0, int nrows, int dst, int accumulate) {
+__global__ void __launch_bounds__(kBlock) k_adj_reduce(Adj A, AdjRows M) {
+  // one block per row; the rows write distinct accumulators
+  const int b = blockIdx.x;
+  if (b >= M.count) return;
   const int nch = num_chunks(A.V.dyn->n);
-  const Reduce R = rows(A, row0);
-  for (int k = 0; k < nrows; ++k) {
-    const double s = block_sum_partials(R, k, nch);
-    if (threadIdx.x == 0) A.glob[dst + k] = accumulate ? A.glob[dst + k] + s : s;
-  }
+  const double s = block_sum_partials(rows(A, M.row[b]), 0, nch);
+  if (threadIdx.x == 0) A.glob[M.dst[b]] = M.accumulate[b] ? A.glob[M.dst[b]] + s : s;
 }
 
 __global__ void __launch_bounds__(kBlock) k_adj_objective(Params P, View V, Reduce R, double* obj) {

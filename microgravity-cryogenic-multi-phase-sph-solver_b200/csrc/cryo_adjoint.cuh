@@ -124,8 +124,12 @@ __global__ void k_adj_wall_local(Params P, Adj A);
 __global__ void k_adj_wall_gather(Params P, Adj A);
 __global__ void k_adj_density_gather(Params P, Adj A);
 __global__ void k_adj_drift_scatter(Params P, Adj A);
-// glob[dst + k] (+)= sum of partial row (row0 + k), k < nrows; one block.
-__global__ void k_adj_reduce(Adj A, int row0, int nrows, int dst, int accumulate);
+// glob[dst[b]] (+)= sum of partial row row[b], b < count; one block per row.
+struct AdjRows {
+  int count;
+  int row[12], dst[12], accumulate[12];
+};
+__global__ void k_adj_reduce(Adj A, AdjRows M);
 // Objective of the forward window: obj[0..2] += dt * (-sum fw), obj[3..5] +=
 // dt * (-sum mw) over fluid particles (the slosh force and moment of
 // sph_solver.cu:219-232 and :640-641, integrated in time).
