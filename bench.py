@@ -416,11 +416,6 @@ def main():
             "sharding": "tanks split over ranks longest-processing-time first by particle count" if world > 1 else None,
         })
 
-    adjoint = None
-    if rank == 0 and args.adjoint_steps > 0 and not args.only_timed:
-        torch.cuda.empty_cache()
-        adjoint = adjoint_run(cs, device, args.adjoint_steps, args.adjoint_every)
-
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
         r = reference_rate(cfg, fluid, p, lo, hi, 2000, 3, budget_s=10.0, cuda=True)
@@ -436,6 +431,12 @@ def main():
             rate, threads, k, el = r
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{k} steps of {label} after 2 warm-up steps ({el:.1f} s, OpenMP)"}
+
+    # the adjoint leg last: its window holds several GB until it is released
+    adjoint = None
+    if rank == 0 and args.adjoint_steps > 0 and not args.only_timed:
+        torch.cuda.empty_cache()
+        adjoint = adjoint_run(cs, device, args.adjoint_steps, args.adjoint_every)
 
     if rank == 0:
         line = {
