@@ -589,6 +589,7 @@ def adjoint_run(cs, device, steps, every, knots=16):
     import torch
     import cryo_adjoint as ca
     free0 = torch.cuda.mem_get_info(device)[0]
+    knots = min(knots, steps)
     s, fluid = c5_solver(cs, device)
     s.run_steps(3)
     blob = s.save_state()

@@ -1219,7 +1219,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_forces_local(Params P, Adj A) {
 // Every force pair from both ends.  Fluid k: its own pairs (adjoints on k as
 // i) and its fluid neighbours' pairs with k (k as j).  Wall k: its fluid
 // neighbours' pairs with k (wall pressures and ghost velocity).
-__global__ void __launch_bounds__(128) k_adj_forces_gather(Params P, Adj A) {
+#ifndef ADJ_FORCES_MIN_BLOCKS
+#define ADJ_FORCES_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(128, ADJ_FORCES_MIN_BLOCKS) k_adj_forces_gather(Params P, Adj A) {
   const View& V = A.V;
   const DynState* d1 = A.dyn1;
   const int n = V.dyn->n;
