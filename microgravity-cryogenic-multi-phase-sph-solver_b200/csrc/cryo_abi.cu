@@ -2700,7 +2700,7 @@ size_t slot_size(int cap, int num_cells) {
   return 4 * c16 + 2 * c4 + r256(sizeof(DynState))  // mid-step tape
          + 6 * c16                                   // force / interface sums
          + 7 * c16 + c4                              // xp vT vt nrm mrps a4 vwp, heat_w
-         + 2 * c4                                    // perm, list counts
+         + 4 * c4                                    // perm, list counts, phase index lists
          + r256((size_t)cap * 4 * kMaxNbr)           // lists
          + r256((size_t)(num_cells + 1) * 4) + r256(sizeof(DynState));
 }
@@ -2766,6 +2766,8 @@ void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
     e.heat_w = (float*)take(n4);
     e.perm = (uint32_t*)take(n4);
     e.nbr_cnt = (int*)take(n4);
+    e.fluid_idx = (int*)take(n4);
+    e.wall_idx = (int*)take(n4);
     e.nbr = (int*)take((size_t)n * 4 * kMaxNbr);
     e.cell_begin = (int*)take((size_t)(c->P.num_cells + 1) * 4);
     e.dyn = (DynState*)take(sizeof(DynState));
@@ -2841,6 +2843,8 @@ View slot_view(const AdjWindow& W, const AdjWindow::Slot& sl) {
   V.capacity = W.cap;
   V.nbr = e.nbr;
   V.nbr_cnt = e.nbr_cnt;
+  V.fluid_idx = e.fluid_idx;
+  V.wall_idx = e.wall_idx;
   return V;
 }
 

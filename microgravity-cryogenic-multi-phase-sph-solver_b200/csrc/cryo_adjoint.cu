@@ -58,6 +58,25 @@ __device__ inline V3 gradW_vjp(V3 rv, float r, float F, float dF, V3 u) {
 __device__ inline Reduce rows(const Adj& A, int row0) {
   return Reduce{A.partials + (size_t)row0 * A.max_chunks, A.ticket, A.max_chunks};
 }
+// Particle order of a gather's threads: the fluid particles' index list,
+// then (with walls) the wall particles' list, so a warp runs one kind of
+// loop; every particle (phase filtered in the body) without lists.
+struct PhaseOrder {
+  const int* f;
+  const int* w;
+  int nf, total;
+};
+__device__ inline PhaseOrder phase_order(const Params& P, const View& V, bool walls) {
+  const int n = V.dyn->n;
+  if (!P.use_lists) return PhaseOrder{nullptr, nullptr, n, n};
+  const int nf = V.dyn->n_fluid_list;
+  return PhaseOrder{V.fluid_idx, V.wall_idx, nf, walls ? nf + V.dyn->n_wall_list : nf};
+}
+__device__ inline int order_at(const PhaseOrder& o, int t) {
+  if (!o.f) return t;
+  return t < o.nf ? __ldg(o.f + t) : __ldg(o.w + (t - o.nf));
+}
+
 __device__ inline void add4(float4* p, V3 a, float w) {
   float4 v = *p;
   v.x += a.x;
@@ -801,7 +820,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_rebalance_gather(Params P, Adj A
   const View& V = A.V;
   const int n = V.dyn->n;
   const float bv = P.vapor_rebalance * P.vol0;
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, false);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     if (ph_of(xpk) != kVapor) continue;
     const float mk = A.m2[k];
@@ -908,7 +929,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_apply_local(Params P, Adj A) {
 __global__ void __launch_bounds__(kBlock) k_adj_apply_gather(Params P, Adj A) {
   const View& V = A.V;
   const int n = V.dyn->n;
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, false);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     const int ph = ph_of(xpk);
     if (!is_fluid(ph)) continue;
@@ -1016,7 +1039,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_normalize_local(Params P, Adj A)
 __global__ void __launch_bounds__(kBlock) k_adj_normalize_gather(Params P, Adj A) {
   const View& V = A.V;
   const int n = V.dyn->n;
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, false);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     const int ph = ph_of(xpk);
     if (!is_fluid(ph)) continue;
@@ -1243,7 +1268,9 @@ __global__ void __launch_bounds__(128, ADJ_FORCES_MIN_BLOCKS) k_adj_forces_gathe
     etp[q] = es > 0.0f ? 2.0f * P.mu[pa] * P.mu[pb] / es : 0.0f;
     kp[q] = 4.0f * P.k[pa] * P.k[pb] / (P.k[pa] + P.k[pb]);
   }
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, true);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     const int phk = ph_of(xpk);
     if (phk == kWall) {
@@ -1381,7 +1408,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_interface_gather(Params P, Adj A
   const View& V = A.V;
   const int n = V.dyn->n;
   const float w0 = kernel_W(P, 0.0f);
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, true);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     const int phk = ph_of(xpk);
     const V3 xk = xyz(xpk);
@@ -1594,7 +1623,9 @@ __global__ void __launch_bounds__(kBlock) k_adj_wall_gather(Params P, Adj A) {
 __global__ void __launch_bounds__(kBlock) k_adj_density_gather(Params P, Adj A) {
   const View& V = A.V;
   const int n = V.dyn->n;
-  PARTICLE_LOOP(k, n) {
+  const PhaseOrder ord = phase_order(P, V, false);
+  PARTICLE_LOOP(t, ord.total) {
+    const int k = order_at(ord, t);
     const float4 xpk = V.xp[k];
     if (!is_fluid(ph_of(xpk))) continue;
     const float sk = A.gP[k].y;
@@ -1682,6 +1713,10 @@ __global__ void __launch_bounds__(kBlock) k_adj_snap_end(View V, const uint32_t*
     S.heat_w[i] = V.heat_w[i];
     S.perm[i] = perm[i];
     S.nbr_cnt[i] = V.nbr_cnt[i];
+    if (V.fluid_idx) {  // valid up to the list lengths, which together are n
+      S.fluid_idx[i] = V.fluid_idx[i];
+      S.wall_idx[i] = V.wall_idx[i];
+    }
   }
 }
 

@@ -63,6 +63,7 @@ struct AdjSlot {
   int* nbr_cnt;
   int* nbr;
   int* cell_begin;
+  int *fluid_idx, *wall_idx;  // the step's ordered phase index lists
   DynState* dyn;
 };
 
