@@ -12,8 +12,19 @@ namespace cryo {
 // compute_density_summation (SPH_kernels.cu:6-34); with fuse_eos the
 // equation of state (navier_stokes.cu:5-14) is applied in the same pass.
 __global__ void __launch_bounds__(kBlock) k_density(Params P, View V, int fuse_eos) {
-  const int n = V.dyn->n;
-  PARTICLE_LOOP(i, n) {
+  // with lists: the walls' constants from the wall list, then the fluid
+  // particles from the fluid list (a warp runs one kind of work)
+  if (P.use_lists) {
+    const Range wr = wall_range(P, V);
+    PARTICLE_LOOP(t, wr.count) {
+      const int i = particle_at(wr, t);
+      reinterpret_cast<float*>(V.mrps + i)[3] = 1.0f / P.vol0;
+      V.rmin[i] = P.support;
+    }
+  }
+  const Range fr = fluid_range(P, V);
+  PARTICLE_LOOP(t, fr.count) {
+    const int i = particle_at(fr, t);
     const float4 xpi = V.xp[i];
     const int ph = ph_of(xpi);
     float* mr = reinterpret_cast<float*>(V.mrps + i);
