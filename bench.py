@@ -629,6 +629,35 @@ def adjoint_run(cs, device, steps, every, knots=16):
     torch.cuda.synchronize()
     t_bwd = time.perf_counter() - t0
     used = free0 - torch.cuda.mem_get_info(device)[0]
+    # full-size check: Richardson-extrapolated central differences of the
+    # same loss through the forward (this library's FP32 steps); steps h and
+    # h/2 with h = 2e-2 of the value (knots: 2e-3 m/s^2); "fd_spread" is
+    # |D(h) - D(h/2)| / |R|, the size of the differences' own error
+    def loss_at(sig=None, th=None, le=None, kk=None):
+        s.load_state(blob)
+        with torch.no_grad():
+            o = ca.slosh_window(s, float(sigma) if sig is None else sig, float(theta) if th is None else th,
+                                float(lee) if le is None else le, kn if kk is None else kk, steps, every)
+        return float((o * weights).sum())
+
+    def knot_loss(kidx, v):
+        kk = kn.copy()
+        kk[kidx, 0] = v
+        return loss_at(kk=kk)
+
+    probes = [("lee", float(lee), 2e-2 * float(lee), lambda v: loss_at(le=v)),
+              ("contact_angle_deg", float(theta), 2e-2 * float(theta), lambda v: loss_at(th=v))]
+    probes += [(f"knot{k}_x", float(kn[k, 0]), 2e-3, (lambda kidx: lambda v: knot_loss(kidx, v))(k))
+               for k in (0, knots // 2)]
+    ad = {"lee": float(lee.grad), "contact_angle_deg": float(theta.grad),
+          **{f"knot{k}_x": float(kt.grad[k, 0]) for k in (0, knots // 2)}}
+    check = {}
+    for name, base, h, get in probes:
+        d1 = (get(base + h) - get(base - h)) / (2 * h)
+        d2 = (get(base + h / 2) - get(base - h / 2)) / h
+        r = (4 * d2 - d1) / 3
+        check[name] = {"adjoint": ad[name], "fd": r, "rel": abs(ad[name] - r) / max(abs(r), 1e-300),
+                       "fd_spread": abs(d1 - d2) / max(abs(r), 1e-300)}
     res = {
         "workload": "c5_ln2_boiloff_cylinder_dx0.0034", "particles": int(s.num_particles), "steps": steps,
         "checkpoint_every": every, "knots": knots,
@@ -640,6 +669,8 @@ def adjoint_run(cs, device, steps, every, knots=16):
         "grad": {"sigma": float(sigma.grad), "contact_angle_deg": float(theta.grad), "lee": float(lee.grad),
                  "knots_x": [float(v) for v in kt.grad[:, 0]]},
         "loss": "sum of int F, int M (N s, N m s) + 1e-4 p_ullage (Pa)",
+        "fd_check": check,
+        "fd_note": "Richardson-extrapolated central differences of the FP32 forward over the same window",
         "timing": "wall clock, device synchronised, after one untimed window (arena allocated); plain forward = "
                   "the same steps through Solver.run_steps",
     }
