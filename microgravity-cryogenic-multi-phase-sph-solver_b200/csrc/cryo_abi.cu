@@ -311,13 +311,22 @@ struct cryo_ctx {
     return V;
   }
   Reduce reduce() const { return Reduce{partials, ticket, max_chunks}; }
+  // Particles the launch grids are sized for (0: the capacity).  Every step
+  // kernel loops over its particles with a grid stride, so any grid gives
+  // the same results; a grid sized for the capacity (up to twice the count)
+  // only adds blocks that find no particle.
+  int grid_span = 0;
+  int span() const { return grid_span > 0 ? std::min(grid_span, capacity) : capacity; }
+  // the particle count last read plus head-room for splits; check_capacity
+  // drops the graphs when the count outgrows it
+  void size_grids() { grid_span = std::max(1, std::min(capacity, hdyn->n + hdyn->n / 8 + 1024)); }
   int grid_blocks() const {
-    const int need = (capacity + kBlock - 1) / kBlock;
+    const int need = (span() + kBlock - 1) / kBlock;
     return std::max(1, std::min(need, sm_count * 8));
   }
   // force pass: one thread per particle up to two full-occupancy waves
   int forces_blocks() const {
-    const int need = (capacity + FORCES_BLOCK - 1) / FORCES_BLOCK;
+    const int need = (span() + FORCES_BLOCK - 1) / FORCES_BLOCK;
     return std::max(1, std::min(need, sm_count * (2048 / FORCES_BLOCK) * 2));
   }
   void invalidate_graphs() {
@@ -766,6 +775,7 @@ void cryo_ctx::launch_step() {
       if (graph[s]) CK(cudaGraphExecDestroy(graph[s]));
       graph[s] = nullptr;
       cudaGraph_t g = nullptr;
+      size_grids();
       CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
       try {
         const long long c0 = launch_counter;
@@ -794,6 +804,7 @@ void cryo_ctx::launch_step() {
 void cryo_ctx::ensure_initialized() {
   if (initialized) return;
   if (!has_particles) throw std::runtime_error("Solver: no particles loaded");
+  size_grids();
   grid_build(cur);
   cur = 1 - cur;
   const int G = grid_blocks();
@@ -809,6 +820,7 @@ void cryo_ctx::ensure_initialized() {
 void cryo_ctx::check_capacity() {
   pull();
   if ((long long)hdyn->n * 4 > (long long)capacity * 3) allocate(capacity * 3 / 2 + 1024);
+  if (grid_span > 0 && hdyn->n > span()) invalidate_graphs();
 }
 
 void cryo_ctx::run_steps(long long n) {
@@ -956,7 +968,10 @@ struct cryo_ensemble {
   void build() {
     drop();
     leave();
-    for (cryo_ctx* c : tanks) c->pull();  // particle counts for the plan
+    for (cryo_ctx* c : tanks) {  // particle counts for the plan and the launch grids
+      c->pull();
+      c->size_grids();
+    }
     enter();
     built_cur.resize(tanks.size());
     built_gen.resize(tanks.size());
