@@ -46,7 +46,9 @@ enum {
   CRYO_DEV_NBR_OVERFLOW = 1u << 0, /* neighbour list capacity exceeded (scan fallback used) */
   CRYO_DEV_SPLIT_DROPPED = 1u << 1,/* split halves dropped: capacity exhausted */
   CRYO_DEV_NONFINITE = 1u << 2,    /* NaN/Inf seen in a dt maximum */
-  CRYO_DEV_BAD_CELL = 1u << 3      /* a cell index fell outside the grid table */
+  CRYO_DEV_BAD_CELL = 1u << 3,     /* a cell index fell outside the grid table */
+  CRYO_DEV_SLAB_HALO = 1u << 4,    /* a slab and its neighbour hold different ghost layers */
+  CRYO_DEV_SLAB_CAPACITY = 1u << 5 /* a refreshed slab did not fit its capacity */
 };
 
 /* ------------------------------------------------------------- enums */
@@ -189,6 +191,7 @@ enum {
 
 typedef struct cryo_ctx cryo_ctx;
 typedef struct cryo_ensemble cryo_ensemble;
+typedef struct cryo_slabs cryo_slabs;
 
 /* Tank geometry for the device lattice generator (geometry.hpp:22-130):
  * a tree of nodes, children before parents, the last node the root.
@@ -412,6 +415,44 @@ int cryo_ensemble_tune(cryo_ensemble* ens, const int* chain_candidates, int ncha
 int cryo_ensemble_launches_per_step(cryo_ensemble* ens, int* launches);
 int cryo_ensemble_synchronize(cryo_ensemble* ens);
 uintptr_t cryo_ensemble_stream(const cryo_ensemble* ens);
+
+/* ------------------------------------------------------------------------
+ * Slab decomposition of one tank (no counterpart in the reference, whose
+ * Solver runs one tank on one device).  The tank is cut along z into slabs
+ * of whole cell layers; slab r is a context on devices[r] (NULL: all on
+ * device 0; slabs may share a device).  Every slab holds its own layers and
+ * ghost copies of its neighbours' facing layers; between passes the ghost
+ * layer next to each slab is copied from the slab that owns it (plain loads
+ * of the neighbour's memory, peer access over NVLink between devices), and
+ * sums and maxima are taken over owned particles and combined in slab order.
+ * Particle results equal the one-context run's: the slabs' sorted orders are
+ * the whole tank's, cut at layer boundaries.  FP64 sums are added per slab,
+ * so the diagnostics' sums may differ from the one-context run's in the
+ * last bits.  The slabs' contexts are private; the group is stepped
+ * through these entry points only (no step graphs, relax, manoeuvres or
+ * differentiated windows). */
+/* Layer partition (host only): slab r gets layers [z_begin[r], z_begin[r+1])
+ * (z_begin has nslabs + 1 entries), each at least min_layers thick, cut
+ * where the running particle count crosses r / nslabs of the total. */
+int cryo_slab_partition(const long long* layer_counts, int nz, int nslabs, int min_layers, int* z_begin);
+int cryo_slabs_create(const cryo_config_t* cfg, const cryo_fluid_t* fluid, int nslabs, const int* devices,
+                      cryo_slabs** out);
+void cryo_slabs_destroy(cryo_slabs* s);
+const char* cryo_slabs_last_error(const cryo_slabs* s);
+int cryo_slabs_count(cryo_slabs* s, int* nslabs);
+/* Solver::set_particles of the whole tank (sph_solver.cu:407-428). */
+int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, const float* lo, const float* hi);
+/* Solver::run_steps (sph_solver.cu:535-538) of the whole tank. */
+int cryo_slabs_run_steps(cryo_slabs* s, long long n);
+int cryo_slabs_num_particles(cryo_slabs* s, int* n);
+/* Solver::particles of the whole tank, in the order the one-context run's
+ * arrays have (out->n as in cryo_download). */
+int cryo_slabs_download(cryo_slabs* s, cryo_host_particles_out_t* out);
+/* Solver::diagnostics (sph_solver.cu:609-653) of the whole tank. */
+int cryo_slabs_diagnostics(cryo_slabs* s, cryo_diagnostics_t* out);
+/* z_begin (nslabs + 1 entries), owned[r] = particles slab r owns, held[r] =
+ * particles its context holds (owned + ghosts); owned / held may be NULL. */
+int cryo_slabs_layout(cryo_slabs* s, int* z_begin, int* owned, int* held);
 
 /* ------------------------------------------------------------------------
  * Differentiated window (no counterpart in the reference).  cryo_adj_forward

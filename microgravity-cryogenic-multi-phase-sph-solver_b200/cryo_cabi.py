@@ -116,6 +116,12 @@ class HostParticles(C.Structure):
                 ("id", C.c_void_p)]
 
 
+class HostParticlesOut(C.Structure):
+    _fields_ = [("n", C.c_int), ("x", C.c_void_p), ("v", C.c_void_p), ("nrm", C.c_void_p), ("m", C.c_void_p),
+                ("rho", C.c_void_p), ("T", C.c_void_p), ("phase", C.c_void_p), ("flags", C.c_void_p),
+                ("id", C.c_void_p)]
+
+
 class CryoError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"[{code}] {msg}")
@@ -290,6 +296,17 @@ def load(path=None):
         "cryo_adj_release": (i, [vp]),
         "cryo_set_surface_tension": (i, [vp, f]),
         "cryo_set_lee_coefficients": (i, [vp, f, f]),
+        "cryo_slab_partition": (i, [C.POINTER(C.c_longlong), i, i, i, ip]),
+        "cryo_slabs_create": (i, [C.POINTER(Config), C.POINTER(Fluid), i, ip, C.POINTER(vp)]),
+        "cryo_slabs_destroy": (None, [vp]),
+        "cryo_slabs_last_error": (C.c_char_p, [vp]),
+        "cryo_slabs_count": (i, [vp, ip]),
+        "cryo_slabs_set_particles": (i, [vp, C.POINTER(HostParticles), fp, fp]),
+        "cryo_slabs_run_steps": (i, [vp, C.c_longlong]),
+        "cryo_slabs_num_particles": (i, [vp, ip]),
+        "cryo_slabs_download": (i, [vp, C.POINTER(HostParticlesOut)]),
+        "cryo_slabs_diagnostics": (i, [vp, C.POINTER(Diagnostics)]),
+        "cryo_slabs_layout": (i, [vp, ip, ip, ip]),
     }
     for name, (res, args) in decl.items():
         fn = getattr(L, name)
@@ -480,3 +497,85 @@ class Context:
         b = C.c_size_t()
         self.check(self.L.cryo_adj_memory(self.h, C.byref(b)))
         return b.value
+
+
+def slab_partition(layer_counts, nslabs, min_layers=3, lib=None):
+    """Layer boundaries of cryo_slab_partition (host arithmetic only)."""
+    L = lib or load()
+    counts = np.ascontiguousarray(layer_counts, dtype=np.int64)
+    out = np.zeros(nslabs + 1, dtype=np.int32)
+    rc = L.cryo_slab_partition(counts.ctypes.data_as(C.POINTER(C.c_longlong)), int(counts.size), int(nslabs),
+                               int(min_layers), out.ctypes.data_as(C.POINTER(C.c_int)))
+    if rc != CRYO_OK:
+        raise CryoError(rc, "cryo_slab_partition: bad arguments")
+    return out
+
+
+class Slabs:
+    """One tank cut into slabs of cell layers (cryo_slabs_*), each slab a
+    context on devices[r]."""
+
+    def __init__(self, cfg: Config, fluid: Fluid, nslabs, devices=None, lib=None):
+        self.L = lib or load()
+        self.h = C.c_void_p()
+        devs = None
+        if devices is not None:
+            self._devs = (C.c_int * nslabs)(*[int(d) for d in devices])
+            devs = self._devs
+        rc = self.L.cryo_slabs_create(C.byref(cfg), C.byref(fluid), int(nslabs), devs, C.byref(self.h))
+        if rc:
+            msg = self.L.cryo_slabs_last_error(None)
+            raise CryoError(rc, msg.decode() if msg else "cryo_slabs_create failed")
+        self.nslabs = int(nslabs)
+
+    def close(self):
+        if self.h:
+            self.L.cryo_slabs_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def check(self, rc):
+        if rc != CRYO_OK:
+            msg = self.L.cryo_slabs_last_error(self.h)
+            raise CryoError(rc, msg.decode() if msg else "")
+
+    def set_particles(self, arrays, lo, hi):
+        keep = []
+        hp = host_particles(arrays, keep)
+        self.check(self.L.cryo_slabs_set_particles(self.h, C.byref(hp), vec3(lo), vec3(hi)))
+
+    def step(self, n=1):
+        self.check(self.L.cryo_slabs_run_steps(self.h, int(n)))
+
+    def num_particles(self):
+        n = C.c_int()
+        self.check(self.L.cryo_slabs_num_particles(self.h, C.byref(n)))
+        return n.value
+
+    def particles(self):
+        n = self.num_particles()
+        out = {"x": np.empty((n, 3), np.float32), "v": np.empty((n, 3), np.float32),
+               "nrm": np.empty((n, 3), np.float32), "m": np.empty(n, np.float32), "rho": np.empty(n, np.float32),
+               "T": np.empty(n, np.float32), "phase": np.empty(n, np.uint8), "flags": np.empty(n, np.uint8),
+               "id": np.empty(n, np.uint32)}
+        o = HostParticlesOut(n, *[_ptr(out[k]) for k in ("x", "v", "nrm", "m", "rho", "T", "phase", "flags", "id")])
+        self.check(self.L.cryo_slabs_download(self.h, C.byref(o)))
+        return out
+
+    def diagnostics(self):
+        d = Diagnostics()
+        self.check(self.L.cryo_slabs_diagnostics(self.h, C.byref(d)))
+        return d
+
+    def layout(self):
+        zb = np.zeros(self.nslabs + 1, np.int32)
+        owned = np.zeros(self.nslabs, np.int32)
+        held = np.zeros(self.nslabs, np.int32)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))
+        self.check(self.L.cryo_slabs_layout(self.h, ip(zb), ip(owned), ip(held)))
+        return zb, owned, held

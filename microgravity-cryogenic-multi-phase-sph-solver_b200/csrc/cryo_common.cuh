@@ -116,6 +116,9 @@ struct Params {
   int nx, ny, nz, num_cells, key_bits;
   // neighbour lists (0: every pass scans the 27 cells)
   int use_lists;
+  // 1: this context is one slab of a decomposed tank; the heat normalisation
+  // and the ullage state come from the slabs' combined sums
+  int slab;
 };
 
 // Capacity of the per-particle neighbour list; a particle with more
@@ -162,7 +165,22 @@ struct DynState {
   // maneuver
   int man_n, man_rot;
   float man_origin[3];
+  // slab decomposition: the sorted range this context owns (0, INT_MAX when
+  // it holds the whole tank), the sorted count (split children follow it),
+  // and the owned sums the slabs combine
+  int own_lo, own_hi, n_sorted;
+  uint32_t id_offset;  // this slab's offset into the step's new split ids
+  int split_total;     // splits requested by every slab this step
+  double heat_sum;     // owned heat weights
+  double sat_sum[3];   // owned liquid mass, vapour mass, vapour m T
+  int n_next;          // particle count of a refreshed slab
 };
+
+// Particle i counts towards this context's global sums and maxima: inside
+// its owned sorted range, or a split child appended after the sorted count.
+__device__ inline bool owned(int own_lo, int own_hi, int n_sorted, int i) {
+  return (i >= own_lo && i < own_hi) || i >= n_sorted;
+}
 
 
 // Solver::compute_dt (sph_solver.cu:482-504); host and device share it so the

@@ -89,6 +89,7 @@ __global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce 
   const bool closed = P.thermo_closed && P.has_vapor;
   const bool damp = end_of_step && d->damp_after_step;
   const float damping = d->damping;
+  const int own_lo = d->own_lo, own_hi = d->own_hi, n_sorted = d->n_sorted;
   if (closed || damp) {
     for (int c = blockIdx.x; c < nch; c += gridDim.x) {
       const int i = c * kChunk + threadIdx.x;
@@ -96,7 +97,7 @@ __global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce 
       if (i < n) {
         const int ph = ph_of(V.xp[i]);
         const float4 vT = V.vT[i];
-        if (closed) {
+        if (closed && owned(own_lo, own_hi, n_sorted, i)) {
           const double m = V.mrps[i].x;
           if (ph == kLiquid) s[0] = m;
           if (ph == kVapor) {
@@ -122,24 +123,10 @@ __global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce 
     mT_vap = block_sum_partials(R, 2, nch);
   }
   if (threadIdx.x != 0) return;
-  bool done = false;
-  if (closed) {
-    if (!(d->fluid_volume0 > 0)) d->fluid_volume0 = m_liq / P.f_rho_l + m_vap / P.f_rho_v;
-    const double v_ullage = d->fluid_volume0 - m_liq / P.f_rho_l;
-    const double ratio = v_ullage > 0 && m_vap > 0 ? (mT_vap / v_ullage) / ((double)P.f_rho_v * P.f_T_sat) : 0.0;
-    if (isfinite(ratio) && ratio > 0) {
-      d->p_ullage = P.f_p_sat * ratio;
-      // FluidProperties::saturation_temperature (fluid_properties.cpp:7-10)
-      const float p = (float)d->p_ullage;
-      const double inv_T = 1.0 / P.f_T_sat - ((double)P.f_R_gas / P.f_h_fg) * log((double)p / P.f_p_sat);
-      d->T_sat = (float)(1.0 / inv_T);
-      done = true;
-    }
-  }
-  if (!done) {
-    d->p_ullage = P.f_p_sat;
-    d->T_sat = P.f_T_sat;
-  }
+  d->sat_sum[0] = m_liq;
+  d->sat_sum[1] = m_vap;
+  d->sat_sum[2] = mT_vap;
+  if (!P.slab) saturation_update(P, d, closed, m_liq, m_vap, mT_vap);
   if (end_of_step) {
     d->time += (double)d->dt;
     d->step += 1;
@@ -183,13 +170,14 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
   DynState* d = V.dyn;
   const int n = d->n;
   const int nch = num_chunks(n);
+  const int own_lo = d->own_lo, own_hi = d->own_hi, n_sorted = d->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double s[23];
 #pragma unroll
     for (int k = 0; k < 23; ++k) s[k] = 0.0;
     float vmax = 0.0f, tmax = 0.0f;
-    if (i < n) {
+    if (i < n && owned(own_lo, own_hi, n_sorted, i)) {
       const float4 xp = V.xp[i];
       const int ph = ph_of(xp);
       const float4 vT = V.vT[i];

@@ -211,6 +211,29 @@ enum { BEGIN_STEP = 0, BEGIN_RATES = 1 };
 __global__ void k_begin_step(Params P, View V, int mode);
 __global__ void k_heat_norm(Params P, View V, Reduce R);
 __global__ void k_maxima(Params P, View V);
+// The ullage pressure and saturation temperature from the phase sums
+// (sph_solver.cu:586-607).
+__device__ inline void saturation_update(const Params& P, DynState* d, bool closed, double m_liq, double m_vap,
+                                         double mT_vap) {
+  bool done = false;
+  if (closed) {
+    if (!(d->fluid_volume0 > 0)) d->fluid_volume0 = m_liq / P.f_rho_l + m_vap / P.f_rho_v;
+    const double v_ullage = d->fluid_volume0 - m_liq / P.f_rho_l;
+    const double ratio = v_ullage > 0 && m_vap > 0 ? (mT_vap / v_ullage) / ((double)P.f_rho_v * P.f_T_sat) : 0.0;
+    if (isfinite(ratio) && ratio > 0) {
+      d->p_ullage = P.f_p_sat * ratio;
+      // FluidProperties::saturation_temperature (fluid_properties.cpp:7-10)
+      const float p = (float)d->p_ullage;
+      const double inv_T = 1.0 / P.f_T_sat - ((double)P.f_R_gas / P.f_h_fg) * log((double)p / P.f_p_sat);
+      d->T_sat = (float)(1.0 / inv_T);
+      done = true;
+    }
+  }
+  if (!done) {
+    d->p_ullage = P.f_p_sat;
+    d->T_sat = P.f_T_sat;
+  }
+}
 __global__ void k_saturation(Params P, View V, Reduce R, int end_of_step);
 __global__ void k_diagnostics(Params P, View V, Reduce R, double* out);
 
@@ -234,6 +257,16 @@ struct GeomNode {
   double ofs[kGeomNodes][3];
 };
 // Lattice nodes at ((i0 + i + 1/2) h, ...), i < nx, ...; band = wall_layers h.
+// Slab decomposition of one tank (cryo_slab.cu).
+__global__ void k_slab_bounds(Params P, View V, int zb, int ze);
+__global__ void k_halo_pull(Params P, View dst, View src, int z);
+__global__ void k_slab_heat(Params P, DynState* const* dyns, int nslabs, DynState* mine, int heat_mode);
+__global__ void k_slab_split(DynState* const* dyns, int nslabs, int rank, DynState* mine);
+__global__ void k_slab_end(Params P, DynState* const* dyns, int nslabs, DynState* mine, int saturation);
+__global__ void k_slab_assemble(Params P, View dst, float4* a4_out, float4* ab4_out, View lo, View me, View up,
+                                int has_lo, int has_up, int zb, int ze, int depth);
+__global__ void k_slab_commit(View V, const float4* a4_in, const float4* ab4_in);
+
 struct Lattice {
   int i0, j0, k0, nx, ny, nz;
   long long total;

@@ -149,6 +149,7 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
   if (sums && !dyn->phase_change_on) return;
   const int n = dyn->n;
   const int nch = num_chunks(n);
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double s[3] = {0.0, 0.0, 0.0};
@@ -176,7 +177,8 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
           if (pc.x > cap) pc.x = cap;
         }
         V.pc[i] = pc;
-        if (!(fl & kDying)) {
+        if (!owned(own_lo, own_hi, n_sorted, i)) {
+        } else if (!(fl & kDying)) {
           if (fl & kTargetVapor) s[0] = (double)pc.x;
           else s[1] = (double)pc.x;
         } else if (pc.x > 0.0f) {
@@ -296,6 +298,7 @@ __global__ void __launch_bounds__(kBlock) k_rebalance2_mark(Params P, View V, Re
   if (gated && !dyn->phase_change_on) return;
   const int n = dyn->n;
   const int nch = num_chunks(n);
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double cnt[1] = {0.0};
@@ -320,7 +323,8 @@ __global__ void __launch_bounds__(kBlock) k_rebalance2_mark(Params P, View V, Re
           m = m_new;
         }
       }
-      const uint32_t f = (is_fluid(ph) && m > P.split_ratio * P.mref[phase_index(ph)]) ? 1u : 0u;
+      const uint32_t f =
+          (is_fluid(ph) && m > P.split_ratio * P.mref[phase_index(ph)] && owned(own_lo, own_hi, n_sorted, i)) ? 1u : 0u;
       flag[i] = f;
       cnt[0] = (double)f;
     }
@@ -329,7 +333,10 @@ __global__ void __launch_bounds__(kBlock) k_rebalance2_mark(Params P, View V, Re
   if (last_block(R.ticket)) {
     // exclusive scan of the chunk counts (in place, exact in double)
     const double total = block_exclusive_scan(R, 0, nch);
-    if (threadIdx.x == 0) dyn->split_requested = (int)total;
+    if (threadIdx.x == 0) {
+      dyn->split_requested = (int)total;
+      dyn->split_total = (int)total;  // the slabs replace it with the sum over slabs
+    }
   }
 }
 
@@ -358,11 +365,15 @@ __global__ void __launch_bounds__(kBlock) k_split(Params P, View V, Reduce R, co
   DynState* dyn = V.dyn;
   if (gated && !dyn->phase_change_on) return;
   const int requested = dyn->split_requested;
-  if (requested == 0) return;
+  if (requested == 0) {
+    // no split here; the ids other slabs hand out this step are still used
+    if (blockIdx.x == 0 && threadIdx.x == 0) dyn->next_id += (uint32_t)dyn->split_total;
+    return;
+  }
   const int n = dyn->n;
   const int cap = dyn->capacity;
   const uint32_t seed = (uint32_t)dyn->step;
-  const uint32_t id_base = dyn->next_id;
+  const uint32_t id_base = dyn->next_id + dyn->id_offset;
   const int nch = num_chunks(n);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
@@ -429,7 +440,7 @@ __global__ void __launch_bounds__(kBlock) k_split(Params P, View V, Reduce R, co
     const int added = (int)((long long)requested < room ? requested : room);
     if (added < requested) dyn->status |= CRYO_DEV_SPLIT_DROPPED;
     dyn->n = n + added;
-    dyn->next_id += (uint32_t)requested;
+    dyn->next_id += (uint32_t)dyn->split_total;
     dyn->splits += added;
   }
 }
@@ -441,6 +452,7 @@ __global__ void __launch_bounds__(kBlock) k_venting(Params P, View V, Reduce R, 
   if (gated && !dyn->phase_change_on) return;
   const int n = dyn->n;
   const int nch = num_chunks(n);
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double s[2] = {0.0, 0.0};
@@ -462,8 +474,10 @@ __global__ void __launch_bounds__(kBlock) k_venting(Params P, View V, Reduce R, 
         }
       }
       V.pc[i] = make_float4(out_m, out_h, wn, 0.0f);
-      s[0] = (double)out_m;
-      s[1] = (double)out_m * (double)out_h;
+      if (owned(own_lo, own_hi, n_sorted, i)) {
+        s[0] = (double)out_m;
+        s[1] = (double)out_m * (double)out_h;
+      }
     }
     publish_chunk<2>(R, c, s, sh);
   }

@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
   const Range rg = fluid_range(P, V);
   const int nch = num_chunks(rg.count);
   const bool write_ns = P.csf_active && !P.csf_smooth;
+  const int own_lo = V.dyn->own_lo, own_hi = V.dyn->own_hi, n_sorted = V.dyn->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int t = c * kChunk + threadIdx.x;
     double hsum[1] = {0.0};
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
         const float alpha = s_all > 0.0f ? s_other / s_all : 0.0f;
         V.wall_w[i] = ww;
         V.heat_w[i] = hw;
-        hsum[0] = (double)hw;
+        if (owned(own_lo, own_hi, n_sorted, i)) hsum[0] = (double)hw;
         if (P.st_model == CRYO_ST_AKINCI) {
           V.nrm[i] = f4(ph == kLiquid ? akn * (-P.h) : V3{0, 0, 0}, alpha);
         } else {
@@ -247,6 +248,8 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
     DynState* dyn = V.dyn;
     const double S = block_sum_partials(R, 0, nch);
     if (threadIdx.x != 0) return;
+    dyn->heat_sum = S;
+    if (P.slab) return;  // the slabs set heat_inv_norm from their combined sums
     if (heat_sum == 2 || dyn->thermal_on) {
       if (P.heat_power != 0.0f) {
         dyn->heat_inv_norm = S > 0 ? (float)(1.0 / S) : 0.0f;
@@ -360,6 +363,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
   const float inv_gamma = 1.0f / P.tait_gamma;
   const float csf_coeff = 2.0f * P.sigma / (P.rho0[0] + P.rho0[1]);
   const bool iso_walls = P.wall_bc == CRYO_WALL_ISOTHERMAL;
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;
   float vmax_l = 0.0f, amax_l = 0.0f, tv_l = 0.0f, sr_l = 0.0f, nut_l = 0.0f;
 
   // walls (and, without lists, every particle that is not fluid): zero outputs
@@ -626,7 +630,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
     }
     V.a4[i] = f4(acc, a4.w);
 
-    if (what & FORCE_MAXIMA) {
+    if ((what & FORCE_MAXIMA) && owned(own_lo, own_hi, n_sorted, i)) {
       vmax_l = fmaxf(vmax_l, norm(vi));
       const float rm = V.rmin[i];
       const float rr = rm > 0.05f * P.dx ? rm : 0.05f * P.dx;
@@ -677,10 +681,11 @@ template __global__ void k_forces_t<359>(Params, View, int);
 __global__ void __launch_bounds__(kBlock) k_maxima(Params P, View V) {
   DynState* dyn = V.dyn;
   const int n = dyn->n;
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;
   float vmax_l = 0.0f, amax_l = 0.0f, tv_l = 0.0f, sr_l = 0.0f, nut_l = 0.0f;
   PARTICLE_LOOP(i, n) {
     const int ph = ph_of(V.xp[i]);
-    if (!is_fluid(ph)) continue;
+    if (!is_fluid(ph) || !owned(own_lo, own_hi, n_sorted, i)) continue;
     const float4 vT = V.vT[i];
     vmax_l = fmaxf(vmax_l, norm(xyz(vT)));
     const float rm = V.rmin[i];
