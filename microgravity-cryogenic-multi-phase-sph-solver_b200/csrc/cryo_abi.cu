@@ -3226,7 +3226,10 @@ class HostBarrier {
 }  // namespace
 
 struct SlabGroup {
-  static constexpr int kRefreshLayers = 3;  // neighbour layers copied in between steps
+  // Neighbour layers copied in between steps.  A particle moves far less
+  // than a layer (2h) per step, so the ghost layer next to a slab after the
+  // drift holds only particles that were in the two layers before it.
+  static constexpr int kRefreshLayers = 2;
   std::vector<cryo_ctx*> slabs;
   std::vector<int> zb;          // slab r owns cell layers [zb[r], zb[r + 1])
   std::vector<View> live;       // each slab's live arrays at the current point

@@ -434,6 +434,13 @@ __global__ void __launch_bounds__(kBlock) k_split(Params P, View V, Reduce R, co
     V.mrps[dst] = make_float4(0.5f * m, mr.y, mr.z, sig2);
     V.id[dst] = id_base + k;
     V.pc[dst] = make_float4(0.0f, 0.0f, V.pc[dst].z, V.pc[dst].w);
+    if (P.slab) {
+      // The new half had no force pass: the whole tank's arrays hold whatever
+      // an earlier particle left in this slot (and so does the reference),
+      // which a slab cannot know; its slot counts as no wall force.
+      V.fw[dst] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      V.mw[dst] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
   }
   if (last_block(R.ticket) && threadIdx.x == 0) {
     const long long room = (long long)cap - n;

@@ -7,7 +7,7 @@
 // holds its owned layers plus ghost copies of the neighbouring slabs' layers:
 //
 //   * between steps every slab rebuilds its arrays from its owned particles
-//     and the three layers of each neighbour that face it (refresh);
+//     and the two layers of each neighbour that face it (refresh);
 //   * during a step, after every pass whose outputs a later neighbour pass
 //     reads, the ghost layer next to the slab (one cell, the whole support)
 //     is copied from the slab that owns it (halo pull);

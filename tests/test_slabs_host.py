@@ -12,14 +12,14 @@ import pytest
 
 import cryo_cabi as cabi
 
-DEPTH = 3  # layers a slab copies from each neighbour between steps
+DEPTH = 2  # layers a slab copies from each neighbour between steps
 
 
 def test_partition_balances_counts():
     counts = np.array([0, 5, 40, 40, 40, 40, 40, 40, 40, 40, 5, 0])
-    zb = cabi.slab_partition(counts, 3, min_layers=3)
+    zb = cabi.slab_partition(counts, 3, min_layers=2)
     assert zb[0] == 0 and zb[-1] == len(counts)
-    assert np.all(np.diff(zb) >= 3)
+    assert np.all(np.diff(zb) >= 2)
     owned = [counts[zb[r]:zb[r + 1]].sum() for r in range(3)]
     assert sum(owned) == counts.sum()
     assert max(owned) - min(owned) <= 2 * counts.max()
@@ -88,6 +88,17 @@ def layer_slice(tank, arr, z0, z1):
 
 @pytest.mark.parametrize("nslabs", [2, 3, 4])
 def test_slab_orders_match_whole_tank(nslabs):
+    run_model(nslabs, DEPTH)
+
+
+def test_one_refresh_layer_is_not_enough():
+    """With one refresh layer a particle that drifts from the second layer
+    into the ghost layer is missing there: the model must notice."""
+    with pytest.raises(AssertionError):
+        run_model(3, 1)
+
+
+def run_model(nslabs, DEPTH):
     rng = np.random.Generator(np.random.PCG64(7))
     tank = Tank(rng, 400)
     zb = [0] + [NZ * r // nslabs for r in range(1, nslabs)] + [NZ]
