@@ -293,6 +293,11 @@ def main():
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval of the adjoint window")
     ap.add_argument("--only-adjoint", action="store_true",
                     help="run only the adjoint leg (C5 window) and print its record; for profiler launch lists")
+    ap.add_argument("--slabs", type=int, default=0,
+                    help="also step the workload as one tank cut into this many slabs (0 = skip)")
+    ap.add_argument("--slab-devices", default=None,
+                    help="comma-separated device per slab (default: every slab on this rank's device)")
+    ap.add_argument("--slab-steps", type=int, default=50, help="timed steps of the slab leg")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
     args = ap.parse_args()
@@ -432,6 +437,12 @@ def main():
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{k} steps of {label} after 2 warm-up steps ({el:.1f} s, OpenMP)"}
 
+    # one tank over several slabs (halo layers exchanged between passes)
+    slabs = None
+    if rank == 0 and args.slabs > 0 and not args.only_timed:
+        devs = [int(d) for d in args.slab_devices.split(",")] if args.slab_devices else [device] * args.slabs
+        slabs = slab_run(cs, cfg, fluid, p, lo, hi, args.slabs, devs, args.slab_steps, label)
+
     # the adjoint leg last: its window holds several GB until it is released
     adjoint = None
     if rank == 0 and args.adjoint_steps > 0 and not args.only_timed:
@@ -456,6 +467,7 @@ def main():
             "reference_gpu": ref_gpu,
             "batched": batched,
             "adjoint": adjoint,
+            "slabs": slabs,
         }
         print(json.dumps(line))
     if dist:
@@ -575,6 +587,36 @@ def c5_solver(cs, device, dx=0.0034):
     fill.T_liquid = fluid.T_sat + 2.0
     s.build_tank(cs.CylinderTank(0.1, 0.25), fill)
     return s, fluid
+
+
+def slab_run(cs, cfg, fluid, p, lo, hi, nslabs, devices, steps, label):
+    """The workload as one tank cut along z into `nslabs` slabs of cell layers
+    (CryoSPH.SlabSolver), against one Solver on the same inputs: wall clock
+    per step with the device synchronised (the slab steps meet on the host
+    between passes and run without step graphs), particle states compared
+    bit for bit after the timed steps."""
+    import torch
+    one = cs.Solver(cfg, fluid, devices[0])
+    load(one, p, lo, hi)
+    sl = cs.SlabSolver(cfg, fluid, slabs=nslabs, devices=devices)
+    sl.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"], domain_lo=lo,
+                     domain_hi=hi, normal=p["normal"], flags=p["flags"])
+    times = {}
+    for name, obj in (("one_context", one), ("slabs", sl)):
+        obj.run_steps(3)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        obj.run_steps(steps)
+        torch.cuda.synchronize()
+        times[name] = (time.perf_counter() - t0) / steps * 1e3
+    a, b = one.particles(), sl.particles()
+    same = all(np.array_equal(np.asarray(a[k]), np.asarray(b[k])) for k in a)
+    lay = sl.layout()
+    return {"workload": label, "slabs": nslabs, "devices": devices, "steps": steps,
+            "ms_per_step": times["slabs"], "one_context_ms_per_step": times["one_context"],
+            "z_begin": list(lay["z_begin"]), "owned": list(lay["owned"]), "held": list(lay["held"]),
+            "ghost_fraction": sum(lay["held"]) / max(sum(lay["owned"]), 1) - 1.0,
+            "bit_identical": bool(same), "timing": "wall clock, device synchronised"}
 
 
 def adjoint_run(cs, device, steps, every, knots=16):

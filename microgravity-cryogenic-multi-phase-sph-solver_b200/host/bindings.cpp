@@ -537,4 +537,43 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property_readonly("launches_per_step", &Ensemble::launches_per_step)
       .def_property_readonly("stream_handle", &Ensemble::stream_handle)
       .def("diagnostics", &Ensemble::diagnostics, "Diagnostics of every member, in insertion order.");
+
+  // One tank over several slabs (B200 extension).
+  py::class_<SlabSolver>(m, "SlabSolver",
+                         "One tank cut along z into slabs of cell layers, each slab a context on its own device "
+                         "(or several on one); the particles equal a Solver's over the same steps.")
+      .def(py::init<const SolverConfig&, const FluidProperties&, int, const std::vector<int>&>(), py::arg("config"),
+           py::arg("fluid"), py::arg("slabs") = 2, py::arg("devices") = std::vector<int>{})
+      .def("build_tank", &SlabSolver::build_tank, py::arg("geometry"), py::arg("fill") = FillSpec{},
+           "Generates the tank's particles (host generator) and cuts them into the slabs.")
+      .def(
+          "set_particles",
+          [](SlabSolver& s, DArr position, DArr mass, DArr density, DArr temperature, U8Arr phase,
+             const Tuple3& domain_lo, const Tuple3& domain_hi, py::object velocity, py::object normal,
+             py::object flags) {
+            const HostParticles hp = from_arrays(position, mass, density, temperature, phase, velocity, normal, flags);
+            s.set_particles(hp, AABB{to_vec(domain_lo), to_vec(domain_hi)});
+          },
+          py::arg("position"), py::arg("mass"), py::arg("density"), py::arg("temperature"), py::arg("phase"),
+          py::arg("domain_lo"), py::arg("domain_hi"), py::arg("velocity") = py::none(), py::arg("normal") = py::none(),
+          py::arg("flags") = py::none(), "Loads the whole tank's particles (as Solver.set_particles).")
+      .def("step", &SlabSolver::step, py::call_guard<py::gil_scoped_release>())
+      .def("run_steps", &SlabSolver::run_steps, py::arg("n"), py::call_guard<py::gil_scoped_release>())
+      .def("diagnostics", &SlabSolver::diagnostics)
+      .def(
+          "particles", [](const SlabSolver& s) { return particles_dict(s.particles()); },
+          "The whole tank's particles, in the order a Solver's arrays have.")
+      .def_property_readonly("num_particles", &SlabSolver::num_particles)
+      .def_property_readonly("slabs", &SlabSolver::slabs)
+      .def(
+          "layout",
+          [](const SlabSolver& s) {
+            auto [zb, owned, held] = s.layout();
+            py::dict d;
+            d["z_begin"] = zb;
+            d["owned"] = owned;
+            d["held"] = held;
+            return d;
+          },
+          "Cell-layer boundaries and the particles each slab owns and holds (owned + ghost copies).");
 }

@@ -427,6 +427,39 @@ class Ensemble {
   std::vector<Solver*> tanks_;
 };
 
+// One tank cut along z into slabs of cell layers, each slab a context on its
+// own device (or several on one device), halo layers exchanged between
+// passes (no counterpart in the reference).  The particles equal a Solver's
+// over the same steps, in the same order.
+class SlabSolver {
+ public:
+  SlabSolver(const SolverConfig& config, const FluidProperties& fluid, int slabs,
+             const std::vector<int>& devices = {});
+  ~SlabSolver();
+  SlabSolver(const SlabSolver&) = delete;
+  SlabSolver& operator=(const SlabSolver&) = delete;
+
+  void set_particles(const HostParticles& particles, const AABB& domain);
+  void build_tank(const Geometry& geometry, const FillSpec& fill);  // the host lattice generator
+  void step() { run_steps(1); }
+  void run_steps(long long n);
+  Diagnostics diagnostics();
+  HostParticles particles() const;
+  std::size_t num_particles() const;
+  int slabs() const noexcept { return slabs_; }
+  // cell-layer boundaries (slabs + 1 entries), then per slab the particles
+  // it owns and the particles its context holds (owned + ghost copies)
+  std::tuple<std::vector<int>, std::vector<int>, std::vector<int>> layout() const;
+  const SolverConfig& config() const noexcept { return cfg_; }
+
+ private:
+  void check(int rc) const;
+  SolverConfig cfg_;
+  FluidProperties fluid_;
+  cryo_slabs* s_ = nullptr;
+  int slabs_ = 0;
+};
+
 std::string device_name(int device = 0);
 int device_count();
 

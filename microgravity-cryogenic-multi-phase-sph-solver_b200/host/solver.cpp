@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <functional>
 #include <stdexcept>
 
 #include "cryosph.hpp"
@@ -203,9 +204,7 @@ double Solver::next_dt() {
   return dt;
 }
 
-Diagnostics Solver::diagnostics() {
-  cryo_diagnostics_t d{};
-  check(cryo_diagnostics(ctx_, &d));
+static Diagnostics to_diagnostics(const cryo_diagnostics_t& d) {
   Diagnostics o;
   o.time = d.time; o.step = d.step; o.dt = d.dt;
   o.n_total = d.n_total; o.n_liquid = d.n_liquid; o.n_vapor = d.n_vapor; o.n_wall = d.n_wall;
@@ -222,20 +221,33 @@ Diagnostics Solver::diagnostics() {
   return o;
 }
 
-HostParticles Solver::particles() const {
-  const std::size_t n = num_particles();
+Diagnostics Solver::diagnostics() {
+  cryo_diagnostics_t d{};
+  check(cryo_diagnostics(ctx_, &d));
+  return to_diagnostics(d);
+}
+
+static HostParticles download(std::size_t n, const std::function<int(cryo_host_particles_out_t*)>& get) {
   HostParticles h;
   std::vector<float> x(3 * n), v(3 * n), nrm(3 * n);
   h.m.resize(n); h.rho.resize(n); h.T.resize(n); h.phase.resize(n); h.flags.resize(n); h.id.resize(n);
   cryo_host_particles_out_t o{static_cast<int>(n), x.data(), v.data(), nrm.data(), h.m.data(), h.rho.data(),
                               h.T.data(), h.phase.data(), h.flags.data(), h.id.data()};
-  check(cryo_download(ctx_, &o));
+  const int rc = get(&o);
+  if (rc) return h;
   h.x.resize(n); h.v.resize(n); h.nrm.resize(n);
   for (std::size_t i = 0; i < n; ++i) {
     h.x[i] = get3(x.data() + 3 * i);
     h.v[i] = get3(v.data() + 3 * i);
     h.nrm[i] = get3(nrm.data() + 3 * i);
   }
+  return h;
+}
+
+HostParticles Solver::particles() const {
+  int rc = 0;
+  HostParticles h = download(num_particles(), [&](cryo_host_particles_out_t* o) { return rc = cryo_download(ctx_, o); });
+  check(rc);
   return h;
 }
 
@@ -461,5 +473,77 @@ std::string device_name(int device) {
   return buf;
 }
 int device_count() { return cryo_device_count(); }
+
+// ------------------------------------------------------------------ slabs
+SlabSolver::SlabSolver(const SolverConfig& config, const FluidProperties& fluid, int slabs,
+                       const std::vector<int>& devices)
+    : cfg_(config), fluid_(fluid), slabs_(slabs) {
+  if (!devices.empty() && static_cast<int>(devices.size()) != slabs)
+    throw std::invalid_argument("SlabSolver: one device per slab");
+  const cryo_config_t c = cfg_.to_c();
+  const cryo_fluid_t f = fluid_.to_c();
+  const int rc = cryo_slabs_create(&c, &f, slabs, devices.empty() ? nullptr : devices.data(), &s_);
+  if (rc) raise(rc, cryo_slabs_last_error(nullptr));
+}
+
+SlabSolver::~SlabSolver() { cryo_slabs_destroy(s_); }
+
+void SlabSolver::check(int rc) const {
+  if (rc) raise(rc, cryo_slabs_last_error(s_));
+}
+
+void SlabSolver::set_particles(const HostParticles& hp, const AABB& domain) {
+  const int n = static_cast<int>(hp.size());
+  std::vector<float> x(3 * hp.size()), v(3 * hp.size()), nrm(3 * hp.size());
+  for (std::size_t i = 0; i < hp.size(); ++i) {
+    put3(x.data() + 3 * i, hp.x[i]);
+    put3(v.data() + 3 * i, hp.v[i]);
+    put3(nrm.data() + 3 * i, hp.nrm[i]);
+  }
+  cryo_host_particles_t p{n, x.data(), v.data(), nrm.data(), hp.m.data(), hp.rho.data(), hp.T.data(),
+                          hp.phase.data(), hp.flags.data(), hp.id.data()};
+  float lo[3], hi[3];
+  put3(lo, domain.lo);
+  put3(hi, domain.hi);
+  check(cryo_slabs_set_particles(s_, &p, lo, hi));
+}
+
+// Solver::build_tank (sph_solver.cu:430-437) with the host generator.
+void SlabSolver::build_tank(const Geometry& geometry, const FillSpec& fill) {
+  const HostParticles hp = build_tank_particles(geometry, fluid_, cfg_.dx, fill);
+  AABB dom = geometry.bounds();
+  const real pad = (fill.wall_layers + 1) * cfg_.dx;
+  dom.lo = dom.lo - Vec3{pad, pad, pad};
+  dom.hi = dom.hi + Vec3{pad, pad, pad};
+  set_particles(hp, dom);
+}
+
+void SlabSolver::run_steps(long long n) { check(cryo_slabs_run_steps(s_, n)); }
+
+Diagnostics SlabSolver::diagnostics() {
+  cryo_diagnostics_t d{};
+  check(cryo_slabs_diagnostics(s_, &d));
+  return to_diagnostics(d);
+}
+
+std::size_t SlabSolver::num_particles() const {
+  int n = 0;
+  check(cryo_slabs_num_particles(s_, &n));
+  return static_cast<std::size_t>(n);
+}
+
+HostParticles SlabSolver::particles() const {
+  int rc = 0;
+  HostParticles h =
+      download(num_particles(), [&](cryo_host_particles_out_t* o) { return rc = cryo_slabs_download(s_, o); });
+  check(rc);
+  return h;
+}
+
+std::tuple<std::vector<int>, std::vector<int>, std::vector<int>> SlabSolver::layout() const {
+  std::vector<int> zb(slabs_ + 1), owned(slabs_), held(slabs_);
+  check(cryo_slabs_layout(s_, zb.data(), owned.data(), held.data()));
+  return {zb, owned, held};
+}
 
 }  // namespace cryosph
