@@ -629,6 +629,8 @@ void cryo_ctx::configure_grid(const float* lo, const float* hi) {
   const long long cells = (long long)P.nx * P.ny * P.nz;
   if (cells > 400000000LL) throw std::runtime_error("SpatialHash: grid too large; increase the cell size");
   P.num_cells = (int)cells;
+  P.slab_z0 = 0;
+  P.slab_z1 = P.nz;
   P.inv_cell = 1.0f / cell;
   int bits = 0;
   while (bits < 32 && ((uint64_t)1 << bits) <= (uint64_t)P.num_cells) ++bits;  // sentinel fits
@@ -672,7 +674,7 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
   sorted_perm = vin;
   const int GC = std::max(1, std::min((P.num_cells + 1 + kBlock - 1) / kBlock, sm_count * 16));
   LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
-  LAUNCH(k_gather, G, kBlock, view(src), view(1 - src), vin, reduce());
+  LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce());
   if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
 }
 
@@ -3579,6 +3581,8 @@ int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, cons
         if (layer[i] >= z0 && layer[i] < z1) idx.push_back(i);
       const int m = (int)idx.size();
       c->begin_load(std::max(m, 1), vap, lo, hi);
+      c->P.slab_z0 = G.zb[r];  // the passes run over owned particles only
+      c->P.slab_z1 = G.zb[r + 1];
       std::vector<float4> xp(m), vT(m), vt(m), nrm(m), mrps(m);
       std::vector<uint32_t> id(m);
       for (int k = 0; k < m; ++k) {

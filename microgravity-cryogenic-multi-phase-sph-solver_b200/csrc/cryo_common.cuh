@@ -119,6 +119,9 @@ struct Params {
   // 1: this context is one slab of a decomposed tank; the heat normalisation
   // and the ullage state come from the slabs' combined sums
   int slab;
+  // cell layers [slab_z0, slab_z1) this context owns (0, nz: the whole tank);
+  // the phase index lists hold only the owned particles
+  int slab_z0, slab_z1;
 };
 
 // Capacity of the per-particle neighbour list; a particle with more
@@ -510,6 +513,12 @@ struct Range {
   int count;
 };
 __device__ inline int particle_at(const Range& r, int t) { return r.idx ? __ldg(r.idx + t) : t; }
+// Sorted index range of the owned cell layers (after the cell table is built).
+__device__ inline void owned_layers(const Params& P, const int* cell_begin, int& lo, int& hi) {
+  const int L = P.nx * P.ny;
+  lo = __ldg(cell_begin + P.slab_z0 * L);
+  hi = __ldg(cell_begin + P.slab_z1 * L);
+}
 __device__ inline Range fluid_range(const Params& P, const View& V) {
   return P.use_lists ? Range{V.fluid_idx, V.dyn->n_fluid_list} : Range{nullptr, V.dyn->n};
 }

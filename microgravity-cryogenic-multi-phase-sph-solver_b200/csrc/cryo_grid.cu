@@ -185,14 +185,18 @@ __global__ void k_cells(Params P, const uint32_t* __restrict__ keys, DynState* d
 
 // Reorder gather of the persistent arrays (spatial_hash.cu:116-138), fused
 // into one pass: dst[i] = src[perm[i]] for i < n_alive; then n = n_alive.
-// Also counts fluid and wall particles per chunk; the last block turns the
-// counts into the chunk offsets of the ordered phase index lists
-// (partials rows 0 and 1) and their lengths.
-__global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uint32_t* __restrict__ perm, Reduce R) {
+// Also counts the owned fluid and wall particles per chunk (every particle
+// unless the context is one slab of a tank); the last block turns the counts
+// into the chunk offsets of the ordered phase index lists (partials rows 0
+// and 1) and their lengths.
+__global__ void __launch_bounds__(kBlock) k_gather(Params P, View src, View dst, const uint32_t* __restrict__ perm,
+                                                   Reduce R) {
   __shared__ double sh[2 * kBlock / 32];
   DynState* dyn = src.dyn;
   const int na = dyn->n_alive;
   const int nch = num_chunks(na);
+  int own_lo, own_hi;
+  owned_layers(P, src.cell_begin, own_lo, own_hi);
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double cnt[2] = {0.0, 0.0};
@@ -206,8 +210,9 @@ __global__ void __launch_bounds__(kBlock) k_gather(View src, View dst, const uin
       dst.mrps[i] = src.mrps[j];
       dst.id[i] = src.id[j];
       const int ph = ph_of(xp);
-      if (is_fluid(ph)) cnt[0] = 1.0;
-      else if (ph == kWall) cnt[1] = 1.0;
+      const bool own = i >= own_lo && i < own_hi;
+      if (is_fluid(ph) && own) cnt[0] = 1.0;
+      else if (ph == kWall && own) cnt[1] = 1.0;
     }
     publish_chunk<2>(R, c, cnt, sh);
   }
@@ -244,8 +249,11 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
     const float4 xpi = valid ? V.xp[i] : make_float4(0, 0, 0, 0);
     const int ph = valid ? ph_of(xpi) : kDead;
     if (mode != LISTS_ONLY) {
-      // ordered phase lists: chunk offset + rank inside the chunk
-      const bool isf = valid && is_fluid(ph), isw = valid && ph == kWall;
+      // ordered phase lists of the owned particles: chunk offset + rank inside the chunk
+      int own_lo, own_hi;
+      owned_layers(P, V.cell_begin, own_lo, own_hi);
+      const bool own = i >= own_lo && i < own_hi;
+      const bool isf = valid && own && is_fluid(ph), isw = valid && own && ph == kWall;
       const unsigned bf = __ballot_sync(0xffffffffu, isf), bw = __ballot_sync(0xffffffffu, isw);
       if (lane == 0) {
         wcnt[0][warp] = __popc(bf);
