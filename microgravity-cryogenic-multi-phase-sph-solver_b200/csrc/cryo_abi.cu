@@ -148,6 +148,7 @@ struct cryo_ctx {
 
   // grid
   int* cell_begin = nullptr;
+  uint8_t* cell_fluid = nullptr;  // 1: a fluid particle was sorted into the cell
   int cell_cap = 0;
 
   // scalar block
@@ -300,6 +301,7 @@ struct cryo_ctx {
     if (stream) cudaStreamSynchronize(stream);
     arena.release();
     if (cell_begin) cudaFree(cell_begin);
+    if (cell_fluid) cudaFree(cell_fluid);
     if (dyn) cudaFree(dyn);
     if (hdyn) cudaFreeHost(hdyn);
     if (diag_host) cudaFreeHost(diag_host);
@@ -321,6 +323,7 @@ struct cryo_ctx {
     V.rmin = rmin; V.wall_w = wall_w; V.heat_w = heat_w; V.nu_t = nu_t;
     V.aux = aux;
     V.cell_begin = cell_begin;
+    V.cell_fluid = cell_fluid;
     V.dyn = dyn;
     V.man_t = man_t; V.man_acc = man_acc; V.man_omega = man_omega;
     V.partials = partials;
@@ -637,7 +640,9 @@ void cryo_ctx::configure_grid(const float* lo, const float* hi) {
   P.key_bits = std::max(bits, 1);
   if (cell_cap < P.num_cells + 2) {
     if (cell_begin) CK(cudaFree(cell_begin));
+    if (cell_fluid) CK(cudaFree(cell_fluid));
     CK(cudaMalloc(&cell_begin, (size_t)(P.num_cells + 2) * sizeof(int)));
+    CK(cudaMalloc(&cell_fluid, (size_t)(P.num_cells + 2)));
     cell_cap = P.num_cells + 2;
   }
   CK(cudaMemsetAsync(cell_begin, 0, (size_t)(P.num_cells + 2) * sizeof(int), stream));
@@ -674,6 +679,7 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
   sorted_perm = vin;
   const int GC = std::max(1, std::min((P.num_cells + 1 + kBlock - 1) / kBlock, sm_count * 16));
   LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
+  if (P.use_lists) CK(cudaMemsetAsync(cell_fluid, 0, (size_t)P.num_cells, stream));
   LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce());
   if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
 }

@@ -222,6 +222,7 @@ struct View {
   // same operations (written by the density pass, valid until the kick)
   float4* aux;
   const int* cell_begin;  // dense cell prefix table, num_cells + 1 entries
+  uint8_t* cell_fluid;    // per cell: 1 if a fluid particle was sorted into it (lists mode)
   DynState* dyn;
   // maneuver table
   const double* man_t;

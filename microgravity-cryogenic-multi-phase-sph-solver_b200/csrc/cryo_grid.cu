@@ -213,6 +213,7 @@ __global__ void __launch_bounds__(kBlock) k_gather(Params P, View src, View dst,
       const bool own = i >= own_lo && i < own_hi;
       if (is_fluid(ph) && own) cnt[0] = 1.0;
       else if (ph == kWall && own) cnt[1] = 1.0;
+      if (P.use_lists && is_fluid(ph)) dst.cell_fluid[cell_index(P, xyz(xp))] = 1;
     }
     publish_chunk<2>(R, c, cnt, sh);
   }
@@ -281,12 +282,22 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
       dst[0] = make_int4(stage[0][t], stage[1][t], stage[2][t], stage[3][t]);
       dst[1] = make_int4(stage[4][t], stage[5][t], stage[6][t], stage[7][t]);
     };
+    // A wall's list holds its fluid neighbours only: every pass that walks
+    // a wall's neighbours (the wall boundary pass and its reverse) skips the
+    // other walls, so the fluid entries in their order are all it needs;
+    // rows of cells with no fluid are not scanned.
+    const bool wall_i = ph == kWall;
     const CellWindow W(P, xi);
     for (int z = W.z0; z <= W.z1; ++z) {
       for (int y = W.y0; y <= W.y1; ++y) {
         int xs, xe;
         if (!W.row(P, y, z, xs, xe)) continue;
         const int row = (z * P.ny + y) * P.nx;
+        if (wall_i) {
+          bool any = false;
+          for (int x = xs; x <= xe; ++x) any |= V.cell_fluid[row + x] != 0;
+          if (!any) continue;
+        }
         const int s = __ldg(V.cell_begin + row + xs);
         const int e = __ldg(V.cell_begin + row + xe + 1);
         // candidates in groups of LIST_GROUP: all loads issued before the
@@ -294,7 +305,7 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
         auto test = [&](const float4& xj, int j) {
           const V3 rij = xi - xyz(xj);
           const float r2 = norm2(rij);
-          if (r2 < P.support2) {
+          if (r2 < P.support2 && (!wall_i || is_fluid(ph_of(xj)))) {
             if (cnt < kMaxNbr) {
               stage[cnt & (kNbrChunk - 1)][t] = j;
               if ((cnt & (kNbrChunk - 1)) == kNbrChunk - 1) store_chunk(cnt / kNbrChunk);
