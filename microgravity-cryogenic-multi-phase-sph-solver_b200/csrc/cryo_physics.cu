@@ -169,29 +169,42 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
         const float ci = ph == kLiquid ? 1.0f : 0.0f;
         V3 gradc{0, 0, 0}, wall_n{0, 0, 0}, akn{0, 0, 0}, gradphi{0, 0, 0};
         float s_all = 0, s_other = 0, ww = 0, hw = 0;
-        for_each_nbr_pf(P, V, i, xi, V.aux, [&](int j, float4 xj, V3 rij, float r2, const float4& auxj) {
-          const float r = sqrtf(r2);
-          const float w = kernel_W(P, r);
-          const int phj = ph_of(xj);
-          if (phj == kWall) {
-            const float vw = P.vol0 * w;
-            ww += vw;
-            if (fl_of(xj) & kHeated) hw += vw;
-            const float4 nj = __ldg(V.nrm + j);
-            wall_n += xyz(nj) * vw;
-            gradphi += kernel_gradW(P, rij, r) * P.vol0;
-            if (P.wall_colour) gradc += kernel_gradW(P, rij, r) * (P.vol0 * (nj.w - ci));
-            return;
-          }
-          const float Vj = auxj.x;  // m_j / rho_j
-          s_all += Vj * w;
-          if (phj != ph) s_other += Vj * w;
-          if (j == i) return;
-          const V3 gw = kernel_gradW(P, rij, r);
-          const float cj = phj == kLiquid ? 1.0f : 0.0f;
-          gradc += gw * (Vj * (cj - ci));
-          if (phj == kLiquid) akn += gw * Vj;
-        });
+        auto wall_term = [&](int j, float4 xj, V3 rij, float r) {
+          const float vw = P.vol0 * kernel_W(P, r);
+          ww += vw;
+          if (fl_of(xj) & kHeated) hw += vw;
+          const float4 nj = __ldg(V.nrm + j);
+          wall_n += xyz(nj) * vw;
+          gradphi += kernel_gradW(P, rij, r) * P.vol0;
+          if (P.wall_colour) gradc += kernel_gradW(P, rij, r) * (P.vol0 * (nj.w - ci));
+        };
+        if (!TAPE && !P.has_vapor && P.st_model != CRYO_ST_AKINCI) {
+          // A tank without vapour: every fluid neighbour is liquid, so its
+          // colour term is gw * (V_j * 0) (a zero, which leaves the sum as
+          // it is) and s_other stays 0, making alpha 0 whatever s_all is;
+          // only the wall neighbours change the outputs.
+          for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
+            if (ph_of(xj) == kWall) wall_term(j, xj, rij, sqrtf(r2));
+          });
+        } else {
+          for_each_nbr_pf(P, V, i, xi, V.aux, [&](int j, float4 xj, V3 rij, float r2, const float4& auxj) {
+            const float r = sqrtf(r2);
+            const int phj = ph_of(xj);
+            if (phj == kWall) {
+              wall_term(j, xj, rij, r);
+              return;
+            }
+            const float w = kernel_W(P, r);
+            const float Vj = auxj.x;  // m_j / rho_j
+            s_all += Vj * w;
+            if (phj != ph) s_other += Vj * w;
+            if (j == i) return;
+            const V3 gw = kernel_gradW(P, rij, r);
+            const float cj = phj == kLiquid ? 1.0f : 0.0f;
+            gradc += gw * (Vj * (cj - ci));
+            if (phj == kLiquid) akn += gw * Vj;
+          });
+        }
         if (TAPE) {
           const int tn = V.tape_n;
           V.tape[3 * tn + i] = f4(gradc, s_all);
