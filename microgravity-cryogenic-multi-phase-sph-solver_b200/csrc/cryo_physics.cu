@@ -199,6 +199,10 @@ __global__ void __launch_bounds__(kBlock) k_interface(Params P, View V, Reduce R
             s_all += Vj * w;
             if (phj != ph) s_other += Vj * w;
             if (j == i) return;
+            // a neighbour of the same phase adds gw * (V_j * 0) to the colour
+            // gradient, a zero that leaves the sum as it is; only Akinci's
+            // normal needs its gradient
+            if (phj == ph && P.st_model != CRYO_ST_AKINCI) return;
             const V3 gw = kernel_gradW(P, rij, r);
             const float cj = phj == kLiquid ? 1.0f : 0.0f;
             gradc += gw * (Vj * (cj - ci));
