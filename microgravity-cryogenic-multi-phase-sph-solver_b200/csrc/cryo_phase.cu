@@ -271,6 +271,9 @@ __global__ void __launch_bounds__(kBlock) k_rebalance1(Params P, View V, int gat
     for_each_nbr_pf(P, V, i, xyz(xpi), V.mrps, [&](int j, float4 xj, V3, float r2, const float4& mrj) {
       if (j == i || ph_of(xj) != kVapor) return;
       const float mj = mrj.x;
+      // equal masses give flow = +0, and every sum below gains a zero that
+      // leaves it as it is
+      if (mj == mi) return;
       const float flow = beta * P.vol0 * kernel_W(P, sqrtf(r2)) * (mj - mi);
       const bool from_j = flow > 0.0f;
       dm += flow;

@@ -524,9 +524,12 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
         if (do_A && r2 > 0.0f) accA -= (rij / r) * (P.akinci_beta * psi * akinci_adhesion(r, akc));
         if (do_D) div += P.vol0 * dot(veli, gw);
         if (thermal && iso_walls) {
-          const float kij = 2.0f * ki;
-          const float rgw = r * dW;
-          q += Vi * P.vol0 * kij * (Ti - __ldg(V.vT + j).w) * rgw / (r2 + eta2);
+          const float Tw = __ldg(V.vT + j).w;
+          if (Ti != Tw) {  // equal temperatures: a zero term
+            const float kij = 2.0f * ki;
+            const float rgw = r * dW;
+            q += Vi * P.vol0 * kij * (Ti - Tw) * rgw / (r2 + eta2);
+          }
         }
         return;
       }
@@ -594,7 +597,8 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
         div += Vj * dot(veli - velj, gw);
         if (phj == ph) diff += Vj * 2.0f * (rhoj - rhoi) * dot(-rij, gw) / (r2 + eta2);
       }
-      if (thermal) {
+      // equal temperatures give a zero term that leaves q as it is
+      if (thermal && Ti != vTj.w) {
         const float kij = k_pair[phase_index(phj)];
         const float rgw = r * dW;
         q += Vi * Vj * kij * (Ti - vTj.w) * rgw / (r2 + eta2);
