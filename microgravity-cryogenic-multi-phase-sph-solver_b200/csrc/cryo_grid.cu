@@ -290,8 +290,10 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
     const CellWindow W(P, xi);
     for (int z = W.z0; z <= W.z1; ++z) {
       for (int y = W.y0; y <= W.y1; ++y) {
-        int xs, xe;
-        if (!W.row(P, y, z, xs, xe)) continue;
+        // every row of the 27-cell block, whole: lanes in one cell then walk
+        // the same ranges (dropping rows beyond the support radius, as the
+        // cell scan does, saves candidates but splits the warp more)
+        const int xs = W.x0, xe = W.x1;
         const int row = (z * P.ny + y) * P.nx;
         if (wall_i) {
           bool any = false;
