@@ -472,7 +472,9 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
     for (int qq = 0; qq < 2; ++qq) k_pair[qq] = 4.0f * ki * P.k[qq] / (ki + P.k[qq]);
     float q = 0.0f;
 
-    for_each_nbr(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
+    constexpr int kUnroll = (FORCES_UNROLL_HEAVY > 1 && WHAT >= 0 && (WHAT & (FORCE_CSF | FORCE_THERMAL)))
+                                ? FORCES_UNROLL_HEAVY : 1;
+    for_each_nbr<kUnroll>(P, V, i, xi, [&](int j, float4 xj, V3 rij, float r2) {
       if (j == i) return;
       const float r = sqrtf(r2);
       const float dW = kernel_dWdr(P, r);
