@@ -3395,14 +3395,14 @@ struct SlabGroup {
     }
   }
 
-  ~SlabGroup() {
+  ~SlabGroup() {  // also after a failed create: slabs not made yet are null
     for (cryo_ctx* c : slabs)
-      if (c->stream) cudaStreamSynchronize(c->stream);
+      if (c && c->stream) cudaStreamSynchronize(c->stream);
     for (size_t r = 0; r < slabs.size(); ++r) {
-      if (spare[r]) cudaFree(spare[r]);
-      if (dyn_table[r]) cudaFree(dyn_table[r]);
-      if (ev_a[r]) cudaEventDestroy(ev_a[r]);
-      if (ev_b[r]) cudaEventDestroy(ev_b[r]);
+      if (r < spare.size() && spare[r]) cudaFree(spare[r]);
+      if (r < dyn_table.size() && dyn_table[r]) cudaFree(dyn_table[r]);
+      if (r < ev_a.size() && ev_a[r]) cudaEventDestroy(ev_a[r]);
+      if (r < ev_b.size() && ev_b[r]) cudaEventDestroy(ev_b[r]);
     }
     for (cryo_ctx* c : slabs) delete c;
   }

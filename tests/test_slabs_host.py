@@ -150,3 +150,15 @@ def run_model(nslabs, DEPTH):
                     tank.dead.add(i)
         # the whole tank's children come in the slabs' order, as their ids do
         assert whole_children == sum(children, [])
+
+
+def test_slabs_create_rejects_bad_arguments_without_a_device():
+    """Argument checks come before any device call (no GPU needed)."""
+    L = cabi.load()
+    h = cabi.C.c_void_p()
+    fl = cabi.py_fluid(cabi.FLUID_LN2)
+    rc = L.cryo_slabs_create(cabi.C.byref(cabi.py_config(dx=0.004)), cabi.C.byref(fl), 0, None, cabi.C.byref(h))
+    assert rc == cabi.CRYO_EINVAL and not h.value
+    assert b"slab" in L.cryo_slabs_last_error(None)
+    rc = L.cryo_slabs_create(cabi.C.byref(cabi.py_config(dx=-1.0)), cabi.C.byref(fl), 2, None, cabi.C.byref(h))
+    assert rc == cabi.CRYO_EINVAL and not h.value
