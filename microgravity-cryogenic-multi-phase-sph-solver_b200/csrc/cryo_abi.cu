@@ -3621,6 +3621,7 @@ int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, cons
 int cryo_slabs_layout(cryo_slabs* s, int* z_begin, int* owned, int* held) {
   return slab_guard(s, [&] {
     SlabGroup& G = *s->g;
+    if (!z_begin) throw std::invalid_argument("cryo_slabs_layout: z_begin is required");
     if (G.zb.empty()) throw std::runtime_error("slabs: no particles loaded");
     G.initialize();
     for (int r = 0; r <= G.count(); ++r) z_begin[r] = G.zb[r];
