@@ -22,7 +22,7 @@ the roofline of the dominant kernel (per-kernel CUDA-event times from a
 profiled run, algorithmic bytes from cryo_roofline.py, DRAM traffic from the
 committed ncu summary), SM clocks sampled during the timed region, the
 reference's own CPU implementation timed on this host (rank 0, N=1), and
-`batched`: BASELINE config 4 (64 seeded tanks of 5k-200k particles) advanced
+`batched`: the 64-tank ensemble (seeded tanks of 5k-200k particles) advanced
 by one cs.Ensemble -- one graph launch per ensemble step, branch count
 autotuned -- against the same tanks stepped back to back by plain Solvers,
 with every tank's diagnostics compared bit for bit.  Under torchrun the
@@ -111,7 +111,7 @@ def workload(name, cs, dx_override=None):
 
 
 def c4_tanks(cs, count=64, n_lo=5_000, n_hi=200_000, seed=SEED):
-    """BASELINE config 4 as seeded synthetic tanks: shape cylinder or sphere,
+    """The 64-tank ensemble as seeded synthetic tanks: shape cylinder or sphere,
     radius U[0.03, 0.3] m (cylinder height 2R x U[1, 2.5]), fill U[0.2, 0.8],
     dx chosen so the particle count (walls included) is log-uniform in
     [n_lo, n_hi], fluid LN2 / LOX / LCH4, gravity 1e-4 g, a lateral pulse of
@@ -289,10 +289,10 @@ def main():
                     help="steps of the batched-ensemble comparison (0 = skip it)")
     ap.add_argument("--batched-tanks", type=int, default=64)
     ap.add_argument("--adjoint-steps", type=int, default=400,
-                    help="steps of the differentiated C5 window (0 = skip the adjoint leg)")
+                    help="steps of the differentiated LN2 boil-off window (0 = skip the adjoint leg)")
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval of the adjoint window")
     ap.add_argument("--only-adjoint", action="store_true",
-                    help="run only the adjoint leg (C5 window) and print its record; for profiler launch lists")
+                    help="run only the adjoint leg (LN2 boil-off window) and print its record; for profiler launch lists")
     ap.add_argument("--slabs", type=int, default=0,
                     help="also step the workload as one tank cut into this many slabs (0 = skip)")
     ap.add_argument("--slab-devices", default=None,
@@ -396,7 +396,7 @@ def main():
         # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
         roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
 
-    # ---- batched ensemble (config 4): tanks sharded over ranks, no collective in the step
+    # ---- batched ensemble (64 tanks): tanks sharded over ranks, no collective in the step
     batched = None
     if args.batched_steps > 0 and not args.only_timed:
         import cryo_shard
@@ -565,7 +565,7 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
 
 
 def c5_solver(cs, device, dx=0.0034):
-    """BASELINE config 5 (differentiation): closed LN2 cylinder R 0.1 m, H
+    """The differentiation workload: closed LN2 cylinder R 0.1 m, H
     0.25 m, dx 3.4 mm, fill 0.5, 2 K superheat, Lee 5 1/s both ways, 20 W
     heater, 1e-4 g; a fixed step of 1 ms and a pinned sound speed (0.5 m/s),
     and no splitting or merging inside the differentiated window."""
@@ -620,7 +620,7 @@ def slab_run(cs, cfg, fluid, p, lo, hi, nslabs, devices, steps, label):
 
 
 def adjoint_run(cs, device, steps, every, knots=16):
-    """gradients of the time-integrated slosh force and
+    """The LN2 boil-off window: gradients of the time-integrated slosh force and
     moment and the final ullage pressure with respect to the surface tension,
     the contact angle, the Lee coefficient and 16 piecewise-constant lateral
     frame-acceleration knots (seeded U[-0.05, 0.05] m/s^2), through the
@@ -721,7 +721,7 @@ def adjoint_run(cs, device, steps, every, knots=16):
 
 
 def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
-    """the tanks advanced together by one cs.Ensemble (one
+    """The 64-tank ensemble: the tanks advanced together by one cs.Ensemble (one
     graph launch per ensemble step, branch count autotuned) against the same
     tanks stepped back to back by plain Solvers.  Both sides take the same
     total number of steps, so every tank's diagnostics can be compared bit for

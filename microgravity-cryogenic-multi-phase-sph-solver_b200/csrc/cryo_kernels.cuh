@@ -183,7 +183,8 @@ constexpr int forces_min_blocks(int what) {
 // Neighbour-list build: candidate positions loaded per group, and the block
 // count per SM the register cap keeps resident.
 // Neighbour-loop unroll of the force-pass variants with surface tension or
-// heat (the two-phase tanks): 2 takes C3 3 % faster, no spills.
+// heat (the two-phase tanks): 2 takes the 4 M-particle LH2 sphere 3 % faster,
+// no spills.
 #ifndef FORCES_UNROLL_HEAVY
 #define FORCES_UNROLL_HEAVY 2
 #endif

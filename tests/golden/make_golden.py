@@ -8,7 +8,7 @@ Fixtures (numpy .npz, small):
   box_split.npz   closed LN2 box with superheat and a low split ratio: the
                   jittered input, and after 1 and 200 steps every per-particle
                   field plus the diagnostics (splits start near step 190)
-  c1_pass.npz     the C1 cylinder: input, then after the first grid build the
+  c1_pass.npz     the LN2 cylinder (R 0.05 m, dx 4 mm): input, then after the first grid build the
                   cell tables and neighbour counts/id sums (neighbor_stats,
                   spatial_hash.cu:140-171)
   cloud.npz       a random cloud (3000 points, seed 7, radius 0.08) as in

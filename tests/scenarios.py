@@ -113,8 +113,8 @@ def options():
 
 
 def lh2_sphere():
-    """C3's physics on a small sphere: closed LH2 tank R 0.05 m, fill 0.5,
-    1e-4 g (the BASELINE C3 configuration at R 0.5 m, scaled to a test size)."""
+    """The LH2 sphere physics on a small sphere: closed LH2 tank R 0.05 m, fill 0.5,
+    1e-4 g (the LH2 sphere workload of R 0.5 m, scaled to a test size)."""
     fl = cabi.py_fluid(cabi.FLUID_LH2)
     cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1)
     parts, lo, hi = tank([(refpy.SPHERE, 0, 0, (0.05, 0, 0))], fl, 0.004, refpy.make_fill(fill_fraction=0.5))
@@ -122,7 +122,7 @@ def lh2_sphere():
 
 
 def ln2_boiloff():
-    """C5's physics on a small cylinder: closed LN2 tank R 0.03 m, H 0.075 m,
+    """The LN2 boil-off physics on a small cylinder: closed LN2 tank R 0.03 m, H 0.075 m,
     fill 0.5, 2 K superheat, Lee coefficient 5, 20 W heater, 1e-4 g."""
     fl = cabi.py_fluid(cabi.FLUID_LN2)
     cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1, lee_evaporation=5, heater_power=20.0)
@@ -132,7 +132,7 @@ def ln2_boiloff():
 
 
 def lch4_box():
-    """A closed methane tank with superheated liquid (one of the C4 presets)."""
+    """A closed methane tank with superheated liquid (one of the ensemble's fluid presets)."""
     fl = cabi.py_fluid(cabi.FLUID_LCH4)
     cfg = cabi.py_config(dx=0.004, gravity=(0, 0, -9.81e-4), thermo_mode=1, lee_evaporation=2, lee_condensation=2,
                          velocity_scale=1, contact_angle_deg=20)

@@ -39,7 +39,7 @@ FROZEN = dict(split_ratio=1000.0, merge_ratio=0.0)  # no topology change inside 
 
 
 def weak_case():
-    """C5's physics on a small cylinder (R 0.03 m, H 0.075 m, dx 4 mm): LN2,
+    """The LN2 boil-off physics on a small cylinder (R 0.03 m, H 0.075 m, dx 4 mm): LN2,
     fill 0.5, 2 K superheat, Lee 5, 20 W heater, 1e-4 g, contact angle 60."""
     cfg, fl, parts, lo, hi = S.ln2_boiloff()
     cfg.update(fixed_dt=DT, sound_speed=0.5, lee_condensation=5.0, contact_angle_deg=60.0, **FROZEN)

@@ -80,7 +80,7 @@ def test_device_lattice_steps_like_host_lattice(cuda_device):
 
 
 def test_device_lattice_timing_large_sphere(cuda_device):
-    """The BASELINE C3 sphere (R 0.5 m, dx 5.2 mm, ~4 M particles), both ways."""
+    """The LH2 sphere workload (R 0.5 m, dx 5.2 mm, ~4 M particles), both ways."""
     geo, f, dx = cs.SphereTank(0.5), fill(), 0.0052
     t0 = time.perf_counter()
     dev = build(geo, f, dx, True)
