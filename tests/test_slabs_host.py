@@ -162,3 +162,28 @@ def test_slabs_create_rejects_bad_arguments_without_a_device():
     assert b"slab" in L.cryo_slabs_last_error(None)
     rc = L.cryo_slabs_create(cabi.C.byref(cabi.py_config(dx=-1.0)), cabi.C.byref(fl), 2, None, cabi.C.byref(h))
     assert rc == cabi.CRYO_EINVAL and not h.value
+
+
+@pytest.mark.parametrize("seed", range(20))
+def test_partition_properties_random(seed):
+    """Random layer counts: cuts increase, every slab keeps min_layers, and
+    each cut lies where the running count first passes its share (or at the
+    nearest cut the thickness rule allows)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    nz = int(rng.integers(6, 80))
+    nslabs = int(rng.integers(1, max(2, nz // 3) + 1))
+    min_layers = int(rng.integers(1, nz // nslabs + 1))
+    counts = rng.integers(0, 1000, size=nz) * (rng.random(nz) < 0.8)
+    zb = cabi.slab_partition(counts, nslabs, min_layers=min_layers)
+    assert zb[0] == 0 and zb[-1] == nz
+    assert np.all(np.diff(zb) >= min_layers)
+    total = int(counts.sum())
+    cum = np.concatenate([[0], np.cumsum(counts)])
+    for r in range(1, nslabs):
+        target = (total * r + nslabs // 2) // nslabs
+        lo = zb[r - 1] + min_layers
+        hi = nz - (nslabs - r) * min_layers
+        assert lo <= zb[r] <= hi
+        # greedy: stops at the first layer whose inclusion would pass the target
+        if lo < zb[r] < hi:
+            assert cum[zb[r]] <= target < cum[zb[r] + 1]
