@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
     const int i = c * kChunk + threadIdx.x;
     double s[3] = {0.0, 0.0, 0.0};
-    if (i < n) {
+    if (i < n && owned(own_lo, own_hi, n_sorted, i)) {  // a slab skips its ghosts
       const float4 xpi = V.xp[i];
       const int fl = fl_of(xpi);
       if (fl & kSource) {
@@ -177,8 +177,7 @@ __global__ void __launch_bounds__(kBlock) k_pc_normalize(Params P, View V, Reduc
           if (pc.x > cap) pc.x = cap;
         }
         V.pc[i] = pc;
-        if (!owned(own_lo, own_hi, n_sorted, i)) {
-        } else if (!(fl & kDying)) {
+        if (!(fl & kDying)) {
           if (fl & kTargetVapor) s[0] = (double)pc.x;
           else s[1] = (double)pc.x;
         } else if (pc.x > 0.0f) {
@@ -205,7 +204,9 @@ __global__ void __launch_bounds__(kBlock) k_pc_apply(Params P, View V, int gated
   const DynState* dyn = V.dyn;
   if (gated && !dyn->phase_change_on) return;
   const int n = dyn->n;
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     const float4 xpi = V.xp[i];
     const int ph = ph_of(xpi);
     if (!is_fluid(ph)) continue;
@@ -253,7 +254,9 @@ __global__ void __launch_bounds__(kBlock) k_rebalance1(Params P, View V, int gat
   if (gated && !dyn->phase_change_on) return;
   const int n = dyn->n;
   const float beta = P.vapor_rebalance;
+  const int own_lo = dyn->own_lo, own_hi = dyn->own_hi, n_sorted = dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     const float4 xpi = V.xp[i];
     const float kap = V.ns4[i].w;
     const float wn = V.pc[i].z;

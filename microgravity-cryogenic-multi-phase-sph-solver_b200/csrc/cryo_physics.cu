@@ -283,7 +283,9 @@ template __global__ void k_interface<1>(Params, View, Reduce, int);
 // compute_sps_viscosity (navier_stokes.cu:71-119)
 __global__ void __launch_bounds__(kBlock) k_sps(Params P, View V) {
   const int n = V.dyn->n;
+  const int own_lo = V.dyn->own_lo, own_hi = V.dyn->own_hi, n_sorted = V.dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     const float4 xpi = V.xp[i];
     if (!is_fluid(ph_of(xpi))) {
       V.nu_t[i] = 0.0f;
@@ -329,7 +331,9 @@ __global__ void __launch_bounds__(kBlock) k_sps(Params P, View V) {
 // smooth_interface_normals (surface_tension.cu:87-118)
 __global__ void __launch_bounds__(kBlock) k_smooth_normals(Params P, View V) {
   const int n = V.dyn->n;
+  const int own_lo = V.dyn->own_lo, own_hi = V.dyn->own_hi, n_sorted = V.dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     const float4 xpi = V.xp[i];
     if (!is_fluid(ph_of(xpi))) continue;
     const V3 gi = xyz(V.nrm[i]);
@@ -742,7 +746,9 @@ __global__ void __launch_bounds__(kBlock) k_shift_compute(Params P, View V) {
   const float w_dx = kernel_W(P, P.dx);
   const float coeff = P.shift_strength * mach * 4.0f * h * h;
   const float cap = 0.1f * P.dx;
+  const int own_lo = V.dyn->own_lo, own_hi = V.dyn->own_hi, n_sorted = V.dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     const float kap = V.ns4[i].w;
     V.ns4[i] = make_float4(0.0f, 0.0f, 0.0f, kap);
     const float4 xpi = V.xp[i];
@@ -780,7 +786,9 @@ __global__ void __launch_bounds__(kBlock) k_shift_compute(Params P, View V) {
 // apply_particle_shifting, pass 2 (SPH_kernels.cu:154-159).
 __global__ void __launch_bounds__(kBlock) k_shift_apply(Params P, View V) {
   const int n = V.dyn->n;
+  const int own_lo = V.dyn->own_lo, own_hi = V.dyn->own_hi, n_sorted = V.dyn->n_sorted;  // a slab skips its ghosts
   PARTICLE_LOOP(i, n) {
+    if (!owned(own_lo, own_hi, n_sorted, i)) continue;
     float4 xp = V.xp[i];
     if (!is_fluid(ph_of(xp))) continue;
     const V3 x = xyz(xp) + xyz(V.ns4[i]);
