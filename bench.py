@@ -53,61 +53,135 @@ SEED = 2002
 
 
 # ----------------------------------------------------------------- workloads
-def workload(name, cs, dx_override=None):
-    """(label, SolverConfig, fluid, particle dict, domain lo, hi)."""
+# Each workload is plain data: the C ABI's config fields, a fluid preset with
+# overrides, the tank as a geometry node list (kind, a, b, p) whose last node
+# is the root (kinds as CRYO_GEOM_*: a/b index child nodes), the fill, a
+# particle filter and the domain.  Both arms build from it: this library's arm
+# through its CryoSPH module, the reference arm through the reference's own
+# lattice generator in oracle/_ref and nothing of this package.  The fluid
+# lattice is then jittered +-0.05 dx by numpy PCG64(SEED) (walls stay on it).
+G_CYLINDER, G_CAPSULE, G_SPHERE, G_BOX, G_TRANSLATED, G_DIFFERENCE, G_UNION = range(7)
+FLUID_LH2, FLUID_LN2, FLUID_H2O = 1, 2, 5
+FILL_FULL = 2
+
+
+def workload_spec(name, dx=None):
     if name == "dam_break":
-        dx = dx_override or 0.02
-        water = cs.FluidProperties.water()
-        water.mu_liquid = 1.0e-3
-        cfg = cs.SolverConfig()
-        cfg.dx = dx
-        cfg.gravity = (0.0, 0.0, -9.81)
-        cfg.surface_tension = cs.SurfaceTensionModel.NoTension
-        cfg.thermal = False
-        cfg.phase_change = False
-        cfg.density_mode = cs.DensityMode.Continuity
-        cfg.velocity_scale = (2 * 9.81 * 0.55) ** 0.5
-        cfg.artificial_viscosity = 0.02
-        cfg.delta_sph = 0.1
-        cfg.no_slip = False
+        # SPHERIC Test 2 (validation/spheric_test2/run.py:36-73 of the reference)
+        dx = dx or 0.02
         x_front, box = 0.744, (0.161, 0.403, 0.161)
-        tank = cs.Translated(cs.BoxTank(3.22, 1.0, 1.0), (1.61, 0.0, 0.5))
-        obst = cs.Translated(cs.BoxTank(*box), (x_front - box[0] / 2, 0.0, box[2] / 2))
-        fill = cs.FillSpec()
-        fill.mode = cs.FillMode.Full
-        p = cs.tank_particles(cs.Difference(tank, obst), water, dx, fill)
-        x, ph = p["position"], p["phase"]
-        keep = (ph == 2) | ((x[:, 0] > 3.22 - 1.228) & (x[:, 2] < 0.55))
-        p = {k: v[keep] for k, v in p.items()}
         pad = 4 * dx
-        lo, hi = (-pad, -0.5 - pad, -pad), (3.22 + pad, 0.5 + pad, 1.0 + pad)
-        label, fluid = f"dam_break_spheric2_dx{dx:g}", water
-    elif name in ("c1", "c3"):
-        if name == "c1":
-            fluid = cs.FluidProperties.liquid_nitrogen()
-            dx, geo, g = dx_override or 0.004, cs.CylinderTank(0.05, 0.12), (0.0, 0.0, -9.81e-4)
-            label = f"c1_ln2_cylinder_dx{dx:g}"
-        else:
-            fluid = cs.FluidProperties.liquid_hydrogen()
-            dx, geo, g = dx_override or 0.0052, cs.SphereTank(0.5), (0.0, 0.0, -9.81e-4)
-            label = f"c3_lh2_sphere_dx{dx:g}"
-        cfg = cs.SolverConfig()
-        cfg.dx = dx
-        cfg.gravity = g
-        cfg.heater_power = 20.0 if name == "c1" else 0.0
-        cfg.thermo_mode = cs.TankThermoMode.Closed
-        fill = cs.FillSpec()
-        fill.fill_fraction = 0.5
-        p = cs.tank_particles(geo, fluid, dx, fill)
-        lo, hi = cs.tank_domain(geo, dx, 3)
-    else:
-        raise SystemExit(f"unknown workload {name}")
+        return dict(
+            label=f"dam_break_spheric2_dx{dx:g}", fluid=(FLUID_H2O, {"mu_liquid": 1.0e-3}),
+            config=dict(dx=dx, gravity=(0.0, 0.0, -9.81), surface_tension=0, thermal=0, phase_change=0,
+                        density_mode=1, velocity_scale=(2 * 9.81 * 0.55) ** 0.5, artificial_viscosity=0.02,
+                        delta_sph=0.1, no_slip=0),
+            nodes=[(G_BOX, 0, 0, (3.22, 1.0, 1.0)), (G_TRANSLATED, 0, 0, (1.61, 0.0, 0.5)),
+                   (G_BOX, 0, 0, box), (G_TRANSLATED, 2, 0, (x_front - box[0] / 2, 0.0, box[2] / 2)),
+                   (G_DIFFERENCE, 1, 3, (0.0, 0.0, 0.0))],
+            fill=dict(mode=FILL_FULL), keep=_dam_break_column,
+            domain=((-pad, -0.5 - pad, -pad), (3.22 + pad, 0.5 + pad, 1.0 + pad)))
+    if name == "c1":
+        dx = dx or 0.004
+        return dict(label=f"c1_ln2_cylinder_dx{dx:g}", fluid=(FLUID_LN2, {}),
+                    config=dict(dx=dx, gravity=(0.0, 0.0, -9.81e-4), heater_power=20.0, thermo_mode=1),
+                    nodes=[(G_CYLINDER, 0, 0, (0.05, 0.12, 0.0))], fill=dict(fill_fraction=0.5), keep=None,
+                    domain=None)
+    if name == "c3":
+        dx = dx or 0.0052
+        return dict(label=f"c3_lh2_sphere_dx{dx:g}", fluid=(FLUID_LH2, {}),
+                    config=dict(dx=dx, gravity=(0.0, 0.0, -9.81e-4), heater_power=0.0, thermo_mode=1),
+                    nodes=[(G_SPHERE, 0, 0, (0.5, 0.0, 0.0))], fill=dict(fill_fraction=0.5), keep=None,
+                    domain=None)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def _dam_break_column(x, phase):
+    """Walls, and the water column 1.228 m long and 0.55 m high at the far end."""
+    return (phase == 2) | ((x[:, 0] > 3.22 - 1.228) & (x[:, 2] < 0.55))
+
+
+def _jitter(x, phase, dx):
     rng = np.random.Generator(np.random.PCG64(SEED))
-    fl = p["phase"] != 2
-    x = p["position"].astype(np.float32).copy()
+    fl = phase != 2
+    x = np.asarray(x, np.float32).copy()
     x[fl] += rng.uniform(-0.05 * dx, 0.05 * dx, size=(int(fl.sum()), 3)).astype(np.float32)
-    p["position"] = x
-    return label, cfg, fluid, p, lo, hi
+    return x
+
+
+def _cs_geometry(cs, nodes):
+    objs = []
+    for kind, a, b, p in nodes:
+        if kind == G_CYLINDER:
+            objs.append(cs.CylinderTank(p[0], p[1]))
+        elif kind == G_CAPSULE:
+            objs.append(cs.CapsuleTank(p[0], p[1]))
+        elif kind == G_SPHERE:
+            objs.append(cs.SphereTank(p[0]))
+        elif kind == G_BOX:
+            objs.append(cs.BoxTank(*p))
+        elif kind == G_TRANSLATED:
+            objs.append(cs.Translated(objs[a], tuple(p)))
+        elif kind == G_DIFFERENCE:
+            objs.append(cs.Difference(objs[a], objs[b]))
+        else:
+            objs.append(cs.Union(objs[a], objs[b]))
+    return objs[-1]
+
+
+def workload(name, cs, dx_override=None):
+    """This library's arm: (label, SolverConfig, fluid, particle dict, domain lo, hi)."""
+    w = workload_spec(name, dx_override)
+    which, over = w["fluid"]
+    fluid = {FLUID_LH2: cs.FluidProperties.liquid_hydrogen, FLUID_LN2: cs.FluidProperties.liquid_nitrogen,
+             FLUID_H2O: cs.FluidProperties.water}[which]()
+    for k, v in over.items():
+        setattr(fluid, k, v)
+    cfg = cs.SolverConfig()
+    for k, v in w["config"].items():
+        cur = getattr(cfg, k)
+        setattr(cfg, k, tuple(v) if k == "gravity" else (type(cur)(int(v)) if hasattr(cur, "value") else
+                                                          (bool(v) if isinstance(cur, bool) else v)))
+    geo = _cs_geometry(cs, w["nodes"])
+    fill = cs.FillSpec()
+    for k, v in w["fill"].items():
+        setattr(fill, k, [cs.FillMode.Settled, cs.FillMode.CentralBubble, cs.FillMode.Full][v] if k == "mode" else v)
+    dx = w["config"]["dx"]
+    p = cs.tank_particles(geo, fluid, dx, fill)
+    if w["keep"] is not None:
+        keep = w["keep"](p["position"], p["phase"])
+        p = {k: v[keep] for k, v in p.items()}
+    lo, hi = w["domain"] if w["domain"] else cs.tank_domain(geo, dx, 3)
+    p["position"] = _jitter(p["position"], p["phase"], dx)
+    return w["label"], cfg, fluid, p, lo, hi
+
+
+def ref_workload(name, dx_override=None):
+    """The reference arm's inputs from the same spec, through the reference's
+    own generator (build_tank_particles, geometry.cpp:242-330, in oracle/_ref):
+    (label, refpy config, refpy fluid, particle arrays, lo, hi)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_abi
+    import refpy
+    w = workload_spec(name, dx_override)
+    which, over = w["fluid"]
+    fluid = ref_abi.fluid(which, **over)
+    cfg = ref_abi.config(**w["config"])
+    dx = w["config"]["dx"]
+    fkw = dict(w["fill"])
+    parts = refpy.tank_particles(w["nodes"], fluid, dx, refpy.make_fill(**fkw))
+    if w["keep"] is not None:
+        keep = w["keep"](parts["x"], parts["phase"])
+        parts = {k: v[keep] for k, v in parts.items()}
+    lo, hi = w["domain"] if w["domain"] else refpy.tank_domain(w["nodes"], dx, 3)
+    parts["x"] = _jitter(parts["x"], parts["phase"], dx)
+    return w["label"], cfg, fluid, parts, lo, hi
+
+
+def config_block(label, n_total, n_fluid, n_wall, world):
+    """The `config` of the JSON line; both arms print the same dict."""
+    return {"workload": label, "particles": n_total, "fluid": n_fluid, "walls": n_wall,
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU", "seed": SEED}
 
 
 def c4_tanks(cs, count=64, n_lo=5_000, n_hi=200_000, seed=SEED):
@@ -166,31 +240,6 @@ def load(solver, p, lo, hi):
                          domain_hi=hi, normal=p["normal"], flags=p["flags"])
 
 
-def c_config(cs_cfg):
-    """SolverConfig (module object) -> cryo_config_t fields (for the reference arm)."""
-    import cryo_cabi as cabi
-    kw = {}
-    for name, _ in cabi.CONFIG_FIELDS:
-        v = getattr(cs_cfg, name)
-        if name == "gravity":
-            kw[name] = tuple(v)
-        elif hasattr(v, "value"):
-            kw[name] = int(v.value)
-        elif isinstance(v, bool):
-            kw[name] = int(v)
-        else:
-            kw[name] = v
-    return cabi.py_config(**kw)
-
-
-def c_fluid(f):
-    import cryo_cabi as cabi
-    out = cabi.Fluid()
-    for k, _ in cabi.Fluid._fields_:
-        setattr(out, k, getattr(f, k))
-    return out
-
-
 # ---------------------------------------------------------------- clocks
 class Clocks:
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -245,22 +294,22 @@ class Clocks:
 
 
 # ------------------------------------------------------------- reference arm
-def reference_rate(cs_cfg, fluid, p, lo, hi, steps, warmup, budget_s=60.0, cuda=False):
+def reference_rate(name, dx, steps, warmup, budget_s=60.0, cuda=False, inputs=None):
     """The reference's own implementation (oracle/_ref, built from its own
-    sources) on the same workload: its CPU/OpenMP backend with all host
-    threads, or (cuda=True) its CUDA backend built for sm_100a, wall clock as
-    its perf_scaling.cpp times it; returns (rate, threads, steps timed,
-    seconds)."""
+    sources) on the workload built by ref_workload(): its CPU/OpenMP backend
+    with every host thread, or (cuda=True) its CUDA backend built for
+    sm_100a, wall clock as its perf_scaling.cpp times it.  At most `steps`
+    steps, fewer when one step times `budget_s` would be exceeded.  Returns
+    (rate, threads, steps timed, seconds, label, particle counts) or None."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import refpy
     if not refpy.ref_available(cuda=cuda):
         return None
-    ref = refpy.Ref(c_config(cs_cfg), c_fluid(fluid), cuda=cuda)
+    label, cfg, fluid, parts, lo, hi = inputs or ref_workload(name, dx)
+    ref = refpy.Ref(cfg, fluid, cuda=cuda)
     threads = os.cpu_count() or 1
     ref.set_threads(threads)
-    arrays = {"x": p["position"], "m": p["mass"], "rho": p["density"], "T": p["temperature"], "phase": p["phase"],
-              "nrm": p["normal"], "flags": p["flags"]}
-    ref.set_particles(arrays, lo, hi)
+    ref.set_particles(parts, lo, hi)
     ref.step(max(1, min(warmup, 2)))
     t0 = time.perf_counter()
     ref.step(1)
@@ -270,7 +319,37 @@ def reference_rate(cs_cfg, fluid, p, lo, hi, steps, warmup, budget_s=60.0, cuda=
     ref.step(k)
     el = time.perf_counter() - t0
     n = ref.num_particles()
-    return n * k / el, threads, k, el
+    n_wall = int((parts["phase"] == 2).sum())
+    return n * k / el, threads, k, el, label, (len(parts["x"]), len(parts["x"]) - n_wall, n_wall)
+
+
+def reference_main(args, world):
+    """--impl reference: the reference's CPU implementation of the path on this
+    host's cores, on the same workload and config as this library's arm.
+    Nothing of this package is imported or loaded in this process."""
+    if args.workload == "c4":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no batched ensemble (one Solver "
+                                                              "per tank); its back-to-back solves are this "
+                                                              "library's own back_to_back leg"}))
+        return 0
+    r = reference_rate(args.workload, args.dx, args.steps, args.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
+        return 0
+    rate, threads, k, el, label, (n_total, n_fluid, n_wall) = r
+    line = {
+        "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
+        "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 fields, f64 reductions", "data": "synthetic",
+        "config": config_block(label, n_total, n_fluid, n_wall, world),
+        "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{k} steps of {label} after 2 warm-up steps (its OpenMP backend, "
+                                   f"{threads} threads)"},
+        "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "timing": "wall clock around the steps; inputs from the reference's own lattice generator",
+    }
+    print(json.dumps(line))
+    return 0
 
 
 # ------------------------------------------------------------------- main
@@ -308,6 +387,10 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
+    if args.impl == "reference":
+        # rank 0 alone times the reference; nothing of this package is loaded
+        return reference_main(args, world) if rank == 0 else 0
+
     import CryoSPH as cs
 
     if args.only_adjoint:
@@ -322,26 +405,6 @@ def main():
     n_wall = int((p["phase"] == 2).sum())
     n_fluid = n_total - n_wall
     has_vapor = bool((p["phase"] == 1).any())
-
-    if args.impl == "reference":
-        if rank != 0:
-            return 0
-        r = reference_rate(cfg, fluid, p, lo, hi, args.steps, args.warmup)
-        if r is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference CPU build (oracle/_ref) not present"}))
-            return 0
-        rate, threads, k, el = r
-        line = {
-            "impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus, "steps": k,
-            "warmup": args.warmup, "ms_per_step": el / k * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": label, "particles": n_total, "fluid": n_fluid, "walls": n_wall},
-            "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
-                             "sample": f"{k} steps of the workload after 2 warm-up steps (OpenMP, {threads} threads)"},
-            "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }
-        print(json.dumps(line))
-        return 0
 
     import torch
     import cryo_cabi as cabi
@@ -423,17 +486,17 @@ def main():
 
     ref_gpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
-        r = reference_rate(cfg, fluid, p, lo, hi, 2000, 3, budget_s=10.0, cuda=True)
+        r = reference_rate(args.workload, args.dx, 2000, 3, budget_s=10.0, cuda=True)
         if r is not None:
-            rate, _, k, el = r
+            rate, _, k, el = r[:4]
             ref_gpu = {"value": rate, "unit": UNIT, "kind": "reference CUDA backend (its own sources, sm_100a)",
                        "sample": f"{k} steps of {label} after 3 warm-up steps ({el:.1f} s wall clock)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and not args.only_timed:
-        r = reference_rate(cfg, fluid, p, lo, hi, 200, 2, budget_s=20.0)
+        r = reference_rate(args.workload, args.dx, 200, 2, budget_s=20.0)
         if r is not None:
-            rate, threads, k, el = r
+            rate, threads, k, el = r[:4]
             cpu = {"value": rate, "unit": UNIT, "cores": threads, "kind": "reference",
                    "sample": f"{k} steps of {label} after 2 warm-up steps ({el:.1f} s, OpenMP)"}
 
@@ -454,10 +517,10 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32 fields, f64 reductions", "data": "synthetic",
-            "config": {"workload": label, "particles": n_total, "fluid": n_fluid, "walls": n_wall,
-                       "particles_after": int(n_now), "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "flushed between timed steps (256 MiB memset outside the events)",
-                       "execution": "CUDA graph per step", "seed": SEED},
+            "config": config_block(label, n_total, n_fluid, n_wall, world),
+            "particles_after": int(n_now),
+            "timing": {"l2": "flushed between timed steps (256 MiB memset outside the events)",
+                       "execution": "CUDA graph per step"},
             "per_gpu": value / world,
             "gpu_launches": per_step * args.steps,
             "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},

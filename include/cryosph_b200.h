@@ -309,10 +309,12 @@ int cryo_probe_pressure(cryo_ctx* ctx, const float* points, int np, float* out);
    where a pool allocation can fail or stall once the particle arena has
    filled the device). Points and results go through one fixed device array
    per device of CRYO_PROBE_STATIC_MAX points; more points return CRYO_ERANGE.
-   The first call on a device sets that array up and should come before any
-   stream capture. Calls whose GPU work overlapped would race on the shared
+   The context must be initialised first (one step, or one cryo_probe_pressure
+   call): an uninitialised context returns CRYO_EINVAL, since initialising it
+   may allocate. Calls whose GPU work overlapped would race on the shared
    array, so calls are serialised by a process-wide lock and return only once
-   their stream has finished. Same results as cryo_probe_pressure. */
+   their stream has finished, on error too. Same results as
+   cryo_probe_pressure. */
 #define CRYO_PROBE_STATIC_MAX 16384
 int cryo_probe_pressure_noalloc(cryo_ctx* ctx, const float* points, int np, float* out);
 

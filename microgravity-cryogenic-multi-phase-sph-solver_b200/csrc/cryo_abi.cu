@@ -2050,18 +2050,27 @@ int cryo_probe_pressure(cryo_ctx* c, const float* pts, int np, float* out) {
 // callers that must not allocate device memory once running: a monitoring or
 // control loop that probes tank pressure every cycle under a fixed memory
 // budget, where a pool allocation can fail or stall once the particle arena
-// has filled the device. The array is set up on the first call on each device
-// (cudaGetSymbolAddress with that device current), so that first call should
-// come before any stream capture. It is shared by every context on the
-// device: calls whose GPU work overlapped would race on it, so calls hold a
-// process-wide lock and wait for their stream before returning. Nothing in
-// the array has to start at zero: each call writes the points it reads and a
-// result for every point before copying the results back.
+// has filled the device. The context must already be initialised (stepped
+// once, or probed once through cryo_probe_pressure): initialisation sizes the
+// cell tables, which may allocate, so an uninitialised context is refused
+// with CRYO_EINVAL instead. The array's device address is looked up on every
+// call (cudaGetSymbolAddress with the context's device current; it allocates
+// nothing), so no address outlives a device reset. The array is shared by
+// every context on the device: calls whose GPU work overlapped would race on
+// it, so calls hold a process-wide lock, and the lock is released only after
+// the call's stream has drained, on the error paths too. Nothing in the array
+// has to start at zero: each call writes the points it reads and a result for
+// every point before copying the results back.
 namespace {
-constexpr int kProbeStaticMaxDevices = 64;
 __device__ __align__(256) float g_probe_scratch[4 * CRYO_PROBE_STATIC_MAX];  // xyz per point, then results
 std::mutex g_probe_scratch_mu;
-float* g_probe_scratch_ptr[kProbeStaticMaxDevices] = {};
+// Waits for the stream when it goes out of scope (declared after the lock, so
+// it runs first): a failed copy or launch cannot leave work that still uses
+// the shared array behind a released lock.
+struct DrainOnExit {
+  cudaStream_t s;
+  ~DrainOnExit() { cudaStreamSynchronize(s); }
+};
 }  // namespace
 
 int cryo_probe_pressure_noalloc(cryo_ctx* c, const float* pts, int np, float* out) {
@@ -2070,11 +2079,15 @@ int cryo_probe_pressure_noalloc(cryo_ctx* c, const float* pts, int np, float* ou
       throw std::out_of_range("cryo_probe_pressure_noalloc: " + std::to_string(np) +
                               " points exceed the fixed scratch of " + std::to_string(CRYO_PROBE_STATIC_MAX) +
                               " points; split the call or use cryo_probe_pressure");
-    if (c->device < 0 || c->device >= kProbeStaticMaxDevices)
-      throw std::out_of_range("cryo_probe_pressure_noalloc: device ordinal out of range");
+    if (!c->initialized)
+      throw std::invalid_argument(
+          "cryo_probe_pressure_noalloc: the context is not initialised (its first step or an allocating "
+          "probe sizes the cell tables); step once or call cryo_probe_pressure first");
+    if (np <= 0) return;
     std::lock_guard<std::mutex> lock(g_probe_scratch_mu);
-    float* d = g_probe_scratch_ptr[c->device];
-    if (!d) {
+    DrainOnExit drain{c->stream};
+    float* d = nullptr;
+    {
       int prev = 0;
       CK(cudaGetDevice(&prev));
       CK(cudaSetDevice(c->device));
@@ -2082,10 +2095,8 @@ int cryo_probe_pressure_noalloc(cryo_ctx* c, const float* pts, int np, float* ou
       const cudaError_t e = cudaGetSymbolAddress(&p, g_probe_scratch);
       CK(cudaSetDevice(prev));
       CK(e);
-      d = g_probe_scratch_ptr[c->device] = static_cast<float*>(p);
+      d = static_cast<float*>(p);
     }
-    c->ensure_initialized();
-    if (np <= 0) return;
     CK(cudaMemcpyAsync(d, pts, (size_t)np * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     const int blocks = std::max(1, std::min((np + 127) / 128, c->sm_count * 8));
     k_probe<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);

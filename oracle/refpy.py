@@ -16,12 +16,10 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REPO = os.path.dirname(HERE)
-PKG = os.path.join(REPO, "microgravity-cryogenic-multi-phase-sph-solver_b200")
-if PKG not in sys.path:
-    sys.path.insert(0, PKG)
+if HERE not in sys.path:
+    sys.path.insert(0, HERE)
 
-import cryo_cabi as cabi  # noqa: E402  (struct layouts of include/cryosph_b200.h)
+import ref_abi as cabi  # noqa: E402  (struct layouts of include/cryosph_b200.h; nothing from the package)
 
 REF_LIB = os.path.join(HERE, "_ref", "libcryoref.so")
 REF_LIB64 = os.path.join(HERE, "_ref", "libcryoref64.so")
@@ -41,13 +39,6 @@ class Fill(C.Structure):
                 ("bubble_center", C.c_float * 3), ("include_vapor", C.c_int), ("wall_layers", C.c_int),
                 ("T_liquid", C.c_float), ("T_vapor", C.c_float), ("T_wall", C.c_float),
                 ("heater_zmin", C.c_double), ("heater_zmax", C.c_double)]
-
-
-class HostOut(C.Structure):
-    _fields_ = [("n", C.c_int), ("x", C.POINTER(C.c_float)), ("v", C.POINTER(C.c_float)),
-                ("nrm", C.POINTER(C.c_float)), ("m", C.POINTER(C.c_float)), ("rho", C.POINTER(C.c_float)),
-                ("T", C.POINTER(C.c_float)), ("phase", C.POINTER(C.c_uint8)), ("flags", C.POINTER(C.c_uint8)),
-                ("id", C.POINTER(C.c_uint32))]
 
 
 def make_fill(mode=0, fill_fraction=0.5, settle=(0, 0, -1), bubble=(0, 0, 0), include_vapor=True, wall_layers=3,
@@ -113,8 +104,8 @@ def _declare(L, has_tank):
         sig.update({
             "build_tank": (i, [vp, C.POINTER(GeomNode), i, C.POINTER(Fill)]),
             "tank_particles": (i, [C.POINTER(GeomNode), i, C.POINTER(cabi.Fluid), f, C.POINTER(Fill),
-                                   C.POINTER(HostOut)]),
-            "free_particles": (None, [C.POINTER(HostOut)]),
+                                   C.POINTER(cabi.HostOut)]),
+            "free_particles": (None, [C.POINTER(cabi.HostOut)]),
             "tank_domain": (i, [C.POINTER(GeomNode), i, f, i, fp, fp]),
             "geom_sdf": (d, [C.POINTER(GeomNode), i, d, d, d]),
             "neighbor_stats": (i, [vp, f, vp, vp]),
@@ -132,6 +123,7 @@ class _Checker:
             fn = getattr(self.L, self.prefix + name)
             fn.restype, fn.argtypes = res, args
         err = C.create_string_buffer(512)
+        cfg, fluid = cabi.as_struct(cabi.Config, cfg), cabi.as_struct(cabi.Fluid, fluid)
         self.h = self._f("create")(C.byref(cfg), C.byref(fluid), err, 512)
         if not self.h:
             raise ValueError(err.value.decode())
@@ -153,7 +145,7 @@ class _Checker:
 
     def check(self, rc):
         if rc:
-            raise cabi.CryoError(rc, self._f("last_error")(self.h).decode())
+            raise cabi.RefError(rc, self._f("last_error")(self.h).decode())
 
     def set_threads(self, n):
         self._f("set_threads")(int(n))
@@ -304,10 +296,11 @@ def tank_particles(nodes, fluid, dx, fill):
     """The reference's lattice generator (geometry.cpp:242-330) as numpy arrays."""
     L = _ref_lib_for_tools()
     g = geom(nodes)
-    out = HostOut()
+    out = cabi.HostOut()
+    fluid = cabi.as_struct(cabi.Fluid, fluid)
     rc = L.ref_tank_particles(g, len(nodes), C.byref(fluid), float(dx), C.byref(fill), C.byref(out))
     if rc:
-        raise cabi.CryoError(rc, "tank_particles failed")
+        raise cabi.RefError(rc, "tank_particles failed")
     n = out.n
     res = {
         "x": np.ctypeslib.as_array(out.x, (n, 3)).copy(),
@@ -330,7 +323,7 @@ def tank_domain(nodes, dx, wall_layers=3):
     lo, hi = (C.c_float * 3)(), (C.c_float * 3)()
     rc = L.ref_tank_domain(g, len(nodes), float(dx), wall_layers, lo, hi)
     if rc:
-        raise cabi.CryoError(rc, "tank_domain failed")
+        raise cabi.RefError(rc, "tank_domain failed")
     return tuple(lo), tuple(hi)
 
 
