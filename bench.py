@@ -455,7 +455,7 @@ def main():
     e2e = roof = None
     if rank == 0 and not args.only_timed:
         # ---- e2e through the public API with host buffers
-        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, args.steps, device, stream, flush)
+        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, args.steps, device, stream, flush, args.warmup)
         # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
         roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
 
@@ -589,34 +589,55 @@ def ctypes_int(L, fn, handle):
     return v.value
 
 
-def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
-    """Public-API run with host buffers: state upload, then per step the
+def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3):
+    """Public-API run with host buffers: the state upload, then per step the
     frame-motion input (host->device) and the diagnostics (device->host), then
-    the state download.  Device-timed per step with L2 flushed between steps."""
+    the state download.  Device-timed per step with L2 flushed between steps.
+    The same sequence runs once untimed first (`warmup` steps): the solver's
+    device storage and step graphs are then in place, and the timed upload of
+    the same-sized state reuses them, as a loop of runs on one Solver does."""
     import torch
     solver = cs.Solver(cfg, fluid, device)
     x = np.ascontiguousarray(p["position"], np.float64)
     arrays = [x, p["mass"].astype(np.float64), p["density"].astype(np.float64), p["temperature"].astype(np.float64)]
     state_in = sum(a.nbytes for a in arrays) + p["phase"].nbytes + p["normal"].nbytes + p["flags"].nbytes
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
     st = torch.cuda.ExternalStream(solver.stream_handle, device=device)
-    torch.cuda.synchronize()
-    state_out = 0
-    with torch.cuda.stream(st):
-        for k in range(steps):
-            flush.zero_()
-            ev[k][0].record(st)
+
+    def run(k_steps, ev=None, host=None):
+        out = 0
+        for k in range(k_steps):
+            if ev is not None:
+                flush.zero_()
+                ev[k][0].record(st)
+            t0 = time.perf_counter()
             if k == 0:
                 load(solver, p, lo, hi)
+            t1 = time.perf_counter()
             a = 0.01 * math.sin(0.01 * k)
             solver.set_frame_motion(acceleration=(a, 0.0, 0.0))
             solver.step()
             d = solver.diagnostics()
             _ = d.slosh_force
-            if k == steps - 1:
+            t2 = time.perf_counter()
+            if k == k_steps - 1:
                 parts = solver.particles()
-                state_out = sum(v.nbytes for v in parts.values())
-            ev[k][1].record(st)
+                out = sum(v.nbytes for v in parts.values())
+            t3 = time.perf_counter()
+            if ev is not None:
+                ev[k][1].record(st)
+            if host is not None:
+                host["upload_ms"] += (t1 - t0) * 1e3
+                host["steps_ms"] += (t2 - t1) * 1e3
+                host["download_ms"] += (t3 - t2) * 1e3
+        return out
+
+    with torch.cuda.stream(st):
+        run(max(warmup, 1))
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    host = {"upload_ms": 0.0, "steps_ms": 0.0, "download_ms": 0.0}
+    with torch.cuda.stream(st):
+        state_out = run(steps, ev, host)
     torch.cuda.synchronize()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     n = solver.num_particles
@@ -624,7 +645,9 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush):
     diag = 8 * 25 + 8 * 64   # diagnostics reduction + scalar block
     return {"value": n * steps / (ms / 1e3), "unit": UNIT,
             "h2d_bytes_per_step": int(state_in / steps + ctl), "d2h_bytes_per_step": int(diag + state_out / steps),
-            "steps": steps, "timing": "CUDA events per step (host work inside), L2 flushed between steps"}
+            "steps": steps, "host_wall_ms": {k: round(v, 3) for k, v in host.items()},
+            "timing": "CUDA events per step (host work inside), L2 flushed between steps; one untimed run of the "
+                      "same sequence first"}
 
 
 def c5_solver(cs, device, dx=0.0034):

@@ -450,6 +450,17 @@ class Context:
         self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), _ptr(lst), total.value, C.byref(total)))
         return counts, lst[: total.value]
 
+    def probe_pressure(self, pts):
+        """Solver::probe_pressure: Shepard liquid pressure at each point (NaN where dry)."""
+        pts = np.ascontiguousarray(pts, np.float32).reshape(-1, 3)
+        out = np.empty(len(pts), np.float32)
+        self.check(self.L.cryo_probe_pressure(self.h, pts.ctypes.data_as(C.POINTER(C.c_float)), len(pts),
+                                              out.ctypes.data_as(C.POINTER(C.c_float))))
+        return out
+
+    def set_frame_motion(self, a=(0, 0, 0), w=(0, 0, 0), wd=(0, 0, 0), o=(0, 0, 0)):
+        self.check(self.L.cryo_set_frame_motion(self.h, vec3(a), vec3(w), vec3(wd), vec3(o)))
+
     # ---------------------------------------------- differentiated window
     ADJ_STATE = {"x": 0, "v": 1, "T": 2, "m": 3, "a": 4, "ab": 5}
 

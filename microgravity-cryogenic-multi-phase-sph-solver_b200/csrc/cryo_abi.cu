@@ -1,475 +1,13 @@
-// cryo_abi.cu -- host side of the B200 hot path: the context (device memory,
-// stream, CUDA graphs), the parameter lowering (Solver::init_params), the
-// step orchestration and every extern "C" entry point of cryosph_b200.h.
-//
-// Nothing here throws across the ABI: each entry point runs inside guard(),
-// which maps exceptions to status codes the way the reference's exceptions
-// map to Python (invalid_argument -> CRYO_EINVAL, out_of_range -> CRYO_ERANGE,
-// runtime_error -> CRYO_ERUNTIME, CUDA failures -> CRYO_ECUDA).
-#include <algorithm>
-#include <cmath>
-#include <condition_variable>
-#include <cstdio>
-#include <cstring>
-#include <limits>
-#include <mutex>
-#include <stdexcept>
-#include <string>
-#include <thread>
-#include <vector>
+// cryo_abi.cu -- the solver's entry points: the context's parameter lowering
+// (Solver::init_params), the step orchestration, loading, fields, probes,
+// passes, checkpoints, telemetry and profiling (the extern "C" functions of
+// cryosph_b200.h not in cryo_ensemble.cu, cryo_adj_abi.cu or
+// cryo_slab_abi.cu).
+#include "cryo_ctx.cuh"
 
-#include "cryo_adjoint.cuh"
-
-using namespace cryo;
-
-namespace {
-
-struct CudaError : std::runtime_error {
-  explicit CudaError(const std::string& m) : std::runtime_error(m) {}
-};
-
-#define CK(expr)                                                                                 \
-  do {                                                                                           \
-    const cudaError_t e__ = (expr);                                                              \
-    if (e__ != cudaSuccess)                                                                      \
-      throw CudaError(std::string("CUDA error '") + cudaGetErrorString(e__) + "' at " #expr);   \
-  } while (0)
-
-#define LAUNCH_CHECK() CK(cudaGetLastError())
-
-// Kernel launch inside a cryo_ctx member: counted, and bracketed by events
-// when profiling is on.
-#define LAUNCH(K, G, B, ...)                     \
-  do {                                           \
-    this->before_launch(#K);                     \
-    K<<<(G), (B), 0, this->stream>>>(__VA_ARGS__); \
-    LAUNCH_CHECK();                              \
-    this->after_launch();                        \
-  } while (0)
-
-struct Persist {
-  float4 *xp = nullptr, *vT = nullptr, *vt = nullptr, *nrm = nullptr, *mrps = nullptr;
-  uint32_t* id = nullptr;
-};
-
-// One device allocation carved into 256-byte aligned arrays.
-struct Arena {
-  char* base = nullptr;
-  size_t size = 0, used = 0;
-  void release() {
-    if (base) cudaFree(base);
-    base = nullptr;
-    size = used = 0;
-  }
-  template <class T>
-  T* take(size_t n) {
-    const size_t bytes = (n * sizeof(T) + 255) & ~size_t(255);
-    T* p = reinterpret_cast<T*>(base + used);
-    used += bytes;
-    return p;
-  }
-};
-
-size_t particle_bytes(size_t cap) {
-  const size_t a = 256;
-  auto r = [&](size_t b) { return (b + a - 1) / a * a; };
-  size_t t = 0;
-  for (int s = 0; s < 2; ++s) t += 5 * r(cap * 16) + r(cap * 4);    // persistent sets
-  t += 8 * r(cap * 16) + 4 * r(cap * 4);                            // scratch
-  t += 5 * r(cap * 4);                                              // sort keys/vals, split flags
-  const size_t tiles = (cap + RS_TILE - 1) / RS_TILE + 1;
-  t += r((tiles + 1) * RS_BINS * 4);                                // radix histogram + digit totals
-  const size_t chunks = cap / kChunk + 2;
-  t += r(chunks * 32 * 8);                                          // reduction partials
-  t += r(64 * 8) + r(64);                                           // diagnostics out, tickets
-  t += r(cap * 4 * (size_t)kMaxNbr) + 3 * r(cap * 4);              // neighbour lists, counts, phase lists
-  return t;
-}
-
-}  // namespace
-
-void ensemble_detach(cryo_ensemble* e, cryo_ctx* c);
-struct AdjWindow;
-struct SlabGroup;
-// Where a slab of a decomposed tank meets its neighbours inside a step:
-// after a sort (its owned range), after a pass a later neighbour pass reads
-// (the ghost layers), after the heat weights (also the heat normalisation),
-// after the force pass (also the dt maxima), after the split marks (the
-// split ids) and at the end (ullage and maxima).
-enum SlabPoint { SLAB_SORTED, SLAB_HALO, SLAB_HEAT, SLAB_FORCES, SLAB_SPLIT, SLAB_END };
-void adj_free(AdjWindow* w);
-
-// Where a step recomputed for the reverse sweep leaves the values its later
-// stages overwrite (cryo_adjoint.cuh, Adj).
-struct StepTape {
-  float4 *vT1, *ns1, *pc2, *vT2;
-  float *m1, *m2;
-  DynState* dyn1;
-  float4* sums;  // View::tape for the taped force / interface variants
-  int n;
-};
-
-// A context that holds the whole tank owns every particle.
-static void set_whole_tank(DynState& d) {
-  d.own_lo = 0;
-  d.own_hi = std::numeric_limits<int>::max();
-  d.n_sorted = std::numeric_limits<int>::max();
-  d.id_offset = 0;
-  d.split_total = 0;
-}
-
-struct cryo_ctx {
-  cryo_config_t cfg{};
-  cryo_fluid_t fluid{};
-  Params P{};
-  int device = 0;
-  int sm_count = 148;
-  cudaStream_t stream = nullptr;
-  std::string err;
-
-  // particle storage
-  int capacity = 0;
-  Arena arena;
-  Persist set[2];
-  int cur = 0;
-  float4 *a4 = nullptr, *ab4 = nullptr, *fw = nullptr, *mw = nullptr, *vwp = nullptr, *ns4 = nullptr,
-         *pc = nullptr, *aux = nullptr;
-  float *rmin = nullptr, *wall_w = nullptr, *heat_w = nullptr, *nu_t = nullptr;
-  uint32_t *keys_a = nullptr, *keys_b = nullptr, *vals_a = nullptr, *vals_b = nullptr, *split_flag = nullptr;
-  uint32_t* hist = nullptr;
-  int *nbr = nullptr, *nbr_cnt = nullptr, *fluid_idx = nullptr, *wall_idx = nullptr;
-  double* partials = nullptr;
-  int max_chunks = 0;
-  double* diag_out = nullptr;
-  unsigned* ticket = nullptr;
-  const uint32_t* sorted_keys = nullptr;  // of the last grid build
-  const uint32_t* sorted_perm = nullptr;
-  int last_sort_n = 0;
-
-  // grid
-  int* cell_begin = nullptr;
-  uint8_t* cell_fluid = nullptr;  // 1: a fluid particle was sorted into the cell
-  int cell_cap = 0;
-
-  // scalar block
-  DynState* dyn = nullptr;   // device
-  DynState* hdyn = nullptr;  // pinned host mirror
-  double* diag_host = nullptr;  // pinned, 64 doubles
-  // Host-owned frame state (authoritative unless a manoeuvre table drives the
-  // frame on the device); updates go out through a ring of pinned slots.
-  DynState::Frame hframe{};
-  bool man_active = false;
-  static constexpr int kFrameSlots = 16;
-  DynState::Frame* frame_ring = nullptr;
-  cudaEvent_t frame_ev[kFrameSlots] = {};
-  int frame_next = 0;
-
-  // maneuver table (device)
-  double* man_t = nullptr;
-  float* man_acc = nullptr;
-  float* man_omega = nullptr;
-  int man_cap = 0;
-  // host copy of the table (for host-side evaluation at set time)
-  std::vector<double> h_man_t;
-  std::vector<float> h_man_acc, h_man_omega;
-
-  // solver state on the host side
-  bool has_particles = false, initialized = false, has_vapor = false;
-  float char_length = 0;
-  float pass_dt = 0;
-
-  // batched stepping: the ensemble this tank belongs to (if any), an event
-  // for ordering its stream against the ensemble's, and a counter bumped
-  // whenever the step graphs are invalidated (the ensemble then rebuilds)
-  cryo_ensemble* ensemble = nullptr;
-  cudaEvent_t ens_ev = nullptr;
-  unsigned long long generation = 0;
-
-  // slab decomposition: the group this context is one slab of (null: it
-  // holds the whole tank)
-  SlabGroup* slab_group = nullptr;
-  int slab_rank = 0;
-  void slab_point(int what, int set);
-
-  // execution
-  bool graph_mode = true;
-  bool graph_valid[2] = {false, false};
-  cudaGraphExec_t graph[2] = {nullptr, nullptr};
-  bool use_lists = true;
-
-  // launch accounting / profiling
-  long long launch_counter = 0;
-  int step_launches = 0;
-  bool profiling = false;
-  struct Mark { cudaEvent_t a, b; int kernel; };
-  std::vector<Mark> marks;
-  std::vector<cudaEvent_t> event_pool;
-  size_t event_used = 0;
-  std::vector<std::string> prof_names;
-  std::vector<double> prof_ms;
-  std::vector<long long> prof_count;
-  int prof_current = -1;
-
-  // telemetry (TelemetryStream, telemetry.cu)
-  int tele_mode = 0;
-  size_t tele_cap = 0;
-  TelemetryRecord* tele_host = nullptr;
-  TelemetryRecord* tele_host_dev = nullptr;
-  TelemetryRecord* tele_stage = nullptr;
-  cudaStream_t tele_stream = nullptr;
-  cudaEvent_t tele_computed = nullptr, tele_landed = nullptr;
-  bool tele_pending = false;
-  double tele_time = 0;
-  long long tele_step = 0;
-  int tele_n = 0;
-
-  // differentiated window (cryo_adj_*), and the sums tape of the step being
-  // recomputed for it (View::tape; null otherwise)
-  AdjWindow* adj = nullptr;
-  float4* tape_sums = nullptr;
-  int tape_n = 0;
-
-  cudaEvent_t next_event() {
-    if (event_used == event_pool.size()) {
-      cudaEvent_t e;
-      CK(cudaEventCreate(&e));
-      event_pool.push_back(e);
-    }
-    return event_pool[event_used++];
-  }
-  void before_launch(const char* raw) {
-    ++launch_counter;
-    if (!profiling) return;
-    std::string name(raw);
-    const size_t lt = name.find('<');
-    if (lt != std::string::npos) name = name.substr(0, lt);
-    if (name == "k_forces_t") name = "k_forces";
-    int k = 0;
-    while (k < (int)prof_names.size() && prof_names[k] != name) ++k;
-    if (k == (int)prof_names.size()) {
-      prof_names.push_back(name);
-      prof_ms.push_back(0.0);
-      prof_count.push_back(0);
-    }
-    Mark m{next_event(), next_event(), k};
-    CK(cudaEventRecord(m.a, stream));
-    marks.push_back(m);
-  }
-  void after_launch() {
-    if (!profiling) return;
-    CK(cudaEventRecord(marks.back().b, stream));
-  }
-  void collect_marks() {
-    if (marks.empty()) return;
-    CK(cudaStreamSynchronize(stream));
-    for (const Mark& m : marks) {
-      float ms = 0;
-      CK(cudaEventElapsedTime(&ms, m.a, m.b));
-      prof_ms[m.kernel] += ms;
-      prof_count[m.kernel] += 1;
-    }
-    marks.clear();
-    event_used = 0;
-  }
-  void telemetry_release() {
-    if (tele_pending) {
-      cudaEventSynchronize(tele_mode == 1 ? tele_computed : tele_landed);
-      tele_pending = false;
-    }
-    if (tele_host) cudaFreeHost(tele_host);
-    if (tele_stage) cudaFree(tele_stage);
-    if (tele_stream) cudaStreamDestroy(tele_stream);
-    if (tele_computed) cudaEventDestroy(tele_computed);
-    if (tele_landed) cudaEventDestroy(tele_landed);
-    tele_host = tele_host_dev = tele_stage = nullptr;
-    tele_stream = nullptr;
-    tele_computed = tele_landed = nullptr;
-    tele_cap = 0;
-  }
-
-  ~cryo_ctx() {
-    if (ensemble) ensemble_detach(ensemble, this);
-    if (adj) {
-      if (stream) cudaStreamSynchronize(stream);
-      adj_free(adj);
-    }
-    if (ens_ev) cudaEventDestroy(ens_ev);
-    telemetry_release();
-    for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
-    for (int k = 0; k < 2; ++k)
-      if (graph[k]) cudaGraphExecDestroy(graph[k]);
-    if (stream) cudaStreamSynchronize(stream);
-    arena.release();
-    if (cell_begin) cudaFree(cell_begin);
-    if (cell_fluid) cudaFree(cell_fluid);
-    if (dyn) cudaFree(dyn);
-    if (hdyn) cudaFreeHost(hdyn);
-    if (diag_host) cudaFreeHost(diag_host);
-    if (frame_ring) cudaFreeHost(frame_ring);
-    for (cudaEvent_t e : frame_ev)
-      if (e) cudaEventDestroy(e);
-    if (man_t) cudaFree(man_t);
-    if (man_acc) cudaFree(man_acc);
-    if (man_omega) cudaFree(man_omega);
-    if (stream) cudaStreamDestroy(stream);
-  }
-
-  // ------------------------------------------------------------ helpers
-  View view(int s) const {
-    View V{};
-    V.xp = set[s].xp; V.vT = set[s].vT; V.vt = set[s].vt; V.nrm = set[s].nrm; V.mrps = set[s].mrps;
-    V.id = set[s].id;
-    V.a4 = a4; V.ab4 = ab4; V.fw = fw; V.mw = mw; V.vwp = vwp; V.ns4 = ns4; V.pc = pc;
-    V.rmin = rmin; V.wall_w = wall_w; V.heat_w = heat_w; V.nu_t = nu_t;
-    V.aux = aux;
-    V.cell_begin = cell_begin;
-    V.cell_fluid = cell_fluid;
-    V.dyn = dyn;
-    V.man_t = man_t; V.man_acc = man_acc; V.man_omega = man_omega;
-    V.partials = partials;
-    V.counters = ticket;
-    V.capacity = capacity;
-    V.nbr = nbr;
-    V.nbr_cnt = nbr_cnt;
-    V.fluid_idx = fluid_idx;
-    V.wall_idx = wall_idx;
-    V.tape = tape_sums;
-    V.tape_n = tape_n;
-    return V;
-  }
-  Reduce reduce() const { return Reduce{partials, ticket, max_chunks}; }
-  // Particles the launch grids are sized for (0: the capacity).  Every step
-  // kernel loops over its particles with a grid stride, so any grid gives
-  // the same results; a grid sized for the capacity (up to twice the count)
-  // only adds blocks that find no particle.
-  int grid_span = 0;
-  int span() const { return grid_span > 0 ? std::min(grid_span, capacity) : capacity; }
-  // the particle count last read plus head-room for splits; check_capacity
-  // drops the graphs when the count outgrows it
-  void size_grids() { grid_span = std::max(1, std::min(capacity, hdyn->n + hdyn->n / 8 + 1024)); }
-  int grid_blocks() const {
-    const int need = (span() + kBlock - 1) / kBlock;
-    return std::max(1, std::min(need, sm_count * 8));
-  }
-  // force pass: one thread per particle up to two full-occupancy waves
-  int forces_blocks() const {
-    const int need = (span() + FORCES_BLOCK - 1) / FORCES_BLOCK;
-    return std::max(1, std::min(need, sm_count * (2048 / FORCES_BLOCK) * 2));
-  }
-  void invalidate_graphs() {
-    ++generation;
-    for (int k = 0; k < 2; ++k) {
-      if (graph[k]) cudaGraphExecDestroy(graph[k]);
-      graph[k] = nullptr;
-      graph_valid[k] = false;
-    }
-  }
-  void sync() { CK(cudaStreamSynchronize(stream)); }
-  void pull() {  // device scalar block -> host mirror
-    CK(cudaMemcpyAsync(hdyn, dyn, sizeof(DynState), cudaMemcpyDeviceToHost, stream));
-    sync();
-    if (man_active) hframe = hdyn->fr;
-  }
-  void push() {  // host mirror -> device scalar block
-    if (!man_active) hdyn->fr = hframe;
-    CK(cudaMemcpyAsync(dyn, hdyn, sizeof(DynState), cudaMemcpyHostToDevice, stream));
-    sync();
-  }
-  // Sends the host frame state without synchronising: the copy reads a
-  // pinned ring slot that is not reused until its previous copy completed.
-  void push_frame() {
-    const int k = frame_next;
-    frame_next = (frame_next + 1) % kFrameSlots;
-    CK(cudaEventSynchronize(frame_ev[k]));
-    frame_ring[k] = hframe;
-    CK(cudaMemcpyAsync(&dyn->fr, frame_ring + k, sizeof(DynState::Frame), cudaMemcpyHostToDevice, stream));
-    CK(cudaEventRecord(frame_ev[k], stream));
-  }
-
-  // -------------------------------------------------------- allocation
-  void allocate(int cap) {
-    sync();
-    invalidate_graphs();
-    Arena a;
-    a.size = particle_bytes((size_t)cap);
-    CK(cudaMalloc(&a.base, a.size));
-    CK(cudaMemsetAsync(a.base, 0, a.size, stream));
-    Persist ns[2];
-    for (int s = 0; s < 2; ++s) {
-      ns[s].xp = a.take<float4>(cap); ns[s].vT = a.take<float4>(cap); ns[s].vt = a.take<float4>(cap);
-      ns[s].nrm = a.take<float4>(cap); ns[s].mrps = a.take<float4>(cap); ns[s].id = a.take<uint32_t>(cap);
-    }
-    float4* na4 = a.take<float4>(cap); float4* nab4 = a.take<float4>(cap); float4* nfw = a.take<float4>(cap);
-    float4* nmw = a.take<float4>(cap); float4* nvwp = a.take<float4>(cap); float4* nns4 = a.take<float4>(cap);
-    float4* npc = a.take<float4>(cap);
-    float4* naux = a.take<float4>(cap);
-    float* nrmin = a.take<float>(cap); float* nwall = a.take<float>(cap); float* nheat = a.take<float>(cap);
-    float* nnut = a.take<float>(cap);
-    uint32_t* nka = a.take<uint32_t>(cap); uint32_t* nkb = a.take<uint32_t>(cap);
-    uint32_t* nva = a.take<uint32_t>(cap); uint32_t* nvb = a.take<uint32_t>(cap);
-    uint32_t* nsf = a.take<uint32_t>(cap);
-    const size_t tiles = (size_t)(cap + RS_TILE - 1) / RS_TILE + 1;
-    uint32_t* nhist = a.take<uint32_t>(tiles * RS_BINS + RS_BINS);
-    const int nchunks = cap / kChunk + 2;
-    double* npart = a.take<double>((size_t)nchunks * 32);
-    double* ndiag = a.take<double>(64);
-    unsigned* ntick = a.take<unsigned>(64);
-    int* nnbr = a.take<int>((size_t)cap * kMaxNbr);
-    int* nnc = a.take<int>(cap);
-    int* nfi = a.take<int>(cap);
-    int* nwi = a.take<int>(cap);
-    if (a.used > a.size) throw std::runtime_error("internal: arena overflow");
-    // keep the first n particles of every array (ParticleSystem::grow,
-    // particle_system.cpp:66-71)
-    if (arena.base && capacity > 0) {
-      pull();
-      const size_t keep = (size_t)std::min(hdyn->n, cap);
-      auto cp = [&](void* dst, const void* src, size_t elem) {
-        if (keep) CK(cudaMemcpyAsync(dst, src, keep * elem, cudaMemcpyDeviceToDevice, stream));
-      };
-      for (int s = 0; s < 2; ++s) {
-        cp(ns[s].xp, set[s].xp, 16); cp(ns[s].vT, set[s].vT, 16); cp(ns[s].vt, set[s].vt, 16);
-        cp(ns[s].nrm, set[s].nrm, 16); cp(ns[s].mrps, set[s].mrps, 16); cp(ns[s].id, set[s].id, 4);
-      }
-      cp(na4, a4, 16); cp(nab4, ab4, 16); cp(nfw, fw, 16); cp(nmw, mw, 16); cp(nvwp, vwp, 16); cp(nns4, ns4, 16);
-      cp(npc, pc, 16); cp(naux, aux, 16); cp(nrmin, rmin, 4); cp(nwall, wall_w, 4); cp(nheat, heat_w, 4); cp(nnut, nu_t, 4);
-      sync();
-    }
-    arena.release();
-    arena = a;
-    set[0] = ns[0]; set[1] = ns[1];
-    a4 = na4; ab4 = nab4; fw = nfw; mw = nmw; vwp = nvwp; ns4 = nns4; pc = npc; aux = naux;
-    rmin = nrmin; wall_w = nwall; heat_w = nheat; nu_t = nnut;
-    keys_a = nka; keys_b = nkb; vals_a = nva; vals_b = nvb; split_flag = nsf;
-    hist = nhist; partials = npart; max_chunks = nchunks; diag_out = ndiag; ticket = ntick;
-    nbr = nnbr; nbr_cnt = nnc; fluid_idx = nfi; wall_idx = nwi;
-    sorted_keys = nullptr;
-    sorted_perm = nullptr;
-    capacity = cap;
-    if (hdyn) {
-      pull();
-      hdyn->capacity = cap;
-      push();
-    }
-  }
-
-  // --------------------------------------------------- parameter lowering
-  void init_params();
-  void configure_grid(const float* lo, const float* hi);
-  void begin_load(int n, bool vapor, const float* lo, const float* hi);
-  void finish_load(int n, uint32_t next_id);
-
-  // ------------------------------------------------------ step pieces
-  void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
-  void sort_and_gather(int src, int list_mode);  // after keys_a holds the keys
-  void evaluate_rates(int s, bool maxima_reset, bool density_done, bool tape = false);
-  void enqueue_step(int s, const StepTape* tape = nullptr);
-  void launch_step();
-  void ensure_initialized();
-  void check_capacity();
-  void run_steps(long long n);
-  void run_until(double t_end);
-};
+namespace cryo {
+thread_local std::string g_create_error;
+}  // namespace cryo
 
 // -------------------------------------------------------------------------
 // Solver::init_params (sph_solver.cu:292-405), host single precision in the
@@ -904,244 +442,7 @@ void cryo_ctx::run_until(double t_end) {
 }
 
 // ---------------------------------------------------------------------------
-// Batched stepping of independent tanks (no counterpart in the reference).
-// Each tank keeps its own context: arena, stream, parameters and step
-// sequence.  A graph launch holds `per_launch` consecutive steps of every
-// tank, each tank's steps a chain of that tank's own kernels, spread over
-// `chains` concurrent branches (tanks assigned longest-processing-time first
-// by particle count; one branch per tank by default).  Tanks far too small
-// to fill the GPU alone then run side by side, and several steps per launch
-// spare the drain at every launch boundary.  Every tank runs exactly the
-// kernels, launch shapes and arguments of its own step graph, so its results
-// are those of stepping it alone, bit for bit.
-struct cryo_ensemble {
-  struct Graphs {  // one launch shape: `steps` steps from either parity
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};
-    int steps = 0;
-    void drop() {
-      for (int k = 0; k < 2; ++k) {
-        if (exec[k]) cudaGraphExecDestroy(exec[k]);
-        exec[k] = nullptr;
-      }
-      steps = 0;
-    }
-  };
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  cudaEvent_t fork = nullptr, done = nullptr, t0 = nullptr, t1 = nullptr;
-  std::vector<cryo_ctx*> tanks;
-  int chains = 0;      // 0: one branch per tank
-  int per_launch = 1;  // steps per graph launch (divides 16)
-  Graphs multi, single;
-  std::vector<int> built_cur;  // each tank's ping-pong parity when the graphs were built
-  std::vector<unsigned long long> built_gen;
-  int built_chains = -1;
-  int phase = 0;  // steps taken since the build, mod 2
-  int step_launches = 0;
-  long long steps_run = 0;
-  std::string err;
-
-  ~cryo_ensemble() {
-    if (stream) cudaStreamSynchronize(stream);
-    drop();
-    for (cryo_ctx* c : tanks) c->ensemble = nullptr;
-    for (cudaEvent_t e : {fork, done, t0, t1})
-      if (e) cudaEventDestroy(e);
-    if (stream) cudaStreamDestroy(stream);
-  }
-  void drop() {
-    multi.drop();
-    single.drop();
-    built_chains = -1;
-  }
-  int branches() const {
-    const int t = (int)tanks.size();
-    return chains <= 0 ? t : std::min(chains, t);
-  }
-  bool valid() const {
-    if (built_chains != branches() || multi.steps != per_launch) return false;
-    for (size_t t = 0; t < tanks.size(); ++t)
-      if (tanks[t]->generation != built_gen[t] || tanks[t]->cur != ((built_cur[t] + phase) & 1)) return false;
-    return true;
-  }
-  // Tanks per branch: largest first, each to the least-loaded branch.
-  std::vector<std::vector<int>> plan() const {
-    const int k = branches();
-    std::vector<int> order(tanks.size());
-    for (size_t t = 0; t < tanks.size(); ++t) order[t] = (int)t;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return tanks[a]->hdyn->n > tanks[b]->hdyn->n; });
-    std::vector<std::vector<int>> out(k);
-    std::vector<long long> load(k, 0);
-    for (int t : order) {
-      int best = 0;
-      for (int b = 1; b < k; ++b)
-        if (load[b] < load[best]) best = b;
-      out[best].push_back(t);
-      load[best] += std::max(tanks[t]->hdyn->n, 1);
-    }
-    return out;
-  }
-  // `steps` steps of every tank starting at parity offset q, as one graph.
-  void capture(int q, int steps, const std::vector<std::vector<int>>& branches_plan, cudaGraphExec_t* out) {
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
-    int launches = 0;
-    try {
-      CK(cudaEventRecord(fork, stream));
-      for (const auto& br : branches_plan) {
-        cudaEvent_t prev = fork;
-        for (int t : br) {
-          cryo_ctx* c = tanks[t];
-          CK(cudaStreamWaitEvent(c->stream, prev, 0));
-          for (int k = 0; k < steps; ++k) {
-            const long long c0 = c->launch_counter;
-            c->enqueue_step((built_cur[t] + q + k) & 1);
-            launches += (int)(c->launch_counter - c0);
-          }
-          CK(cudaEventRecord(c->ens_ev, c->stream));
-          prev = c->ens_ev;
-        }
-      }
-      for (cryo_ctx* c : tanks) CK(cudaStreamWaitEvent(stream, c->ens_ev, 0));
-    } catch (...) {
-      cudaStreamEndCapture(stream, &g);
-      if (g) cudaGraphDestroy(g);
-      throw;
-    }
-    CK(cudaStreamEndCapture(stream, &g));
-    const cudaError_t e = cudaGraphInstantiate(out, g, 0);
-    cudaGraphDestroy(g);
-    CK(e);
-    step_launches = launches / std::max(steps, 1);
-  }
-  // Graphs for both start parities (a run can reach either before a launch).
-  void build_shape(Graphs& gr, int steps, const std::vector<std::vector<int>>& pl) {
-    gr.drop();
-    capture(0, steps, pl, &gr.exec[0]);
-    capture(1, steps, pl, &gr.exec[1]);
-    gr.steps = steps;
-  }
-  void build() {
-    drop();
-    leave();
-    for (cryo_ctx* c : tanks) {  // particle counts for the plan and the launch grids
-      c->pull();
-      c->size_grids();
-    }
-    enter();
-    built_cur.resize(tanks.size());
-    built_gen.resize(tanks.size());
-    for (size_t t = 0; t < tanks.size(); ++t) {
-      built_cur[t] = tanks[t]->cur;
-      built_gen[t] = tanks[t]->generation;
-    }
-    phase = 0;
-    const auto pl = plan();
-    build_shape(multi, per_launch, pl);
-    if (per_launch > 1) build_shape(single, 1, pl);
-    built_chains = branches();
-  }
-  // tank streams -> ensemble stream, and back
-  void enter() {
-    for (cryo_ctx* c : tanks) {
-      CK(cudaEventRecord(c->ens_ev, c->stream));
-      CK(cudaStreamWaitEvent(stream, c->ens_ev, 0));
-    }
-  }
-  void leave() {
-    CK(cudaEventRecord(done, stream));
-    for (cryo_ctx* c : tanks) CK(cudaStreamWaitEvent(c->stream, done, 0));
-  }
-  void prepare() {
-    for (cryo_ctx* c : tanks) {
-      if (c->profiling) throw std::invalid_argument("ensemble: a tank has per-kernel profiling on");
-      c->ensure_initialized();
-    }
-  }
-  // One launch of `steps` (per_launch or 1) steps of every tank.
-  void launch(int steps) {
-    const Graphs& gr = (steps == per_launch) ? multi : single;
-    CK(cudaGraphLaunch(gr.exec[phase], stream));
-    phase = (phase + steps) & 1;
-    for (cryo_ctx* c : tanks) c->cur = (c->cur + steps) & 1;
-    steps_run += steps;
-  }
-  // Head-room for splits, per tank, between steps (sph_solver.cu:556-560).
-  void check_capacity() {
-    leave();
-    for (cryo_ctx* c : tanks) c->check_capacity();
-  }
-  void run(long long n) {
-    if (tanks.empty() || n <= 0) return;
-    prepare();
-    enter();
-    long long since_check = 0;
-    while (n > 0) {
-      if (!valid()) build();
-      const int k = n >= per_launch ? per_launch : 1;
-      launch(k);
-      n -= k;
-      since_check += k;
-      if (since_check >= 16 && n > 0) {
-        check_capacity();
-        enter();
-        since_check = 0;
-      }
-    }
-    check_capacity();
-  }
-  // Device time per step over `steps` steps (rounded up to whole launches)
-  // with the current shape, after one untimed launch that also builds it.
-  float time_steps(int steps) {
-    run(per_launch);
-    enter();
-    if (!valid()) build();
-    const int launches = std::max(1, (steps + per_launch - 1) / per_launch);
-    CK(cudaEventRecord(t0, stream));
-    for (int k = 0; k < launches; ++k) launch(per_launch);
-    CK(cudaEventRecord(t1, stream));
-    check_capacity();
-    CK(cudaEventSynchronize(t1));
-    float ms = 0.0f;
-    CK(cudaEventElapsedTime(&ms, t0, t1));
-    return ms / (float)(launches * per_launch);
-  }
-};
-
-void ensemble_detach(cryo_ensemble* e, cryo_ctx* c) {
-  cudaStreamSynchronize(e->stream);
-  e->drop();
-  e->tanks.erase(std::remove(e->tanks.begin(), e->tanks.end(), c), e->tanks.end());
-  c->ensemble = nullptr;
-}
-
-// ---------------------------------------------------------------------------
 namespace {
-
-thread_local std::string g_create_error;
-
-template <class F>
-int guard(cryo_ctx* ctx, F&& f) {
-  try {
-    f();
-    return CRYO_OK;
-  } catch (const std::invalid_argument& e) {
-    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
-    return CRYO_EINVAL;
-  } catch (const std::out_of_range& e) {
-    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
-    return CRYO_ERANGE;
-  } catch (const CudaError& e) {
-    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
-    return CRYO_ECUDA;
-  } catch (const std::exception& e) {
-    if (ctx) ctx->err = e.what(); else g_create_error = e.what();
-    return CRYO_ERUNTIME;
-  }
-}
-
-void set3(float* d, const float* s) { d[0] = s[0]; d[1] = s[1]; d[2] = s[2]; }
 
 void fluid_from(int which, cryo_fluid_t* f) {
   // FluidProperties presets (fluid_properties.cpp:16-79); custom = the
@@ -1334,6 +635,12 @@ void cryo_ctx::begin_load(int n, bool vap, const float* lo, const float* hi) {
         "Solver: the Akinci surface-tension model is a free-surface (liquid-only) model; use CSF when vapour "
         "particles are present (FillSpec.include_vapor = false for Akinci runs)");
   sync();
+  // What the step graphs captured: the parameter block (by value), the arena
+  // and cell-table addresses, and the launch grids sized for the count.
+  const Params old_P = P;
+  const void* old_arena = arena.base;
+  const int* old_cells = cell_begin;
+  const int old_n = loaded_n;
   has_vapor = vap;
   const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
   float cl = ex;
@@ -1352,7 +659,14 @@ void cryo_ctx::begin_load(int n, bool vap, const float* lo, const float* hi) {
     }
   }
   this->configure_grid(lo, hi);
-  this->invalidate_graphs();
+  // A reload with the same count, parameters, grid and storage (an
+  // optimisation or restart loop) keeps the captured step graphs: every
+  // argument they hold is unchanged, so its first step replays instead of
+  // capturing again.  Anything else drops them.
+  const bool same = n == old_n && old_arena == arena.base && old_cells == cell_begin &&
+                    std::memcmp(&old_P, &P, sizeof(Params)) == 0;
+  if (!same) this->invalidate_graphs();
+  loaded_n = n;
   cur = 0;
 }
 
@@ -1728,7 +1042,6 @@ int cryo_capacity(cryo_ctx* c, int* cap) {
 
 // Solver::diagnostics (sph_solver.cu:609-653): one reduction kernel and one
 // device-to-host copy.
-static void diag_fill(const double* v, cryo_diagnostics_t* o);
 
 int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
   return guard(c, [&] {
@@ -1744,7 +1057,8 @@ int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
 }
 
 // The Diagnostics record from the k_diagnostics output row.
-static void diag_fill(const double* v, cryo_diagnostics_t* o) {
+}  // extern "C"
+void cryo::diag_fill(const double* v, cryo_diagnostics_t* o) {
   std::memset(o, 0, sizeof(*o));
   o->time = v[25];
   o->step = (long long)v[26];
@@ -1784,6 +1098,7 @@ static void diag_fill(const double* v, cryo_diagnostics_t* o) {
     o->frame_angular_velocity[k] = (float)v[41 + k];
   }
 }
+extern "C" {
 
 int cryo_get_field(cryo_ctx* c, int field, void* out, size_t cap) {
   return guard(c, [&] {
@@ -2516,1251 +1831,5 @@ int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {
   });
 }
 
-
-// ------------------------------------------------------------ ensembles
-}  // extern "C"
-namespace {
-template <class F>
-int eguard(cryo_ensemble* e, F&& f) {
-  try {
-    f();
-    return CRYO_OK;
-  } catch (const std::invalid_argument& x) {
-    if (e) e->err = x.what(); else g_create_error = x.what();
-    return CRYO_EINVAL;
-  } catch (const std::out_of_range& x) {
-    if (e) e->err = x.what(); else g_create_error = x.what();
-    return CRYO_ERANGE;
-  } catch (const CudaError& x) {
-    if (e) e->err = x.what(); else g_create_error = x.what();
-    return CRYO_ECUDA;
-  } catch (const std::exception& x) {
-    if (e) e->err = x.what(); else g_create_error = x.what();
-    return CRYO_ERUNTIME;
-  }
-}
-}  // namespace
-extern "C" {
-
-int cryo_ensemble_create(int device, cryo_ensemble** out) {
-  *out = nullptr;
-  cryo_ensemble* e = nullptr;
-  const int rc = eguard(nullptr, [&] {
-    e = new cryo_ensemble;
-    try {
-      e->device = device;
-      CK(cudaSetDevice(device));
-      CK(cudaStreamCreateWithFlags(&e->stream, cudaStreamDefault));
-      CK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&e->done, cudaEventDisableTiming));
-      CK(cudaEventCreate(&e->t0));
-      CK(cudaEventCreate(&e->t1));
-    } catch (...) {
-      delete e;
-      e = nullptr;
-      throw;
-    }
-  });
-  *out = e;
-  return rc;
-}
-
-void cryo_ensemble_destroy(cryo_ensemble* e) { delete e; }
-
-const char* cryo_ensemble_last_error(const cryo_ensemble* e) { return e ? e->err.c_str() : g_create_error.c_str(); }
-
-int cryo_ensemble_add(cryo_ensemble* e, cryo_ctx* c) {
-  return eguard(e, [&] {
-    if (!c) throw std::invalid_argument("ensemble: null tank");
-    if (c->ensemble) throw std::invalid_argument("ensemble: the tank already belongs to an ensemble");
-    if (c->device != e->device) throw std::invalid_argument("ensemble: the tank lives on another device");
-    if (!c->has_particles) throw std::invalid_argument("ensemble: the tank has no particles");
-    if (!c->ens_ev) CK(cudaEventCreateWithFlags(&c->ens_ev, cudaEventDisableTiming));
-    CK(cudaStreamSynchronize(e->stream));
-    e->drop();
-    e->tanks.push_back(c);
-    c->ensemble = e;
-  });
-}
-
-int cryo_ensemble_remove(cryo_ensemble* e, cryo_ctx* c) {
-  return eguard(e, [&] {
-    if (!c || c->ensemble != e) throw std::invalid_argument("ensemble: the tank is not a member");
-    ensemble_detach(e, c);
-  });
-}
-
-int cryo_ensemble_size(cryo_ensemble* e, int* tanks) {
-  return eguard(e, [&] { *tanks = (int)e->tanks.size(); });
-}
-
-int cryo_ensemble_set_chains(cryo_ensemble* e, int chains) {
-  return eguard(e, [&] {
-    if (chains < 0) throw std::invalid_argument("ensemble: chains must be >= 0");
-    e->chains = chains;
-  });
-}
-
-int cryo_ensemble_chains(cryo_ensemble* e, int* chains) {
-  return eguard(e, [&] { *chains = e->branches(); });
-}
-
-int cryo_ensemble_set_steps_per_launch(cryo_ensemble* e, int steps) {
-  return eguard(e, [&] {
-    if (steps < 1 || steps > 16 || (16 % steps) != 0)
-      throw std::invalid_argument("ensemble: steps per launch must be 1, 2, 4, 8 or 16");
-    e->per_launch = steps;
-  });
-}
-
-int cryo_ensemble_steps_per_launch(cryo_ensemble* e, int* steps) {
-  return eguard(e, [&] { *steps = e->per_launch; });
-}
-
-int cryo_ensemble_run_steps(cryo_ensemble* e, long long n) {
-  return eguard(e, [&] { e->run(n); });
-}
-
-int cryo_ensemble_step_time(cryo_ensemble* e, int steps, float* ms_per_step) {
-  return eguard(e, [&] {
-    if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
-    *ms_per_step = e->tanks.empty() ? 0.0f : e->time_steps(steps);
-  });
-}
-
-int cryo_ensemble_tune(cryo_ensemble* e, const int* chain_candidates, int nchain, const int* launch_candidates,
-                       int nlaunch, int steps, int* best_chains, int* best_steps_per_launch, float* best_ms) {
-  return eguard(e, [&] {
-    if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
-    const int t = (int)e->tanks.size();
-    if (t == 0) throw std::invalid_argument("ensemble: no tanks");
-    std::vector<int> cc, lc;
-    if (chain_candidates && nchain > 0) cc.assign(chain_candidates, chain_candidates + nchain);
-    else for (int k = t; k >= 1; k /= 2) cc.push_back(k);
-    if (launch_candidates && nlaunch > 0) lc.assign(launch_candidates, launch_candidates + nlaunch);
-    else lc.push_back(e->per_launch);
-    for (int k : cc)
-      if (k < 0) throw std::invalid_argument("ensemble: chain counts must be >= 0");
-    for (int k : lc)
-      if (k < 1 || k > 16 || (16 % k) != 0)
-        throw std::invalid_argument("ensemble: steps per launch must be 1, 2, 4, 8 or 16");
-    int best_c = -1, best_l = 1;
-    float best_t = 0.0f;
-    for (int l : lc)
-      for (int k : cc) {
-        e->chains = k;
-        e->per_launch = l;
-        const float ms = e->time_steps(steps);
-        if (best_c < 0 || ms < best_t) {
-          best_c = k;
-          best_l = l;
-          best_t = ms;
-        }
-      }
-    e->chains = best_c;
-    e->per_launch = best_l;
-    if (best_chains) *best_chains = best_c;
-    if (best_steps_per_launch) *best_steps_per_launch = best_l;
-    if (best_ms) *best_ms = best_t;
-  });
-}
-
-int cryo_ensemble_launches_per_step(cryo_ensemble* e, int* launches) {
-  return eguard(e, [&] { *launches = e->step_launches; });
-}
-
-int cryo_ensemble_synchronize(cryo_ensemble* e) {
-  return eguard(e, [&] { CK(cudaStreamSynchronize(e->stream)); });
-}
-
-uintptr_t cryo_ensemble_stream(const cryo_ensemble* e) { return reinterpret_cast<uintptr_t>(e->stream); }
-
-}  // extern "C"
-
-// ---------------------------------------------------------------------------
-// Differentiated window (no counterpart in the reference).  The forward run
-// steps as usual (step graphs), keeps a state checkpoint every `every` steps
-// and integrates the slosh force and moment.  The backward sweep takes the
-// segments from the last: it restores the segment's checkpoint, re-runs the
-// segment keeping every step's start state, then for each step from the last
-// restores its start state, recomputes it eagerly with the one-step tape and
-// runs the reverse passes (cryo_adjoint.cu).  At the end the window's final
-// state is restored, so the solver continues as if only the forward had run.
-namespace {
-
-struct AdjSnap {
-  char* base = nullptr;
-  int cur = 0;
-};
-
-}  // namespace
-
-struct AdjWindow {
-  int n = 0, every = 20, cap = 0;
-  long long steps = 0;
-  bool recorded = false;
-  int splits0 = 0, merges0 = 0;
-  char* arena = nullptr;
-  size_t bytes = 0, snap_bytes = 0;
-  std::vector<AdjSnap> ckpt;  // start of every segment + the window's end
-  // one per step of a segment: the step's tape and its end-of-step arrays
-  struct Slot {
-    StepTape tape;
-    AdjSlot end;
-  };
-  std::vector<Slot> slots;
-  size_t slot_bytes = 0;
-  float4 *cX[2]{}, *cV[2]{}, *cA[2]{}, *cB[2]{};
-  float4 *gP = nullptr, *gN = nullptr, *gG = nullptr, *gC = nullptr, *gU1 = nullptr, *gU2 = nullptr,
-         *gU3 = nullptr, *R1 = nullptr, *R2 = nullptr;
-  int* argmax = nullptr;
-  double *glob = nullptr, *partials = nullptr, *obj = nullptr, *ggrav = nullptr;
-  unsigned *ticket = nullptr, *status = nullptr;
-  int max_chunks = 0;
-  int q = 0;
-  // final-state seeds (float4 per particle, final order): x|m, v|T, a, ab
-  std::vector<float4> seed[4];
-};
-
-void adj_free(AdjWindow* w) {
-  if (!w) return;
-  if (w->arena) cudaFree(w->arena);
-  delete w;
-}
-
-namespace {
-
-constexpr int kSnap16 = 7;  // xp, vT, vt, nrm, mrps, a4, ab4
-
-size_t r256(size_t b) { return (b + 255) & ~size_t(255); }
-
-size_t snap_size(int n) { return kSnap16 * r256((size_t)n * 16) + r256((size_t)n * 4) + r256(sizeof(DynState)); }
-
-void snap_save(cryo_ctx* c, AdjWindow& W, AdjSnap& S) {
-  const size_t n = (size_t)W.n;
-  const Persist& p = c->set[c->cur];
-  const void* src[kSnap16] = {p.xp, p.vT, p.vt, p.nrm, p.mrps, c->a4, c->ab4};
-  char* q = S.base;
-  for (const void* a : src) {
-    CK(cudaMemcpyAsync(q, a, n * 16, cudaMemcpyDeviceToDevice, c->stream));
-    q += r256(n * 16);
-  }
-  CK(cudaMemcpyAsync(q, p.id, n * 4, cudaMemcpyDeviceToDevice, c->stream));
-  q += r256(n * 4);
-  CK(cudaMemcpyAsync(q, c->dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
-  S.cur = c->cur;
-}
-
-void snap_load(cryo_ctx* c, AdjWindow& W, const AdjSnap& S) {
-  const size_t n = (size_t)W.n;
-  c->cur = S.cur;
-  const Persist& p = c->set[c->cur];
-  void* dst[kSnap16] = {p.xp, p.vT, p.vt, p.nrm, p.mrps, c->a4, c->ab4};
-  const char* q = S.base;
-  for (void* a : dst) {
-    CK(cudaMemcpyAsync(a, q, n * 16, cudaMemcpyDeviceToDevice, c->stream));
-    q += r256(n * 16);
-  }
-  CK(cudaMemcpyAsync(p.id, q, n * 4, cudaMemcpyDeviceToDevice, c->stream));
-  q += r256(n * 4);
-  CK(cudaMemcpyAsync(c->dyn, q, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
-}
-
-// The configurations the reverse passes cover.
-void adj_check_config(const cryo_ctx* c) {
-  const cryo_config_t& g = c->cfg;
-  const Params& P = c->P;
-  auto no = [](const char* what) { throw std::invalid_argument(std::string("adjoint: not supported: ") + what); };
-  if (!(P.fixed_dt > 0.0f)) no("adaptive time step (set fixed_dt)");
-  if (!(g.sound_speed > 0 || g.velocity_scale > 0)) no("sound speed derived from the surface tension (set sound_speed)");
-  if (P.density_mode != CRYO_DENSITY_SUMMATION) no("continuity density");
-  if (P.sps) no("SPS turbulence");
-  if (P.shift_strength > 0.0f) no("particle shifting");
-  if (P.tvf_stress) no("transport-velocity stress");
-  if (P.st_model == CRYO_ST_AKINCI) no("Akinci surface tension");
-  if (P.csf_smooth || P.csf_balanced) no("smoothed or balanced CSF");
-  if (P.wetting_model != 0) no("contact-line force wetting");
-  if (P.wall_bc != CRYO_WALL_ADIABATIC) no("isothermal walls");
-  if (P.clamp_neg) no("negative-pressure clamp");
-  if (g.thermo_mode == CRYO_THERMO_VENTED && c->has_vapor && P.cfg_phase_change) no("vented tank");
-}
-
-// Device bytes of one segment slot: the tape and end-of-step arrays of one
-// step, every per-particle array sized by the capacity.
-size_t slot_size(int cap, int num_cells) {
-  const size_t c16 = r256((size_t)cap * 16), c4 = r256((size_t)cap * 4);
-  return 4 * c16 + 2 * c4 + r256(sizeof(DynState))  // mid-step tape
-         + 6 * c16                                   // force / interface sums
-         + 7 * c16 + c4                              // xp vT vt nrm mrps a4 vwp, heat_w
-         + 4 * c4                                    // perm, list counts, phase index lists
-         + r256((size_t)cap * 4 * kMaxNbr)           // lists
-         + r256((size_t)(num_cells + 1) * 4) + r256(sizeof(DynState));
-}
-
-void adj_alloc(cryo_ctx* c, AdjWindow& W, long long steps, int every) {
-  // snapshots hold the window's n particles; the tape and the adjoints are
-  // sized by the capacity, which every kernel's particle count stays within
-  const int n = W.cap;
-  const long long nck = (steps + every - 1) / every + 1;
-  const int nslot = (int)std::min<long long>(every, steps);
-  W.snap_bytes = snap_size(W.n);
-  W.slot_bytes = slot_size(n, c->P.num_cells);
-  const size_t n16 = r256((size_t)n * 16), n4 = r256((size_t)n * 4);
-  W.max_chunks = n / kChunk + 2;
-  size_t t = (size_t)nck * W.snap_bytes + (size_t)nslot * W.slot_bytes;
-  t += 8 * n16 + 9 * n16 + n4;                                // adjoints, force-pass records
-  t += r256(AG_COUNT * 8) + r256((size_t)AR_COUNT * W.max_chunks * 8) + r256(8 * 8) + r256((size_t)steps * 3 * 8);
-  t += r256(64) + r256(64);
-  if (W.arena && W.bytes >= t) {
-    // reuse
-  } else {
-    if (W.arena) CK(cudaFree(W.arena));
-    W.arena = nullptr;
-    W.bytes = 0;
-    size_t free_b = 0, total_b = 0;
-    CK(cudaMemGetInfo(&free_b, &total_b));
-    if (t > free_b)
-      throw std::invalid_argument("adjoint: the window needs " + std::to_string(t >> 20) + " MiB of device memory, " +
-                                  std::to_string(free_b >> 20) +
-                                  " MiB are free; use a smaller checkpoint interval (one segment of steps is held "
-                                  "at a time) or a shorter window");
-    CK(cudaMalloc(&W.arena, t));
-    W.bytes = t;
-  }
-  char* p = W.arena;
-  auto take = [&](size_t b) {
-    char* r = p;
-    p += r256(b);
-    return r;
-  };
-  W.ckpt.assign((size_t)nck, AdjSnap{});
-  for (auto& s : W.ckpt) s.base = take(W.snap_bytes);
-  W.slots.assign((size_t)nslot, AdjWindow::Slot{});
-  for (auto& sl : W.slots) {
-    StepTape& tp = sl.tape;
-    tp.vT1 = (float4*)take(n16);
-    tp.ns1 = (float4*)take(n16);
-    tp.pc2 = (float4*)take(n16);
-    tp.vT2 = (float4*)take(n16);
-    tp.m1 = (float*)take(n4);
-    tp.m2 = (float*)take(n4);
-    tp.dyn1 = (DynState*)take(sizeof(DynState));
-    tp.sums = (float4*)take(6 * (size_t)n * 16);
-    tp.n = n;
-    AdjSlot& e = sl.end;
-    e.xp = (float4*)take(n16);
-    e.vT = (float4*)take(n16);
-    e.vt = (float4*)take(n16);
-    e.nrm = (float4*)take(n16);
-    e.mrps = (float4*)take(n16);
-    e.a4 = (float4*)take(n16);
-    e.vwp = (float4*)take(n16);
-    e.heat_w = (float*)take(n4);
-    e.perm = (uint32_t*)take(n4);
-    e.nbr_cnt = (int*)take(n4);
-    e.fluid_idx = (int*)take(n4);
-    e.wall_idx = (int*)take(n4);
-    e.nbr = (int*)take((size_t)n * 4 * kMaxNbr);
-    e.cell_begin = (int*)take((size_t)(c->P.num_cells + 1) * 4);
-    e.dyn = (DynState*)take(sizeof(DynState));
-  }
-  for (int k = 0; k < 2; ++k) {
-    W.cX[k] = (float4*)take(n16);
-    W.cV[k] = (float4*)take(n16);
-    W.cA[k] = (float4*)take(n16);
-    W.cB[k] = (float4*)take(n16);
-  }
-  W.gP = (float4*)take(n16);
-  W.gN = (float4*)take(n16);
-  W.gG = (float4*)take(n16);
-  W.gC = (float4*)take(n16);
-  W.gU1 = (float4*)take(n16);
-  W.gU2 = (float4*)take(n16);
-  W.gU3 = (float4*)take(n16);
-  W.R1 = (float4*)take(n16);
-  W.R2 = (float4*)take(n16);
-  W.argmax = (int*)take(n4);
-  W.glob = (double*)take(AG_COUNT * 8);
-  W.partials = (double*)take((size_t)AR_COUNT * W.max_chunks * 8);
-  W.obj = (double*)take(8 * 8);
-  W.ggrav = (double*)take((size_t)steps * 3 * 8);
-  W.ticket = (unsigned*)take(64);
-  W.status = (unsigned*)take(64);
-  if ((size_t)(p - W.arena) > W.bytes) throw std::runtime_error("internal: adjoint arena overflow");
-  CK(cudaMemsetAsync(W.ticket, 0, 64, c->stream));
-  CK(cudaMemsetAsync(W.status, 0, 64, c->stream));
-  W.steps = steps;
-  W.every = every;
-}
-
-#define ALAUNCH(c, K, G, B, ...)                      \
-  do {                                                \
-    ++(c)->launch_counter;                            \
-    K<<<(G), (B), 0, (c)->stream>>>(__VA_ARGS__);     \
-    LAUNCH_CHECK();                                   \
-  } while (0)
-
-// End-of-step copies into a slot: the per-particle arrays by one kernel, the
-// lists (chunk rows of n entries), the cell table and the scalar block by
-// copies.
-void adj_snap_end(cryo_ctx* c, AdjWindow& W, AdjWindow::Slot& sl) {
-  const View V = c->view(c->cur);
-  ALAUNCH(c, k_adj_snap_end, c->grid_blocks(), kBlock, V, c->sorted_perm, sl.end);
-  const size_t row = (size_t)W.n * kNbrChunk * 4;  // bytes of one chunk row of the n particles
-  const size_t pitch = (size_t)c->capacity * kNbrChunk * 4, dpitch = (size_t)W.cap * kNbrChunk * 4;
-  if (W.n > 0)
-    CK(cudaMemcpy2DAsync(sl.end.nbr, dpitch, c->nbr, pitch, row, kMaxNbr / kNbrChunk, cudaMemcpyDeviceToDevice,
-                         c->stream));
-  CK(cudaMemcpyAsync(sl.end.cell_begin, c->cell_begin, (size_t)(c->P.num_cells + 1) * 4, cudaMemcpyDeviceToDevice,
-                     c->stream));
-  CK(cudaMemcpyAsync(sl.end.dyn, c->dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, c->stream));
-}
-
-// The arrays of a recomputed step (slot) through View, as the reverse
-// kernels read them; the list chunk stride is the capacity the slot was
-// sized by.
-View slot_view(const AdjWindow& W, const AdjWindow::Slot& sl) {
-  View V{};
-  const AdjSlot& e = sl.end;
-  V.xp = e.xp;
-  V.vT = e.vT;
-  V.vt = e.vt;
-  V.nrm = e.nrm;
-  V.mrps = e.mrps;
-  V.a4 = e.a4;
-  V.vwp = e.vwp;
-  V.heat_w = e.heat_w;
-  V.cell_begin = e.cell_begin;
-  V.dyn = e.dyn;
-  V.capacity = W.cap;
-  V.nbr = e.nbr;
-  V.nbr_cnt = e.nbr_cnt;
-  V.fluid_idx = e.fluid_idx;
-  V.wall_idx = e.wall_idx;
-  return V;
-}
-
-void adj_reverse_step(cryo_ctx* c, AdjWindow& W, long long k, const AdjWindow::Slot& sl) {
-  const Params& P = c->P;
-  Adj A{};
-  A.V = slot_view(W, sl);
-  A.vT1 = sl.tape.vT1;
-  A.m1 = sl.tape.m1;
-  A.ns1 = sl.tape.ns1;
-  A.pc2 = sl.tape.pc2;
-  A.vT2 = sl.tape.vT2;
-  A.m2 = sl.tape.m2;
-  A.dyn1 = sl.tape.dyn1;
-  A.sums = sl.tape.sums;
-  A.sums_n = sl.tape.n;
-  A.gX = W.cX[W.q];
-  A.gV = W.cV[W.q];
-  A.gA = W.cA[W.q];
-  A.gB = W.cB[W.q];
-  A.prevX = W.cX[1 - W.q];
-  A.prevV = W.cV[1 - W.q];
-  A.prevA = W.cA[1 - W.q];
-  A.prevB = W.cB[1 - W.q];
-  A.gP = W.gP;
-  A.gN = W.gN;
-  A.gG = W.gG;
-  A.gC = W.gC;
-  A.gU1 = W.gU1;
-  A.gU2 = W.gU2;
-  A.gU3 = W.gU3;
-  A.R1 = W.R1;
-  A.R2 = W.R2;
-  A.argmax = W.argmax;
-  A.perm = sl.end.perm;
-  A.glob = W.glob;
-  A.partials = W.partials;
-  A.ticket = W.ticket;
-  A.max_chunks = W.max_chunks;
-  A.status = W.status;
-  const size_t n16 = (size_t)W.n * 16;
-  for (float4* a : {W.gP, W.gN, W.gG, W.gC, W.gU1, W.gU2, W.gU3}) CK(cudaMemsetAsync(a, 0, n16, c->stream));
-  const int G = c->grid_blocks();
-  const int GF = std::max(1, std::min((W.n + 127) / 128, c->sm_count * 16));
-  ALAUNCH(c, k_adj_saturation_sums, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_rebalance_local, G, kBlock, P, A);
-  if (P.cfg_phase_change) {
-    ALAUNCH(c, k_adj_rebalance_gather, G, kBlock, P, A);
-    ALAUNCH(c, k_adj_apply_local, G, kBlock, P, A);
-    ALAUNCH(c, k_adj_apply_gather, G, kBlock, P, A);
-    ALAUNCH(c, k_adj_normalize_local, G, kBlock, P, A);
-    ALAUNCH(c, k_adj_normalize_gather, G, kBlock, P, A);
-  }
-  ALAUNCH(c, k_adj_kick_sources, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_forces_local, G, kBlock, P, A);
-  {
-    // heater-norm and gravity adjoints of this step (set), sigma and heater (summed)
-    const AdjRows M{6, {AR_FORCE, AR_FORCE + 1, AR_FORCE + 2, AR_FORCE + 3, AR_FORCE + 4, AR_FORCE + 5},
-                    {AG_HINV, AG_GRAV, AG_GRAV + 1, AG_GRAV + 2, AG_SIGMA, AG_HEAT}, {0, 0, 0, 0, 1, 1}};
-    ALAUNCH(c, k_adj_reduce, M.count, kBlock, A, M);
-  }
-  ALAUNCH(c, k_adj_forces_gather, GF, 128, P, A);
-  ALAUNCH(c, k_adj_interface_local, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_interface_gather, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_wall_local, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_wall_gather, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_density_gather, G, kBlock, P, A);
-  {
-    // T_sat adjoint of this step's input (set); Lee, contact angle (summed); wall part of gravity (added)
-    const AdjRows M{8,
-                    {AR_SRC, AR_SRC + 1, AR_SRC + 2, AR_IFACE, AR_IFACE + 1, AR_WALL, AR_WALL + 1, AR_WALL + 2},
-                    {AG_TSAT_IN, AG_LEE_E, AG_LEE_C, AG_COS, AG_SIN, AG_GRAV, AG_GRAV + 1, AG_GRAV + 2},
-                    {0, 1, 1, 1, 1, 1, 1, 1}};
-    ALAUNCH(c, k_adj_reduce, M.count, kBlock, A, M);
-  }
-  ALAUNCH(c, k_adj_drift_scatter, G, kBlock, P, A);
-  ALAUNCH(c, k_adj_step_end, 1, 32, W.glob, W.ggrav + 3 * k);
-  W.q = 1 - W.q;
-}
-
-AdjWindow& adj_window(cryo_ctx* c) {
-  if (!c->adj || !c->adj->recorded) throw std::runtime_error("adjoint: no recorded window (call cryo_adj_forward)");
-  return *c->adj;
-}
-
-}  // namespace
-
-extern "C" {
-
-int cryo_set_surface_tension(cryo_ctx* c, float sigma) {
-  return guard(c, [&] {
-    if (!(sigma >= 0)) throw std::invalid_argument("surface tension must be >= 0");
-    c->sync();
-    c->fluid.sigma = sigma;
-    c->P.sigma = c->cfg.surface_tension != CRYO_ST_NONE ? sigma : 0.0f;
-    c->invalidate_graphs();
-  });
-}
-
-int cryo_set_lee_coefficients(cryo_ctx* c, float evaporation, float condensation) {
-  return guard(c, [&] {
-    if (!(evaporation >= 0 && condensation >= 0)) throw std::invalid_argument("Lee coefficients must be >= 0");
-    c->sync();
-    c->cfg.lee_evaporation = evaporation;
-    c->cfg.lee_condensation = condensation;
-    c->P.lee_evap = evaporation;
-    c->P.lee_cond = condensation;
-    c->invalidate_graphs();
-  });
-}
-
-int cryo_adj_forward(cryo_ctx* c, long long steps, int every, double* objectives) {
-  return guard(c, [&] {
-    if (steps < 1) throw std::invalid_argument("adjoint: steps must be >= 1");
-    if (every < 1) throw std::invalid_argument("adjoint: checkpoint interval must be >= 1");
-    adj_check_config(c);
-    c->ensure_initialized();
-    c->pull();
-    if (!c->adj) c->adj = new AdjWindow;
-    AdjWindow& W = *c->adj;
-    W.recorded = false;
-    W.n = c->hdyn->n;
-    W.cap = c->capacity;
-    W.splits0 = c->hdyn->splits;
-    W.merges0 = c->hdyn->merges;
-    adj_alloc(c, W, steps, every);
-    CK(cudaMemsetAsync(W.obj, 0, 8 * 8, c->stream));
-    for (long long k = 0; k < steps; ++k) {
-      if (k % every == 0) snap_save(c, W, W.ckpt[(size_t)(k / every)]);
-      c->launch_step();
-      const View V = c->view(c->cur);
-      ALAUNCH(c, k_adj_objective, c->grid_blocks(), kBlock, c->P, V, c->reduce(), W.obj);
-    }
-    snap_save(c, W, W.ckpt.back());
-    double obj[6];
-    CK(cudaMemcpyAsync(obj, W.obj, sizeof(obj), cudaMemcpyDeviceToHost, c->stream));
-    c->pull();
-    if (c->hdyn->n != W.n || c->hdyn->splits != W.splits0 || c->hdyn->merges != W.merges0)
-      throw std::runtime_error("adjoint: particles split, merged or died inside the window (topology must stay fixed)");
-    for (int k = 0; k < 6; ++k) objectives[k] = obj[k];
-    objectives[6] = c->hdyn->p_ullage;
-    for (auto& v : W.seed) v.clear();
-    W.recorded = true;
-  });
-}
-
-// Seeds of the final state's adjoint (tests): which 0 x, 1 v, 2 T, 3 m, 4 a,
-// 5 ab; 3 or 1 floats per particle in the window's final order.
-int cryo_adj_seed_state(cryo_ctx* c, int which, const float* data, size_t count) {
-  return guard(c, [&] {
-    AdjWindow& W = adj_window(c);
-    if (which < 0 || which > 5) throw std::invalid_argument("adjoint: unknown state field");
-    const int comps = (which == 2 || which == 3) ? 1 : 3;
-    if (count != (size_t)W.n * comps) throw std::invalid_argument("adjoint: seed size mismatch");
-    const int slot = which == 0 || which == 3 ? 0 : (which == 1 || which == 2 ? 1 : which - 2);
-    std::vector<float4>& s = W.seed[slot];
-    if (s.empty()) s.assign((size_t)W.n, make_float4(0, 0, 0, 0));
-    for (int i = 0; i < W.n; ++i) {
-      if (comps == 3) {
-        s[i].x = data[3 * i];
-        s[i].y = data[3 * i + 1];
-        s[i].z = data[3 * i + 2];
-      } else {
-        s[i].w = data[i];
-      }
-    }
-  });
-}
-
-int cryo_adj_backward(cryo_ctx* c, const double* seed, double* grads, double* frame_grads) {
-  return guard(c, [&] {
-    AdjWindow& W = adj_window(c);
-    double g[AG_COUNT] = {0};
-    for (int k = 0; k < 3; ++k) {
-      g[AG_FW + k] = seed[k];
-      g[AG_MW + k] = seed[3 + k];
-    }
-    g[AG_P_OBJ] = seed[6];
-    CK(cudaMemcpyAsync(W.glob, g, sizeof(g), cudaMemcpyHostToDevice, c->stream));
-    const size_t n16 = (size_t)W.n * 16;
-    for (int k = 0; k < 2; ++k)
-      for (float4* a : {W.cX[k], W.cV[k], W.cA[k], W.cB[k]}) CK(cudaMemsetAsync(a, 0, n16, c->stream));
-    W.q = 0;
-    float4* dst[4] = {W.cX[0], W.cV[0], W.cA[0], W.cB[0]};
-    for (int k = 0; k < 4; ++k)
-      if (!W.seed[k].empty()) CK(cudaMemcpyAsync(dst[k], W.seed[k].data(), n16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemsetAsync(W.status, 0, 4, c->stream));
-    c->sync();  // the pageable sources above are free again
-    const long long nseg = (W.steps + W.every - 1) / W.every;
-    for (long long sg = nseg - 1; sg >= 0; --sg) {
-      const long long k0 = sg * W.every, k1 = std::min(W.steps, k0 + W.every);
-      // recompute the segment once, keeping what each step's reverse reads
-      snap_load(c, W, W.ckpt[(size_t)sg]);
-      for (long long k = k0; k < k1; ++k) {
-        AdjWindow::Slot& sl = W.slots[(size_t)(k - k0)];
-        const int s = c->cur;
-        c->enqueue_step(s, &sl.tape);
-        c->cur = 1 - s;
-        adj_snap_end(c, W, sl);
-      }
-      for (long long k = k1 - 1; k >= k0; --k) adj_reverse_step(c, W, k, W.slots[(size_t)(k - k0)]);
-    }
-    snap_load(c, W, W.ckpt.back());
-    unsigned status = 0;
-    std::vector<double> gg((size_t)W.steps * 3);
-    CK(cudaMemcpyAsync(g, W.glob, sizeof(g), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(&status, W.status, 4, cudaMemcpyDeviceToHost, c->stream));
-    if (frame_grads) CK(cudaMemcpyAsync(gg.data(), W.ggrav, gg.size() * 8, cudaMemcpyDeviceToHost, c->stream));
-    c->pull();
-    if (status & ADJ_TOPOLOGY) throw std::runtime_error("adjoint: a particle died inside the window");
-    const double deg = (double)kPi / 180.0;
-    grads[0] = g[AG_SIGMA];
-    grads[1] = (-(double)c->P.sin_theta * g[AG_COS] + (double)c->P.cos_theta * g[AG_SIN]) * deg;
-    grads[2] = g[AG_LEE_E];
-    grads[3] = g[AG_LEE_C];
-    grads[4] = g[AG_HEAT];
-    if (frame_grads)
-      for (size_t k = 0; k < gg.size(); ++k) frame_grads[k] = -gg[k];  // gravity = g - a_frame
-  });
-}
-
-// Adjoint of the window's initial state (after cryo_adj_backward): which as
-// in cryo_adj_seed_state, in the order of the state the window started from.
-int cryo_adj_state_gradient(cryo_ctx* c, int which, float* out, size_t count) {
-  return guard(c, [&] {
-    AdjWindow& W = adj_window(c);
-    if (which < 0 || which > 5) throw std::invalid_argument("adjoint: unknown state field");
-    const int comps = (which == 2 || which == 3) ? 1 : 3;
-    if (count != (size_t)W.n * comps) throw std::invalid_argument("adjoint: output size mismatch");
-    const float4* src[6] = {W.cX[W.q], W.cV[W.q], W.cV[W.q], W.cX[W.q], W.cA[W.q], W.cB[W.q]};
-    std::vector<float4> h((size_t)W.n);
-    CK(cudaMemcpyAsync(h.data(), src[which], (size_t)W.n * 16, cudaMemcpyDeviceToHost, c->stream));
-    c->sync();
-    for (int i = 0; i < W.n; ++i) {
-      if (comps == 3) {
-        out[3 * i] = h[i].x;
-        out[3 * i + 1] = h[i].y;
-        out[3 * i + 2] = h[i].z;
-      } else {
-        out[i] = h[i].w;
-      }
-    }
-  });
-}
-
-int cryo_adj_memory(cryo_ctx* c, size_t* bytes) {
-  return guard(c, [&] { *bytes = c->adj ? c->adj->bytes : 0; });
-}
-
-int cryo_adj_release(cryo_ctx* c) {
-  return guard(c, [&] {
-    c->sync();
-    adj_free(c->adj);
-    c->adj = nullptr;
-  });
-}
-
-}  // extern "C"
-
-// ===========================================================================
-// Slab decomposition of one tank (no counterpart in the reference; the device
-// side and the ownership rules are in cryo_slab.cu).  Each slab is a context
-// on its own device (or several on one device).  One host thread per slab
-// enqueues that slab's step; the threads meet at every SlabPoint (a host
-// barrier), so each slab's stream can wait on its neighbours' events before
-// it reads their memory, and they wait on its events before they overwrite
-// what it read.  No kernel waits on another slab's kernel.
-namespace {
-
-class HostBarrier {
- public:
-  explicit HostBarrier(int n) : count_(n) {}
-  // Blocks until every thread arrived; throws when another thread gave up.
-  void wait() {
-    std::unique_lock<std::mutex> lk(m_);
-    if (broken_) throw std::runtime_error("slabs: another slab failed");
-    const unsigned g = gen_;
-    if (++waiting_ == count_) {
-      waiting_ = 0;
-      ++gen_;
-      cv_.notify_all();
-      return;
-    }
-    cv_.wait(lk, [&] { return gen_ != g || broken_; });
-    if (gen_ == g) throw std::runtime_error("slabs: another slab failed");
-  }
-  void fail() {
-    std::lock_guard<std::mutex> lk(m_);
-    broken_ = true;
-    cv_.notify_all();
-  }
-  void reset() {
-    std::lock_guard<std::mutex> lk(m_);
-    broken_ = false;
-    waiting_ = 0;
-  }
-
- private:
-  std::mutex m_;
-  std::condition_variable cv_;
-  int count_, waiting_ = 0;
-  unsigned gen_ = 0;
-  bool broken_ = false;
-};
-
-}  // namespace
-
-struct SlabGroup {
-  // Neighbour layers copied in between steps.  A particle moves far less
-  // than a layer (2h) per step, so the ghost layer next to a slab after the
-  // drift holds only particles that were in the two layers before it.
-  static constexpr int kRefreshLayers = 2;
-  std::vector<cryo_ctx*> slabs;
-  std::vector<int> zb;          // slab r owns cell layers [zb[r], zb[r + 1])
-  std::vector<View> live;       // each slab's live arrays at the current point
-  std::vector<cudaEvent_t> ev_a, ev_b;
-  std::vector<DynState**> dyn_table;  // per slab, on its device: every slab's scalar block
-  std::vector<float4*> spare;         // per slab: a4 / ab4 of a refresh (2 x capacity)
-  std::vector<int> spare_cap;
-  HostBarrier barrier;
-
-  explicit SlabGroup(int n) : barrier(n) {}
-  int count() const { return (int)slabs.size(); }
-
-  // A pass's outputs are complete on every slab: pull the ghost layers next
-  // to this slab from their owners, then combine what `what` needs.
-  void point(int r, int what, int set) {
-    cryo_ctx* c = slabs[r];
-    if (what == SLAB_SORTED) {
-      k_slab_bounds<<<1, 1, 0, c->stream>>>(c->P, c->view(set), zb[r], zb[r + 1]);
-      CK(cudaGetLastError());
-      return;
-    }
-    const int R = count();
-    const bool every = what != SLAB_HALO;  // the combines read every slab
-    live[r] = c->view(set);
-    CK(cudaEventRecord(ev_a[r], c->stream));
-    barrier.wait();
-    for (int q = 0; q < R; ++q)
-      if (q != r && (every || q == r - 1 || q == r + 1)) CK(cudaStreamWaitEvent(c->stream, ev_a[q], 0));
-    if (what == SLAB_HALO || what == SLAB_HEAT || what == SLAB_FORCES) {
-      const int G = std::max(1, c->sm_count * 2);
-      if (r > 0) k_halo_pull<<<G, kBlock, 0, c->stream>>>(c->P, live[r], live[r - 1], zb[r] - 1);
-      if (r + 1 < R) k_halo_pull<<<G, kBlock, 0, c->stream>>>(c->P, live[r], live[r + 1], zb[r + 1]);
-    }
-    if (what == SLAB_HEAT) k_slab_heat<<<1, 1, 0, c->stream>>>(c->P, dyn_table[r], R, c->dyn, 1);
-    if (what == SLAB_SPLIT) k_slab_split<<<1, 1, 0, c->stream>>>(dyn_table[r], R, r, c->dyn);
-    if (what == SLAB_FORCES) k_slab_end<<<1, 1, 0, c->stream>>>(c->P, dyn_table[r], R, c->dyn, 0);
-    if (what == SLAB_END) k_slab_end<<<1, 1, 0, c->stream>>>(c->P, dyn_table[r], R, c->dyn, 1);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ev_b[r], c->stream));
-    barrier.wait();
-    for (int q = 0; q < R; ++q)
-      if (q != r && (every || q == r - 1 || q == r + 1)) CK(cudaStreamWaitEvent(c->stream, ev_b[q], 0));
-  }
-
-  // Between steps: rebuild this slab's arrays from its owned particles and
-  // the layers of its neighbours that face it (cryo_slab.cu, k_slab_assemble).
-  void refresh(int r) {
-    cryo_ctx* c = slabs[r];
-    const int R = count();
-    live[r] = c->view(c->cur);
-    CK(cudaEventRecord(ev_a[r], c->stream));
-    barrier.wait();
-    if (r > 0) CK(cudaStreamWaitEvent(c->stream, ev_a[r - 1], 0));
-    if (r + 1 < R) CK(cudaStreamWaitEvent(c->stream, ev_a[r + 1], 0));
-    const View dst = c->view(1 - c->cur);
-    const View& lo = r > 0 ? live[r - 1] : live[r];
-    const View& up = r + 1 < R ? live[r + 1] : live[r];
-    float4* a4 = spare[r];
-    float4* ab4 = spare[r] + spare_cap[r];
-    const int G = c->grid_blocks();
-    k_slab_assemble<<<G, kBlock, 0, c->stream>>>(c->P, dst, a4, ab4, lo, live[r], up, r > 0 ? 1 : 0,
-                                                  r + 1 < R ? 1 : 0, zb[r], zb[r + 1], kRefreshLayers);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ev_b[r], c->stream));
-    barrier.wait();
-    if (r > 0) CK(cudaStreamWaitEvent(c->stream, ev_b[r - 1], 0));
-    if (r + 1 < R) CK(cudaStreamWaitEvent(c->stream, ev_b[r + 1], 0));
-    k_slab_commit<<<G, kBlock, 0, c->stream>>>(dst, a4, ab4);
-    CK(cudaGetLastError());
-    c->cur = 1 - c->cur;
-  }
-
-  // Runs body(r) for every slab in its own thread; the first failure is
-  // rethrown after every thread has ended.
-  template <class F>
-  void lockstep(F&& body) {
-    barrier.reset();
-    const int R = count();
-    std::vector<std::exception_ptr> errs(R);
-    std::vector<std::thread> th;
-    th.reserve(R);
-    for (int r = 0; r < R; ++r)
-      th.emplace_back([&, r] {
-        try {
-          CK(cudaSetDevice(slabs[r]->device));
-          body(r);
-        } catch (...) {
-          errs[r] = std::current_exception();
-          barrier.fail();
-        }
-      });
-    for (auto& t : th) t.join();
-    for (cryo_ctx* c : slabs) cudaStreamSynchronize(c->stream);
-    // a real error first, not another thread's "another slab failed"
-    for (int pass = 0; pass < 2; ++pass)
-      for (int r = 0; r < R; ++r) {
-        if (!errs[r]) continue;
-        try {
-          std::rethrow_exception(errs[r]);
-        } catch (const std::runtime_error& e) {
-          if (pass == 0 && std::string(e.what()).rfind("slabs: another slab failed", 0) == 0) continue;
-          throw;
-        }
-      }
-  }
-
-  // Guard words, capacity head-room and spare arrays between step batches.
-  void check() {
-    unsigned bad = 0;
-    for (cryo_ctx* c : slabs) {
-      CK(cudaSetDevice(c->device));
-      c->pull();
-      bad |= c->hdyn->status & (CRYO_DEV_SLAB_HALO | CRYO_DEV_SLAB_CAPACITY);
-    }
-    if (bad & CRYO_DEV_SLAB_HALO)
-      throw std::runtime_error("slabs: a slab and its neighbour hold different ghost layers (a particle moved "
-                               "more than a cell layer in one step?)");
-    if (bad & CRYO_DEV_SLAB_CAPACITY) throw std::runtime_error("slabs: a refreshed slab did not fit its capacity");
-    for (int r = 0; r < count(); ++r) {
-      cryo_ctx* c = slabs[r];
-      CK(cudaSetDevice(c->device));
-      c->check_capacity();
-      if (spare_cap[r] < c->capacity) alloc_spare(r);
-    }
-  }
-  void alloc_spare(int r) {
-    cryo_ctx* c = slabs[r];
-    CK(cudaSetDevice(c->device));
-    if (spare[r]) CK(cudaFree(spare[r]));
-    spare[r] = nullptr;
-    CK(cudaMalloc(&spare[r], (size_t)2 * c->capacity * sizeof(float4)));
-    spare_cap[r] = c->capacity;
-  }
-
-  void initialize() {
-    bool need = false;
-    for (cryo_ctx* c : slabs) need |= !c->initialized;
-    if (!need) return;
-    lockstep([&](int r) { slabs[r]->ensure_initialized(); });
-    check();
-  }
-
-  void run(long long n) {
-    initialize();
-    while (n > 0) {
-      const int k = (int)std::min<long long>(n, 16);
-      lockstep([&](int r) {
-        for (int q = 0; q < k; ++q) {
-          refresh(r);
-          slabs[r]->launch_step();
-        }
-      });
-      check();
-      n -= k;
-    }
-  }
-
-  ~SlabGroup() {  // also after a failed create: slabs not made yet are null
-    for (cryo_ctx* c : slabs)
-      if (c && c->stream) cudaStreamSynchronize(c->stream);
-    for (size_t r = 0; r < slabs.size(); ++r) {
-      if (r < spare.size() && spare[r]) cudaFree(spare[r]);
-      if (r < dyn_table.size() && dyn_table[r]) cudaFree(dyn_table[r]);
-      if (r < ev_a.size() && ev_a[r]) cudaEventDestroy(ev_a[r]);
-      if (r < ev_b.size() && ev_b[r]) cudaEventDestroy(ev_b[r]);
-    }
-    for (cryo_ctx* c : slabs) delete c;
-  }
-};
-
-void cryo_ctx::slab_point(int what, int set) {
-  if (slab_group) slab_group->point(slab_rank, what, set);
-}
-
-struct cryo_slabs {
-  SlabGroup* g = nullptr;
-  std::string err;
-  ~cryo_slabs() { delete g; }
-};
-
-namespace {
-
-template <class F>
-int slab_guard(cryo_slabs* s, F&& f) {
-  try {
-    f();
-    return CRYO_OK;
-  } catch (const std::invalid_argument& e) {
-    s->err = e.what();
-    return CRYO_EINVAL;
-  } catch (const std::out_of_range& e) {
-    s->err = e.what();
-    return CRYO_ERANGE;
-  } catch (const CudaError& e) {
-    s->err = e.what();
-    return CRYO_ECUDA;
-  } catch (const std::exception& e) {
-    s->err = e.what();
-    return CRYO_ERUNTIME;
-  }
-}
-
-// Cell layer of a position, with the device's cell_coords operations.
-int host_layer(const Params& P, float z) {
-  const float f = std::floor((z - P.oz) * P.inv_cell);
-  const int cz = (f >= 2147483648.0f || f < -2147483648.0f || f != f) ? std::numeric_limits<int>::min() : (int)f;
-  return std::min(std::max(cz, 0), P.nz - 1);
-}
-
-}  // namespace
-
-extern "C" {
-
-// Slab boundaries: layers [z_begin[r], z_begin[r+1]) to slab r, each slab at
-// least min_layers thick, the cuts where the running particle count crosses
-// r / nslabs of the total.
-int cryo_slab_partition(const long long* layer_counts, int nz, int nslabs, int min_layers, int* z_begin) {
-  if (nslabs < 1 || min_layers < 1 || nz < 1 || (long long)nslabs * min_layers > nz || !layer_counts || !z_begin)
-    return CRYO_EINVAL;
-  long long total = 0;
-  for (int z = 0; z < nz; ++z) {
-    if (layer_counts[z] < 0) return CRYO_EINVAL;
-    total += layer_counts[z];
-  }
-  z_begin[0] = 0;
-  z_begin[nslabs] = nz;
-  long long before = 0;  // particles in layers [0, cut)
-  int cut = 0;
-  for (int r = 1; r < nslabs; ++r) {
-    const long long target = (total * r + nslabs / 2) / nslabs;
-    const int lo = z_begin[r - 1] + min_layers;    // the slab before keeps min_layers
-    const int hi = nz - (nslabs - r) * min_layers;  // and so can every slab after
-    while (cut < lo) before += layer_counts[cut++];
-    while (cut < hi && before + layer_counts[cut] <= target) before += layer_counts[cut++];
-    z_begin[r] = cut;
-  }
-  return CRYO_OK;
-}
-
-int cryo_slabs_create(const cryo_config_t* cfg, const cryo_fluid_t* fluid, int nslabs, const int* devices,
-                      cryo_slabs** out) {
-  *out = nullptr;
-  if (nslabs < 1) {
-    g_create_error = "slabs: need at least one slab";
-    return CRYO_EINVAL;
-  }
-  cryo_slabs* S = new cryo_slabs;
-  const int rc = slab_guard(S, [&] {
-    S->g = new SlabGroup(nslabs);
-    SlabGroup& G = *S->g;
-    G.slabs.assign(nslabs, nullptr);
-    G.live.resize(nslabs);
-    G.ev_a.assign(nslabs, nullptr);
-    G.ev_b.assign(nslabs, nullptr);
-    G.dyn_table.assign(nslabs, nullptr);
-    G.spare.assign(nslabs, nullptr);
-    G.spare_cap.assign(nslabs, 0);
-    for (int r = 0; r < nslabs; ++r) {
-      const int dev = devices ? devices[r] : 0;
-      cryo_ctx* c = nullptr;
-      if (cryo_create(cfg, fluid, dev, &c) != CRYO_OK) throw std::invalid_argument(g_create_error);
-      G.slabs[r] = c;
-      c->slab_group = &G;
-      c->slab_rank = r;
-      c->graph_mode = false;  // the slabs' steps meet on the host between passes
-      CK(cudaEventCreateWithFlags(&G.ev_a[r], cudaEventDisableTiming));
-      CK(cudaEventCreateWithFlags(&G.ev_b[r], cudaEventDisableTiming));
-    }
-    // neighbours on other devices read each other's memory
-    for (int r = 0; r + 1 < nslabs; ++r) {
-      const int a = G.slabs[r]->device, b = G.slabs[r + 1]->device;
-      if (a == b) continue;
-      for (const auto& pr : {std::make_pair(a, b), std::make_pair(b, a)}) {
-        int can = 0;
-        CK(cudaDeviceCanAccessPeer(&can, pr.first, pr.second));
-        if (!can) throw std::runtime_error("slabs: devices " + std::to_string(pr.first) + " and " +
-                                           std::to_string(pr.second) + " cannot reach each other's memory");
-        CK(cudaSetDevice(pr.first));
-        const cudaError_t e = cudaDeviceEnablePeerAccess(pr.second, 0);
-        if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
-        else CK(e);
-      }
-    }
-    std::vector<DynState*> table(nslabs);
-    for (int r = 0; r < nslabs; ++r) table[r] = G.slabs[r]->dyn;
-    for (int r = 0; r < nslabs; ++r) {
-      CK(cudaSetDevice(G.slabs[r]->device));
-      CK(cudaMalloc(&G.dyn_table[r], nslabs * sizeof(DynState*)));
-      CK(cudaMemcpy(G.dyn_table[r], table.data(), nslabs * sizeof(DynState*), cudaMemcpyHostToDevice));
-    }
-  });
-  if (rc != CRYO_OK) {
-    g_create_error = S->err;
-    delete S;
-    return rc;
-  }
-  *out = S;
-  return CRYO_OK;
-}
-
-void cryo_slabs_destroy(cryo_slabs* s) { delete s; }
-
-const char* cryo_slabs_last_error(const cryo_slabs* s) { return s ? s->err.c_str() : g_create_error.c_str(); }
-
-int cryo_slabs_count(cryo_slabs* s, int* nslabs) {
-  return slab_guard(s, [&] { *nslabs = s->g->count(); });
-}
-
-// Solver::set_particles of the whole tank (sph_solver.cu:407-428), cut into
-// the slabs: slab r receives, in input order, the particles of its layers and
-// of kRefreshLayers layers on either side.
-int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, const float* lo, const float* hi) {
-  return slab_guard(s, [&] {
-    SlabGroup& G = *s->g;
-    const int n = p->n;
-    if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
-    bool vap = false;
-    for (int i = 0; i < n; ++i) vap |= p->phase[i] == CRYO_VAPOR;
-    uint32_t next_id = 0;
-    for (int i = 0; i < n; ++i) next_id = std::max(next_id, (p->id ? p->id[i] : (uint32_t)i) + 1);
-    const int R = G.count();
-    cryo_ctx* c0 = G.slabs[0];
-    CK(cudaSetDevice(c0->device));
-    c0->begin_load(1, vap, lo, hi);  // the grid the whole tank has
-    const Params P0 = c0->P;
-    std::vector<int> layer(n);
-    std::vector<long long> counts(P0.nz, 0);
-    for (int i = 0; i < n; ++i) {
-      layer[i] = host_layer(P0, p->x[3 * i + 2]);
-      ++counts[layer[i]];
-    }
-    G.zb.assign(R + 1, 0);
-    if (cryo_slab_partition(counts.data(), P0.nz, R, SlabGroup::kRefreshLayers, G.zb.data()) != CRYO_OK)
-      throw std::invalid_argument("slabs: the tank has " + std::to_string(P0.nz) + " cell layers, fewer than " +
-                                  std::to_string(SlabGroup::kRefreshLayers) + " per slab");
-    for (int r = 0; r < R; ++r) {
-      long long own = 0;
-      for (int z = G.zb[r]; z < G.zb[r + 1]; ++z) own += counts[z];
-      if (own == 0) throw std::invalid_argument("slabs: slab " + std::to_string(r) + " would hold no particle");
-    }
-    for (int r = 0; r < R; ++r) {
-      cryo_ctx* c = G.slabs[r];
-      CK(cudaSetDevice(c->device));
-      const int z0 = G.zb[r] - SlabGroup::kRefreshLayers, z1 = G.zb[r + 1] + SlabGroup::kRefreshLayers;
-      std::vector<int> idx;
-      for (int i = 0; i < n; ++i)
-        if (layer[i] >= z0 && layer[i] < z1) idx.push_back(i);
-      const int m = (int)idx.size();
-      c->begin_load(std::max(m, 1), vap, lo, hi);
-      c->P.slab_z0 = G.zb[r];  // the passes run over owned particles only
-      c->P.slab_z1 = G.zb[r + 1];
-      std::vector<float4> xp(m), vT(m), vt(m), nrm(m), mrps(m);
-      std::vector<uint32_t> id(m);
-      for (int k = 0; k < m; ++k) {
-        const int i = idx[k];
-        const float* x = p->x + 3 * i;
-        const float v0 = p->v ? p->v[3 * i] : 0.f, v1 = p->v ? p->v[3 * i + 1] : 0.f, v2 = p->v ? p->v[3 * i + 2] : 0.f;
-        xp[k] = make_float4(x[0], x[1], x[2], pack_pf(p->phase[i], p->flags ? p->flags[i] : 0));
-        vT[k] = make_float4(v0, v1, v2, p->T[i]);
-        vt[k] = make_float4(v0, v1, v2, p->m[i]);
-        nrm[k] = p->nrm ? make_float4(p->nrm[3 * i], p->nrm[3 * i + 1], p->nrm[3 * i + 2], 0.f)
-                        : make_float4(0.f, 0.f, 0.f, 0.f);
-        mrps[k] = make_float4(p->m[i], p->rho[i], 0.f, 0.f);
-        id[k] = p->id ? p->id[i] : (uint32_t)i;
-      }
-      const Persist& st = c->set[0];
-      if (m > 0) {
-        CK(cudaMemcpyAsync(st.xp, xp.data(), (size_t)m * 16, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(st.vT, vT.data(), (size_t)m * 16, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(st.vt, vt.data(), (size_t)m * 16, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(st.nrm, nrm.data(), (size_t)m * 16, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(st.mrps, mrps.data(), (size_t)m * 16, cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(st.id, id.data(), (size_t)m * 4, cudaMemcpyHostToDevice, c->stream));
-      }
-      c->finish_load(m, next_id);
-      G.alloc_spare(r);
-    }
-  });
-}
-
-int cryo_slabs_layout(cryo_slabs* s, int* z_begin, int* owned, int* held) {
-  return slab_guard(s, [&] {
-    SlabGroup& G = *s->g;
-    if (!z_begin) throw std::invalid_argument("cryo_slabs_layout: z_begin is required");
-    if (G.zb.empty()) throw std::runtime_error("slabs: no particles loaded");
-    G.initialize();
-    for (int r = 0; r <= G.count(); ++r) z_begin[r] = G.zb[r];
-    for (int r = 0; r < G.count(); ++r) {
-      cryo_ctx* c = G.slabs[r];
-      CK(cudaSetDevice(c->device));
-      c->pull();
-      const DynState& d = *c->hdyn;
-      if (owned) owned[r] = (d.own_hi - d.own_lo) + (d.n - d.n_sorted);
-      if (held) held[r] = d.n;
-    }
-  });
-}
-
-int cryo_slabs_run_steps(cryo_slabs* s, long long n) {
-  return slab_guard(s, [&] {
-    if (s->g->zb.empty()) throw std::runtime_error("Solver: no particles loaded");
-    s->g->run(n);
-  });
-}
-
-int cryo_slabs_num_particles(cryo_slabs* s, int* n) {
-  return slab_guard(s, [&] {
-    SlabGroup& G = *s->g;
-    if (G.zb.empty()) throw std::runtime_error("Solver: no particles loaded");
-    G.initialize();
-    long long t = 0;
-    for (cryo_ctx* c : G.slabs) {
-      CK(cudaSetDevice(c->device));
-      c->pull();
-      const DynState& d = *c->hdyn;
-      t += (d.own_hi - d.own_lo) + (d.n - d.n_sorted);
-    }
-    *n = (int)t;
-  });
-}
-
-// Solver::particles of the whole tank: every slab's owned sorted range in slab
-// order, then every slab's split children in slab order -- the order the whole
-// tank's own arrays have.
-int cryo_slabs_download(cryo_slabs* s, cryo_host_particles_out_t* o) {
-  return slab_guard(s, [&] {
-    SlabGroup& G = *s->g;
-    if (G.zb.empty()) throw std::runtime_error("Solver: no particles loaded");
-    G.initialize();
-    const int R = G.count();
-    struct Part {
-      std::vector<float> x, v, nrm, m, rho, T;
-      std::vector<uint8_t> phase, flags;
-      std::vector<uint32_t> id;
-      int n, lo, hi, ns;
-    };
-    std::vector<Part> parts(R);
-    long long total = 0;
-    for (int r = 0; r < R; ++r) {
-      cryo_ctx* c = G.slabs[r];
-      CK(cudaSetDevice(c->device));
-      c->pull();
-      Part& q = parts[r];
-      q.n = c->hdyn->n;
-      q.lo = c->hdyn->own_lo;
-      q.hi = c->hdyn->own_hi;
-      q.ns = c->hdyn->n_sorted;
-      q.x.resize(3 * (size_t)q.n); q.v.resize(3 * (size_t)q.n); q.nrm.resize(3 * (size_t)q.n);
-      q.m.resize(q.n); q.rho.resize(q.n); q.T.resize(q.n);
-      q.phase.resize(q.n); q.flags.resize(q.n); q.id.resize(q.n);
-      cryo_host_particles_out_t t{q.n, q.x.data(), q.v.data(), q.nrm.data(), q.m.data(), q.rho.data(),
-                                  q.T.data(), q.phase.data(), q.flags.data(), q.id.data()};
-      if (cryo_download(c, &t) != CRYO_OK) throw std::runtime_error(c->err);
-      total += (q.hi - q.lo) + (q.n - q.ns);
-    }
-    if (o->n < total) {
-      o->n = (int)total;
-      throw std::out_of_range("cryo_slabs_download: arrays too small");
-    }
-    o->n = (int)total;
-    long long k = 0;
-    auto put = [&](const Part& q, int i) {
-      for (int a = 0; a < 3; ++a) {
-        if (o->x) o->x[3 * k + a] = q.x[3 * (size_t)i + a];
-        if (o->v) o->v[3 * k + a] = q.v[3 * (size_t)i + a];
-        if (o->nrm) o->nrm[3 * k + a] = q.nrm[3 * (size_t)i + a];
-      }
-      if (o->m) o->m[k] = q.m[i];
-      if (o->rho) o->rho[k] = q.rho[i];
-      if (o->T) o->T[k] = q.T[i];
-      if (o->phase) o->phase[k] = q.phase[i];
-      if (o->flags) o->flags[k] = q.flags[i];
-      if (o->id) o->id[k] = q.id[i];
-      ++k;
-    };
-    for (const Part& q : parts)
-      for (int i = q.lo; i < q.hi; ++i) put(q, i);
-    for (const Part& q : parts)
-      for (int i = q.ns; i < q.n; ++i) put(q, i);
-  });
-}
-
-// Solver::diagnostics of the whole tank: each slab's owned sums (added in
-// slab order), maxima over the slabs, the shared scalar state of slab 0 and
-// the per-slab counters added up.
-int cryo_slabs_diagnostics(cryo_slabs* s, cryo_diagnostics_t* out) {
-  return slab_guard(s, [&] {
-    SlabGroup& G = *s->g;
-    if (G.zb.empty()) throw std::runtime_error("Solver: no particles loaded");
-    G.initialize();
-    double v[44];
-    long long owned = 0;
-    for (int r = 0; r < G.count(); ++r) {
-      cryo_ctx* c = G.slabs[r];
-      CK(cudaSetDevice(c->device));
-      k_diagnostics<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), c->diag_out);
-      CK(cudaGetLastError());
-      double* h = c->diag_host;
-      CK(cudaMemcpyAsync(h, c->diag_out, 44 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      c->pull();  // also waits for the copy
-      owned += (c->hdyn->own_hi - c->hdyn->own_lo) + (c->hdyn->n - c->hdyn->n_sorted);
-      if (r == 0) {
-        std::memcpy(v, h, sizeof(v));
-        continue;
-      }
-      for (int k = 0; k < 23; ++k) v[k] += h[k];
-      for (int k = 23; k < 25; ++k) v[k] = std::max(v[k], h[k]);
-      for (int k : {30, 31, 32, 33, 36, 37}) v[k] += h[k];
-    }
-    v[28] = (double)owned;
-    diag_fill(v, out);
-  });
-}
 
 }  // extern "C"
