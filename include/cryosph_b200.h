@@ -275,6 +275,26 @@ int cryo_diagnostics(cryo_ctx* ctx, cryo_diagnostics_t* out);
 /* Solver::particles (persistent arrays).  out->n must be >= the particle count;
  * on return out->n holds the count. */
 int cryo_download(cryo_ctx* ctx, cryo_host_particles_out_t* out);
+/* Output frames packed on the device from the current state (no counterpart
+ * as entry points in the reference; they carry what its write_vtk and
+ * make_frame + write_json_frame write, io.cpp:52-142).
+ *
+ * cryo_frame_vtk: the binary payload of the legacy VTK polydata file, every
+ * word big-endian, in file order: POINTS (3 floats per particle), VERTICES
+ * (the int pair 1, i), SCALARS temperature, mass, density, phase, pressure
+ * (1 float each), VECTORS velocity (3 floats): CRYO_VTK_WORDS_PER_PARTICLE
+ * 32-bit words per particle.  `out` (cap bytes) may be null to query the
+ * particle count (*count). */
+#define CRYO_VTK_WORDS_PER_PARTICLE 13
+int cryo_frame_vtk(cryo_ctx* ctx, void* out, size_t cap, int* count);
+/* cryo_frame_viewer: the viewer frame of write_json (TelemetryFrame,
+ * telemetry.hpp:16-25): particles in state order, walls left out unless
+ * include_walls; position (3 floats), temperature, pressure, speed (|v|),
+ * phase.  Each array holds `cap` >= the particle count entries; *count gets
+ * the number written. */
+int cryo_frame_viewer(cryo_ctx* ctx, int include_walls, float* position, float* temperature, float* pressure,
+                      float* speed, uint8_t* phase, int cap, int* count);
+
 /* One per-particle field (CRYO_F_*) into a host buffer of `cap` bytes.
  * Vector fields: 3 floats per particle; phase/flags: uint8; id: uint32. */
 int cryo_get_field(cryo_ctx* ctx, int field, void* host_out, size_t cap);

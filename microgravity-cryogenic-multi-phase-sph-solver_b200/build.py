@@ -25,7 +25,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 CXX = os.environ.get("CXX_HOST", "/usr/bin/g++")
 
 CU_SOURCES = ["cryo_grid.cu", "cryo_physics.cu", "cryo_phase.cu", "cryo_control.cu", "cryo_setup.cu", "cryo_adjoint.cu",
-              "cryo_slab.cu", "cryo_abi.cu", "cryo_ensemble.cu", "cryo_adj_abi.cu", "cryo_slab_abi.cu"]
+              "cryo_slab.cu", "cryo_abi.cu", "cryo_io.cu", "cryo_ensemble.cu", "cryo_adj_abi.cu", "cryo_slab_abi.cu"]
 # -fmad=false: no FMA contraction, so single-precision results follow the
 # reference's IEEE operation sequence (see csrc/cryo_common.cuh).
 NVCC_FLAGS = [

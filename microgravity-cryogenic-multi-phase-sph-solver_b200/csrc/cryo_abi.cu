@@ -712,40 +712,6 @@ void cryo_ctx::finish_load(int n, uint32_t next_id) {
   c->initialized = false;
 }
 
-int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float* lo, const float* hi) {
-  return guard(c, [&] {
-    const int n = p->n;
-    if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
-    bool vap = false;
-    for (int i = 0; i < n; ++i) vap |= p->phase[i] == CRYO_VAPOR;
-    c->begin_load(n, vap, lo, hi);
-    // pack the host arrays into the device layout
-    std::vector<float4> xp(n), vT(n), vt(n), nrm(n), mrps(n);
-    std::vector<uint32_t> id(n);
-    uint32_t next_id = 0;
-    for (int i = 0; i < n; ++i) {
-      const float* x = p->x + 3 * i;
-      const float v0 = p->v ? p->v[3 * i] : 0.f, v1 = p->v ? p->v[3 * i + 1] : 0.f, v2 = p->v ? p->v[3 * i + 2] : 0.f;
-      xp[i] = make_float4(x[0], x[1], x[2], pack_pf(p->phase[i], p->flags ? p->flags[i] : 0));
-      vT[i] = make_float4(v0, v1, v2, p->T[i]);
-      vt[i] = make_float4(v0, v1, v2, p->m[i]);
-      nrm[i] = p->nrm ? make_float4(p->nrm[3 * i], p->nrm[3 * i + 1], p->nrm[3 * i + 2], 0.f)
-                      : make_float4(0.f, 0.f, 0.f, 0.f);
-      mrps[i] = make_float4(p->m[i], p->rho[i], 0.f, 0.f);
-      id[i] = p->id ? p->id[i] : (uint32_t)i;
-      next_id = std::max(next_id, id[i] + 1);
-    }
-    const Persist& s = c->set[0];
-    CK(cudaMemcpyAsync(s.xp, xp.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(s.vT, vT.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(s.vt, vt.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(s.nrm, nrm.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(s.mrps, mrps.data(), n * 16, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(s.id, id.data(), n * 4, cudaMemcpyHostToDevice, c->stream));
-    c->finish_load(n, next_id);
-  });
-}
-
 // Solver::build_tank with the lattice generated on the device (see
 // cryo_setup.cu).  The lattice range, the liquid cut and the particle
 // constants follow build_tank_particles (geometry.cpp:242-330) operation for
@@ -1154,39 +1120,6 @@ int cryo_set_field(cryo_ctx* c, int field, const void* in, size_t bytes) {
   });
 }
 
-// Solver::particles (particle_system.cpp:95-101)
-int cryo_download(cryo_ctx* c, cryo_host_particles_out_t* o) {
-  return guard(c, [&] {
-    c->pull();
-    const int n = c->has_particles ? c->hdyn->n : 0;
-    if (o->n < n) {
-      o->n = n;
-      throw std::out_of_range("cryo_download: arrays too small");
-    }
-    o->n = n;
-    if (n == 0) return;
-    const Persist& s = c->set[c->cur];
-    std::vector<float4> xp(n), vT(n), nrm(n), mrps(n);
-    CK(cudaMemcpyAsync(xp.data(), s.xp, n * 16, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(vT.data(), s.vT, n * 16, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(nrm.data(), s.nrm, n * 16, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaMemcpyAsync(mrps.data(), s.mrps, n * 16, cudaMemcpyDeviceToHost, c->stream));
-    if (o->id) CK(cudaMemcpyAsync(o->id, s.id, n * 4, cudaMemcpyDeviceToHost, c->stream));
-    c->sync();
-    for (int i = 0; i < n; ++i) {
-      if (o->x) { o->x[3 * i] = xp[i].x; o->x[3 * i + 1] = xp[i].y; o->x[3 * i + 2] = xp[i].z; }
-      if (o->v) { o->v[3 * i] = vT[i].x; o->v[3 * i + 1] = vT[i].y; o->v[3 * i + 2] = vT[i].z; }
-      if (o->nrm) { o->nrm[3 * i] = nrm[i].x; o->nrm[3 * i + 1] = nrm[i].y; o->nrm[3 * i + 2] = nrm[i].z; }
-      if (o->m) o->m[i] = mrps[i].x;
-      if (o->rho) o->rho[i] = mrps[i].y;
-      if (o->T) o->T[i] = vT[i].w;
-      int bits;
-      std::memcpy(&bits, &xp[i].w, 4);
-      if (o->phase) o->phase[i] = (uint8_t)(bits & 0xff);
-      if (o->flags) o->flags[i] = (uint8_t)((bits >> 8) & 0xff);
-    }
-  });
-}
 
 // Solver::set_gravity (sph_solver.cu:655-658)
 int cryo_set_gravity(cryo_ctx* c, const float* g) {

@@ -228,6 +228,13 @@ struct cryo_ctx {
   long long tele_step = 0;
   int tele_n = 0;
 
+  // host <-> device particle transfers and output frames (cryo_io.cu): a
+  // device and a pinned host buffer of the same size, grown on demand
+  char* io_dev = nullptr;
+  char* io_host = nullptr;
+  size_t io_cap = 0;
+  void io_reserve(size_t bytes);
+
   // differentiated window (cryo_adj_*), and the sums tape of the step being
   // recomputed for it (View::tape; null otherwise)
   AdjWindow* adj = nullptr;
@@ -300,6 +307,11 @@ struct cryo_ctx {
     }
     if (ens_ev) cudaEventDestroy(ens_ev);
     telemetry_release();
+    if (io_dev || io_host) {
+      if (stream) cudaStreamSynchronize(stream);
+      if (io_dev) cudaFree(io_dev);
+      if (io_host) cudaFreeHost(io_host);
+    }
     for (cudaEvent_t e : event_pool) cudaEventDestroy(e);
     for (int k = 0; k < 2; ++k)
       if (graph[k]) cudaGraphExecDestroy(graph[k]);

@@ -2,24 +2,21 @@
 // (build_tank_particles, geometry.cpp:242-330): signed distances of the tank
 // geometry at every lattice node, ordered compaction of wall and fluid nodes,
 // the liquid/vapour split at an order statistic of the fill key, and the
-// particles written into the solver's arrays.  The signed distances are the
-// host generator's double-precision operations in the same order (std::max,
-// std::min and std::clamp restated with their tie rules), so the particles
-// are identical to the host's.
+// particles written into the solver's arrays.  The signed distances come from
+// cryo_sdf.h, which the host generator evaluates too, so the particles are
+// identical to the host's.
 #include "cryo_kernels.cuh"
+#include "cryo_sdf.h"
 
 namespace cryo {
 
 namespace {
 
-__device__ inline double mx(double a, double b) { return (a < b) ? b : a; }  // std::max
-__device__ inline double mn(double a, double b) { return (b < a) ? b : a; }  // std::min
-__device__ inline double clampd(double v, double lo, double hi) { return (v < lo) ? lo : (hi < v) ? hi : v; }
-
-// Geometry::sdf of the node tree (CylinderTank, CapsuleTank, SphereTank,
-// BoxTank, Translated, Difference, Union of geometry.cpp).  Nodes come
-// children first; a primitive is evaluated at the query point shifted by the
-// offsets of its Translated ancestors, root first, as the nested calls do.
+// Geometry::sdf of the node tree (the analytic shapes and their CSG).  Nodes
+// come children first; a primitive is evaluated at the query point shifted
+// by the offsets of its Translated ancestors, root first, as nested calls to
+// the host classes shift it.  The primitives are cryo_sdf.h's, which the host
+// classes evaluate too.
 __device__ double geom_sdf(const GeomNode* __restrict__ G, int ng, double x, double y, double z) {
   double val[kGeomNodes];
   for (int k = 0; k < ng; ++k) {
@@ -33,33 +30,17 @@ __device__ double geom_sdf(const GeomNode* __restrict__ G, int ng, double x, dou
         qz = qz - g.ofs[f][2];
       }
       switch (g.kind) {
-        case CRYO_GEOM_CYLINDER: {
-          const double qr = sqrt(qx * qx + qy * qy) - g.p[0];
-          const double qh = fabs(qz) - 0.5 * g.p[1];
-          const double er = mx(qr, 0.0), ez = mx(qh, 0.0);
-          v = mn(mx(qr, qh), 0.0) + sqrt(er * er + ez * ez);
-          break;
-        }
-        case CRYO_GEOM_CAPSULE: {
-          const double hz = 0.5 * g.p[1];
-          const double dz = qz - clampd(qz, -hz, hz);
-          v = sqrt(qx * qx + qy * qy + dz * dz) - g.p[0];
-          break;
-        }
-        case CRYO_GEOM_SPHERE: v = sqrt(qx * qx + qy * qy + qz * qz) - g.p[0]; break;
-        default: {  // CRYO_GEOM_BOX
-          const double bx = fabs(qx) - 0.5 * g.p[0], by = fabs(qy) - 0.5 * g.p[1], bz = fabs(qz) - 0.5 * g.p[2];
-          const double ex = mx(bx, 0.0), ey = mx(by, 0.0), ez = mx(bz, 0.0);
-          v = sqrt(ex * ex + ey * ey + ez * ez) + mn(mx(mx(bx, by), bz), 0.0);
-          break;
-        }
+        case CRYO_GEOM_CYLINDER: v = cryo_sdf::cylinder(qx, qy, qz, g.p[0], g.p[1]); break;
+        case CRYO_GEOM_CAPSULE: v = cryo_sdf::capsule(qx, qy, qz, g.p[0], g.p[1]); break;
+        case CRYO_GEOM_SPHERE: v = cryo_sdf::sphere(qx, qy, qz, g.p[0]); break;
+        default: v = cryo_sdf::box(qx, qy, qz, g.p[0], g.p[1], g.p[2]); break;
       }
     } else if (g.kind == CRYO_GEOM_TRANSLATED) {
       v = val[g.a];
     } else if (g.kind == CRYO_GEOM_DIFFERENCE) {
-      v = mx(val[g.a], -val[g.b]);
+      v = cryo_sdf::subtract(val[g.a], val[g.b]);
     } else {  // CRYO_GEOM_UNION
-      v = mn(val[g.a], val[g.b]);
+      v = cryo_sdf::unite(val[g.a], val[g.b]);
     }
     val[k] = v;
   }

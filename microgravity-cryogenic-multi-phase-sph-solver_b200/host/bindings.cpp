@@ -18,120 +18,166 @@ using namespace cryosph;
 
 namespace {
 
-using Tuple3 = std::array<double, 3>;
-using DArr = py::array_t<double, py::array::c_style | py::array::forcecast>;
-using U8Arr = py::array_t<std::uint8_t, py::array::c_style | py::array::forcecast>;
+using Triple = std::array<double, 3>;
+using F64 = py::array_t<double, py::array::c_style | py::array::forcecast>;
+using F32 = py::array_t<float, py::array::c_style | py::array::forcecast>;
+using U8 = py::array_t<std::uint8_t, py::array::c_style | py::array::forcecast>;
+using U32 = py::array_t<std::uint32_t, py::array::c_style | py::array::forcecast>;
 
-Vec3 to_vec(const Tuple3& t) { return Vec3{static_cast<real>(t[0]), static_cast<real>(t[1]), static_cast<real>(t[2])}; }
-py::tuple to_tuple(Vec3 v) { return py::make_tuple(double(v.x), double(v.y), double(v.z)); }
+Vec3 vec(const Triple& t) { return {static_cast<real>(t[0]), static_cast<real>(t[1]), static_cast<real>(t[2])}; }
+py::tuple triple(Vec3 v) { return py::make_tuple(static_cast<double>(v.x), static_cast<double>(v.y), static_cast<double>(v.z)); }
 
+// A NumPy array of the given shape filled from `src` (element count = the shape's product).
 template <class T>
-py::array_t<T> to_array(const std::vector<T>& v) {
-  py::array_t<T> out(static_cast<py::ssize_t>(v.size()));
-  if (!v.empty()) std::memcpy(out.mutable_data(), v.data(), v.size() * sizeof(T));
+py::array_t<T> numpy_copy(const T* src, std::initializer_list<py::ssize_t> shape) {
+  py::array_t<T> out{std::vector<py::ssize_t>(shape)};
+  if (out.size() > 0) std::memcpy(out.mutable_data(), src, static_cast<std::size_t>(out.size()) * sizeof(T));
   return out;
 }
+template <class T>
+py::array_t<T> numpy_copy(const std::vector<T>& v) {
+  return numpy_copy(v.data(), {static_cast<py::ssize_t>(v.size())});
+}
 
-py::array_t<real> vec3_array(const std::vector<Vec3>& v) {
-  py::array_t<real> out({static_cast<py::ssize_t>(v.size()), py::ssize_t{3}});
-  auto r = out.mutable_unchecked<2>();
-  for (py::ssize_t i = 0; i < static_cast<py::ssize_t>(v.size()); ++i) {
-    r(i, 0) = v[i].x;
-    r(i, 1) = v[i].y;
-    r(i, 2) = v[i].z;
+// One input column of a particle set, converted to the solver's element type
+// by NumPy: n rows of `width` values ((n, 3) for vectors, n values otherwise).
+template <class Arr>
+Arr column(py::handle src, py::ssize_t n, int width, const char* name) {
+  Arr a = py::cast<Arr>(src);
+  const bool ok = width == 3 ? (a.ndim() == 2 && a.shape(0) == n && a.shape(1) == 3) : a.size() == n;
+  if (!ok)
+    throw std::invalid_argument(std::string(name) + (width == 3 ? ": expected an array of shape (N, 3)"
+                                                                : ": expected N values (one per particle)"));
+  return a;
+}
+
+// The particle set a caller hands over, held in the solver's element types;
+// view() gives the C ABI's structure of arrays over it (absent columns null).
+struct ParticleColumns {
+  F32 x, v, nrm, m, rho, T;
+  U8 phase, flags;
+  bool has_v = false, has_nrm = false, has_flags = false;
+  py::ssize_t n = 0;
+
+  ParticleColumns(py::handle position, py::handle mass, py::handle density, py::handle temperature,
+                  py::handle phase_in, py::handle velocity, py::handle normal, py::handle flags_in) {
+    x = py::cast<F32>(position);
+    if (x.ndim() != 2 || x.shape(1) != 3) throw std::invalid_argument("position: expected an array of shape (N, 3)");
+    n = x.shape(0);
+    m = column<F32>(mass, n, 1, "mass");
+    rho = column<F32>(density, n, 1, "density");
+    T = column<F32>(temperature, n, 1, "temperature");
+    phase = column<U8>(phase_in, n, 1, "phase");
+    const std::uint8_t* ph = phase.data();
+    for (py::ssize_t i = 0; i < n; ++i)
+      if (ph[i] > kWall) throw std::invalid_argument("phase: values must be 0 (liquid), 1 (vapour) or 2 (wall)");
+    if ((has_v = !velocity.is_none())) v = column<F32>(velocity, n, 3, "velocity");
+    if ((has_nrm = !normal.is_none())) nrm = column<F32>(normal, n, 3, "normal");
+    if ((has_flags = !flags_in.is_none())) flags = column<U8>(flags_in, n, 1, "flags");
   }
-  return out;
+  cryo_host_particles_t view() const {
+    auto p = [](const auto& a, bool on) { return on ? const_cast<std::remove_const_t<std::remove_pointer_t<decltype(a.data())>>*>(a.data()) : nullptr; };
+    return cryo_host_particles_t{static_cast<int>(n), p(x, true), p(v, has_v), p(nrm, has_nrm), p(m, true),
+                                 p(rho, true), p(T, true), p(phase, true), p(flags, has_flags), nullptr};
+  }
+};
+
+// The state of a solver (anything with num_particles() and download()) as
+// the reference's dict of NumPy arrays, filled in place by one download.
+template <class S>
+py::dict state_dict(const S& s) {
+  const auto n = static_cast<py::ssize_t>(s.num_particles());
+  py::array_t<real> x({n, py::ssize_t{3}}), v({n, py::ssize_t{3}}), nrm({n, py::ssize_t{3}});
+  py::array_t<real> m(n), rho(n), T(n);
+  py::array_t<std::uint8_t> phase(n), flags(n);
+  py::array_t<std::uint32_t> id(n);
+  cryo_host_particles_out_t o{static_cast<int>(n), x.mutable_data(), v.mutable_data(), nrm.mutable_data(),
+                              m.mutable_data(), rho.mutable_data(), T.mutable_data(), phase.mutable_data(),
+                              flags.mutable_data(), id.mutable_data()};
+  {
+    py::gil_scoped_release nogil;
+    s.download(o);
+  }
+  py::dict d;
+  d["position"] = x;
+  d["velocity"] = v;
+  d["normal"] = nrm;
+  d["mass"] = m;
+  d["density"] = rho;
+  d["temperature"] = T;
+  d["phase"] = phase;
+  d["flags"] = flags;
+  d["id"] = id;
+  return d;
 }
 
-py::dict particles_dict(const HostParticles& hp) {
+// Host particles (the generators' output) as the same dict.
+py::dict host_dict(const HostParticles& hp) {
+  const auto n = static_cast<py::ssize_t>(hp.size());
+  auto vecs = [n](const std::vector<Vec3>& a) { return numpy_copy(reinterpret_cast<const real*>(a.data()), {n, 3}); };
   py::dict d;
-  d["position"] = vec3_array(hp.x);
-  d["velocity"] = vec3_array(hp.v);
-  d["normal"] = vec3_array(hp.nrm);
-  d["mass"] = to_array(hp.m);
-  d["density"] = to_array(hp.rho);
-  d["temperature"] = to_array(hp.T);
-  d["phase"] = to_array(hp.phase);
-  d["flags"] = to_array(hp.flags);
-  d["id"] = to_array(hp.id);
+  d["position"] = vecs(hp.x);
+  d["velocity"] = vecs(hp.v);
+  d["normal"] = vecs(hp.nrm);
+  d["mass"] = numpy_copy(hp.m);
+  d["density"] = numpy_copy(hp.rho);
+  d["temperature"] = numpy_copy(hp.T);
+  d["phase"] = numpy_copy(hp.phase);
+  d["flags"] = numpy_copy(hp.flags);
+  d["id"] = numpy_copy(hp.id);
   return d;
+}
+
+// The reverse, for the host writers: a particles dict into HostParticles.
+HostParticles host_particles_of(const py::dict& d) {
+  const ParticleColumns c(d["position"], d["mass"], d["density"], d["temperature"], d["phase"],
+                          d.contains("velocity") ? py::handle(d["velocity"]) : py::handle(py::none()),
+                          d.contains("normal") ? py::handle(d["normal"]) : py::handle(py::none()),
+                          d.contains("flags") ? py::handle(d["flags"]) : py::handle(py::none()));
+  const auto n = static_cast<std::size_t>(c.n);
+  HostParticles hp;
+  auto vecs = [n](std::vector<Vec3>& dst, const F32& a, bool on) {
+    dst.assign(n, Vec3{0, 0, 0});
+    if (on && n) std::memcpy(dst.data(), a.data(), 12 * n);
+  };
+  vecs(hp.x, c.x, true);
+  vecs(hp.v, c.v, c.has_v);
+  vecs(hp.nrm, c.nrm, c.has_nrm);
+  hp.m.assign(c.m.data(), c.m.data() + n);
+  hp.rho.assign(c.rho.data(), c.rho.data() + n);
+  hp.T.assign(c.T.data(), c.T.data() + n);
+  hp.phase.assign(c.phase.data(), c.phase.data() + n);
+  hp.flags = c.has_flags ? std::vector<std::uint8_t>(c.flags.data(), c.flags.data() + n) : std::vector<std::uint8_t>(n, 0);
+  hp.id.resize(n);
+  for (std::size_t i = 0; i < n; ++i) hp.id[i] = static_cast<std::uint32_t>(i);
+  if (d.contains("id")) {
+    const U32 id = column<U32>(d["id"], c.n, 1, "id");
+    std::memcpy(hp.id.data(), id.data(), 4 * n);
+  }
+  return hp;
 }
 
 py::dict frame_dict(const TelemetryFrame& f) {
   py::dict d;
   d["time"] = f.time;
   d["step"] = f.step;
-  py::array_t<float> pos({static_cast<py::ssize_t>(f.n), py::ssize_t{3}});
-  if (f.n > 0) std::memcpy(pos.mutable_data(), f.position.data(), f.position.size() * sizeof(float));
-  d["position"] = pos;
-  d["temperature"] = to_array(f.temperature);
-  d["pressure"] = to_array(f.pressure);
-  d["speed"] = to_array(f.speed);
-  d["phase"] = to_array(f.phase);
+  d["position"] = numpy_copy(f.position.data(), {static_cast<py::ssize_t>(f.n), 3});
+  d["temperature"] = numpy_copy(f.temperature);
+  d["pressure"] = numpy_copy(f.pressure);
+  d["speed"] = numpy_copy(f.speed);
+  d["phase"] = numpy_copy(f.phase);
   return d;
 }
 
-// Host particles from NumPy inputs (all arrays of length N; position (N, 3)).
-HostParticles from_arrays(DArr position, DArr mass, DArr density, DArr temperature, U8Arr phase, py::object velocity,
-                          py::object normal, py::object flags) {
-  if (position.ndim() != 2 || position.shape(1) != 3) throw std::invalid_argument("position must have shape (N, 3)");
-  const py::ssize_t n = position.shape(0);
-  auto need_n = [n](const py::array& a, const char* name) {
-    if (a.size() != n) throw std::invalid_argument(std::string(name) + " must have length N");
-  };
-  need_n(mass, "mass");
-  need_n(density, "density");
-  need_n(temperature, "temperature");
-  need_n(phase, "phase");
-  DArr vel, nrm;
-  if (!velocity.is_none()) {
-    vel = velocity.cast<DArr>();
-    if (vel.ndim() != 2 || vel.shape(0) != n || vel.shape(1) != 3)
-      throw std::invalid_argument("velocity must have shape (N, 3)");
-  }
-  if (!normal.is_none()) {
-    nrm = normal.cast<DArr>();
-    if (nrm.ndim() != 2 || nrm.shape(0) != n || nrm.shape(1) != 3)
-      throw std::invalid_argument("normal must have shape (N, 3)");
-  }
-  U8Arr fl;
-  if (!flags.is_none()) {
-    fl = flags.cast<U8Arr>();
-    need_n(fl, "flags");
-  }
-  auto P = position.unchecked<2>();
-  const double* m = mass.data();
-  const double* rho = density.data();
-  const double* T = temperature.data();
-  const std::uint8_t* ph = phase.data();
-  HostParticles hp;
-  hp.reserve(static_cast<std::size_t>(n));
-  for (py::ssize_t i = 0; i < n; ++i) {
-    if (ph[i] > kWall) throw std::invalid_argument("phase values must be 0 (liquid), 1 (vapour) or 2 (wall)");
-    const Vec3 x{static_cast<real>(P(i, 0)), static_cast<real>(P(i, 1)), static_cast<real>(P(i, 2))};
-    Vec3 v{0, 0, 0}, nn{0, 0, 0};
-    if (vel.size()) {
-      const double* q = vel.data() + 3 * i;
-      v = Vec3{static_cast<real>(q[0]), static_cast<real>(q[1]), static_cast<real>(q[2])};
-    }
-    if (nrm.size()) {
-      const double* q = nrm.data() + 3 * i;
-      nn = Vec3{static_cast<real>(q[0]), static_cast<real>(q[1]), static_cast<real>(q[2])};
-    }
-    hp.push(x, v, static_cast<real>(m[i]), static_cast<real>(rho[i]), static_cast<real>(T[i]),
-            static_cast<Phase>(ph[i]), nn, fl.size() ? fl.data()[i] : std::uint8_t{0});
-  }
-  return hp;
-}
-
-std::vector<Vec3> rows3(const DArr& a, std::size_t n, const char* what) {
-  if (a.ndim() != 2 || a.shape(1) != 3 || static_cast<std::size_t>(a.shape(0)) != n)
-    throw std::invalid_argument(std::string(what) + " must have shape (len(time), 3)");
-  std::vector<Vec3> v(n);
-  auto r = a.unchecked<2>();
-  for (std::size_t i = 0; i < n; ++i)
-    v[i] = Vec3{static_cast<real>(r(i, 0)), static_cast<real>(r(i, 1)), static_cast<real>(r(i, 2))};
-  return v;
+// Rows of a (count, 3) array as Vec3 (manoeuvre tables).
+std::vector<Vec3> vec_rows(const F64& a, std::size_t count, const char* what) {
+  if (a.ndim() != 2 || a.shape(1) != 3 || static_cast<std::size_t>(a.shape(0)) != count)
+    throw std::invalid_argument(std::string(what) + ": expected an array of shape (len(time), 3)");
+  std::vector<Vec3> out;
+  out.reserve(count);
+  const double* p = a.data();
+  for (std::size_t k = 0; k < count; ++k, p += 3) out.push_back(Vec3{static_cast<real>(p[0]), static_cast<real>(p[1]), static_cast<real>(p[2])});
+  return out;
 }
 
 }  // namespace
@@ -207,7 +253,7 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property_readonly("name", &Geometry::name)
       .def_property_readonly("bounds", [](const Geometry& g) {
         const AABB b = g.bounds();
-        return std::make_pair(to_tuple(b.lo), to_tuple(b.hi));
+        return std::make_pair(triple(b.lo), triple(b.hi));
       });
   py::class_<CylinderTank, Geometry, std::shared_ptr<CylinderTank>>(m, "CylinderTank")
       .def(py::init<double, double>(), py::arg("radius"), py::arg("height"));
@@ -218,7 +264,7 @@ PYBIND11_MODULE(CryoSPH, m) {
   py::class_<BoxTank, Geometry, std::shared_ptr<BoxTank>>(m, "BoxTank")
       .def(py::init<double, double, double>(), py::arg("lx"), py::arg("ly"), py::arg("lz"));
   py::class_<Translated, Geometry, std::shared_ptr<Translated>>(m, "Translated", "Geometry shifted by a constant offset.")
-      .def(py::init([](std::shared_ptr<Geometry> g, const Tuple3& o) { return std::make_shared<Translated>(g, to_vec(o)); }),
+      .def(py::init([](std::shared_ptr<Geometry> g, const Triple& o) { return std::make_shared<Translated>(g, vec(o)); }),
            py::arg("geometry"), py::arg("offset"));
   py::class_<Difference, Geometry, std::shared_ptr<Difference>>(
       m, "Difference", "Fluid domain of `a` minus the solid `b` (obstacles, baffles, PMD vanes).")
@@ -226,10 +272,10 @@ PYBIND11_MODULE(CryoSPH, m) {
   py::class_<Union, Geometry, std::shared_ptr<Union>>(m, "Union", "Fluid domain of `a` united with `b`.")
       .def(py::init<std::shared_ptr<const Geometry>, std::shared_ptr<const Geometry>>(), py::arg("a"), py::arg("b"));
   py::class_<MeshTank, Geometry, std::shared_ptr<MeshTank>>(m, "MeshTank")
-      .def(py::init([](const std::string& path, double scale, const Tuple3& offset) {
-             return std::make_shared<MeshTank>(path, scale, to_vec(offset));
+      .def(py::init([](const std::string& path, double scale, const Triple& offset) {
+             return std::make_shared<MeshTank>(path, scale, vec(offset));
            }),
-           py::arg("obj_path"), py::arg("scale") = 1.0, py::arg("offset") = Tuple3{0, 0, 0})
+           py::arg("obj_path"), py::arg("scale") = 1.0, py::arg("offset") = Triple{0, 0, 0})
       .def_property_readonly("num_triangles", &MeshTank::num_triangles)
       .def("winding_number", &MeshTank::winding_number, py::arg("x"), py::arg("y"), py::arg("z"));
 
@@ -238,11 +284,11 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_readwrite("mode", &FillSpec::mode)
       .def_readwrite("fill_fraction", &FillSpec::fill_fraction)
       .def_property(
-          "settle_direction", [](const FillSpec& f) { return to_tuple(f.settle_direction); },
-          [](FillSpec& f, const Tuple3& t) { f.settle_direction = to_vec(t); })
+          "settle_direction", [](const FillSpec& f) { return triple(f.settle_direction); },
+          [](FillSpec& f, const Triple& t) { f.settle_direction = vec(t); })
       .def_property(
-          "bubble_center", [](const FillSpec& f) { return to_tuple(f.bubble_center); },
-          [](FillSpec& f, const Tuple3& t) { f.bubble_center = to_vec(t); })
+          "bubble_center", [](const FillSpec& f) { return triple(f.bubble_center); },
+          [](FillSpec& f, const Triple& t) { f.bubble_center = vec(t); })
       .def_readwrite("include_vapor", &FillSpec::include_vapor)
       .def_readwrite("wall_layers", &FillSpec::wall_layers)
       .def_readwrite("T_liquid", &FillSpec::T_liquid)
@@ -256,7 +302,7 @@ PYBIND11_MODULE(CryoSPH, m) {
   m.def(
       "tank_particles",
       [](const Geometry& g, const FluidProperties& f, real dx, const FillSpec& fill) {
-        return particles_dict(build_tank_particles(g, f, dx, fill));
+        return host_dict(build_tank_particles(g, f, dx, fill));
       },
       py::arg("geometry"), py::arg("fluid"), py::arg("dx"), py::arg("fill") = FillSpec{},
       "Lattice particles of a filled tank (walls first, then fluid) as a dict of NumPy arrays.");
@@ -265,21 +311,73 @@ PYBIND11_MODULE(CryoSPH, m) {
       [](const Geometry& g, real dx, int wall_layers) {
         AABB dom = g.bounds();
         const real pad = (wall_layers + 1) * dx;
-        return std::make_pair(to_tuple(dom.lo - Vec3{pad, pad, pad}), to_tuple(dom.hi + Vec3{pad, pad, pad}));
+        return std::make_pair(triple(dom.lo - Vec3{pad, pad, pad}), triple(dom.hi + Vec3{pad, pad, pad}));
       },
       py::arg("geometry"), py::arg("dx"), py::arg("wall_layers") = 3);
   m.def(
       "make_block",
-      [](const Tuple3& lo, const Tuple3& hi, real dx, Phase phase, real density, real temperature) {
-        return particles_dict(make_block(to_vec(lo), to_vec(hi), dx, phase, density, temperature));
+      [](const Triple& lo, const Triple& hi, real dx, Phase phase, real density, real temperature) {
+        return host_dict(make_block(vec(lo), vec(hi), dx, phase, density, temperature));
       },
       py::arg("lo"), py::arg("hi"), py::arg("dx"), py::arg("phase"), py::arg("density"), py::arg("temperature"));
+
+  // The writers of io.hpp:13-22 for host particle dicts (no device needed;
+  // Solver.write_vtk / write_json write the same files from the device).
+  m.def(
+      "write_vtk",
+      [](const std::string& path, const py::dict& particles, py::object pressure) {
+        const HostParticles hp = host_particles_of(particles);
+        std::vector<real> p;
+        if (!pressure.is_none()) {
+          const F32 a = column<F32>(pressure, static_cast<py::ssize_t>(hp.size()), 1, "pressure");
+          p.assign(a.data(), a.data() + a.size());
+        }
+        write_vtk(path, hp, p);
+      },
+      py::arg("path"), py::arg("particles"), py::arg("pressure") = py::none(),
+      "Legacy binary VTK polydata of a particle dict (pressure scalars when given).");
+  m.def(
+      "make_frame",
+      [](const py::dict& particles, py::object pressure, double time, long long step) {
+        const HostParticles hp = host_particles_of(particles);
+        std::vector<real> p;
+        if (!pressure.is_none()) {
+          const F32 a = column<F32>(pressure, static_cast<py::ssize_t>(hp.size()), 1, "pressure");
+          p.assign(a.data(), a.data() + a.size());
+        }
+        return frame_dict(make_frame(hp, p, time, step));
+      },
+      py::arg("particles"), py::arg("pressure") = py::none(), py::arg("time") = 0.0, py::arg("step") = 0,
+      "The viewer frame of a particle dict (as fetch_telemetry returns it).");
+  m.def(
+      "write_json_frame",
+      [](const std::string& path, const py::dict& frame, bool include_walls) {
+        TelemetryFrame f;
+        f.time = frame["time"].cast<double>();
+        f.step = frame["step"].cast<long long>();
+        const F32 pos = py::cast<F32>(frame["position"]);
+        f.n = static_cast<int>(pos.size() / 3);
+        const py::ssize_t n = f.n;
+        f.position.assign(pos.data(), pos.data() + 3 * n);
+        auto col = [&](const char* k) {
+          const F32 a = column<F32>(frame[k], n, 1, k);
+          return std::vector<float>(a.data(), a.data() + n);
+        };
+        f.temperature = col("temperature");
+        f.pressure = col("pressure");
+        f.speed = col("speed");
+        const U8 ph = column<U8>(frame["phase"], n, 1, "phase");
+        f.phase.assign(ph.data(), ph.data() + n);
+        write_json_frame(path, f, include_walls);
+      },
+      py::arg("path"), py::arg("frame"), py::arg("include_walls") = true,
+      "The viewer's JSON frame file of a frame dict (walls left out unless include_walls).");
 
   py::class_<SolverConfig> cfg(m, "SolverConfig", "Solver parameters (the reference's SolverConfig).");
   cfg.def(py::init<>())
       .def_property(
-          "gravity", [](const SolverConfig& c) { return to_tuple(c.gravity); },
-          [](SolverConfig& c, const Tuple3& t) { c.gravity = to_vec(t); });
+          "gravity", [](const SolverConfig& c) { return triple(c.gravity); },
+          [](SolverConfig& c, const Triple& t) { c.gravity = vec(t); });
 #define CRYO_RW(field) cfg.def_readwrite(#field, &SolverConfig::field)
   CRYO_RW(dx); CRYO_RW(h_factor); CRYO_RW(kernel); CRYO_RW(density_mode); CRYO_RW(normalize_initial_masses);
   CRYO_RW(velocity_scale); CRYO_RW(sound_speed); CRYO_RW(tait_gamma); CRYO_RW(background_pressure);
@@ -305,13 +403,13 @@ PYBIND11_MODULE(CryoSPH, m) {
   CRYO_RO(vented_enthalpy); CRYO_RO(T_sat); CRYO_RO(p_ullage); CRYO_RO(max_speed); CRYO_RO(T_liquid_mean);
   CRYO_RO(T_liquid_max); CRYO_RO(T_vapor_mean); CRYO_RO(splits); CRYO_RO(merges);
 #undef CRYO_RO
-  diag.def_property_readonly("liquid_com", [](const Diagnostics& d) { return to_tuple(d.liquid_com); })
-      .def_property_readonly("slosh_force", [](const Diagnostics& d) { return to_tuple(d.slosh_force); })
-      .def_property_readonly("slosh_moment", [](const Diagnostics& d) { return to_tuple(d.slosh_moment); })
-      .def_property_readonly("frame_acceleration", [](const Diagnostics& d) { return to_tuple(d.frame_acceleration); })
+  diag.def_property_readonly("liquid_com", [](const Diagnostics& d) { return triple(d.liquid_com); })
+      .def_property_readonly("slosh_force", [](const Diagnostics& d) { return triple(d.slosh_force); })
+      .def_property_readonly("slosh_moment", [](const Diagnostics& d) { return triple(d.slosh_moment); })
+      .def_property_readonly("frame_acceleration", [](const Diagnostics& d) { return triple(d.frame_acceleration); })
       .def_property_readonly("frame_angular_velocity",
-                             [](const Diagnostics& d) { return to_tuple(d.frame_angular_velocity); })
-      .def_property_readonly("liquid_momentum", [](const Diagnostics& d) { return to_tuple(d.liquid_momentum); })
+                             [](const Diagnostics& d) { return triple(d.frame_angular_velocity); })
+      .def_property_readonly("liquid_momentum", [](const Diagnostics& d) { return triple(d.liquid_momentum); })
       .def("as_dict", [](const Diagnostics& d) {
         py::dict r;
         py::object self = py::cast(d);
@@ -327,23 +425,23 @@ PYBIND11_MODULE(CryoSPH, m) {
 
   py::class_<ManeuverProfile>(m, "ManeuverProfile",
                               "Prescribed tank motion (tank frame): piecewise-linear acceleration and angular velocity.")
-      .def(py::init([](std::vector<double> time, DArr acc, py::object omega, const Tuple3& origin) {
+      .def(py::init([](std::vector<double> time, F64 acc, py::object omega, const Triple& origin) {
              ManeuverProfile p;
              p.time = std::move(time);
-             p.acceleration = rows3(acc, p.time.size(), "acceleration");
-             if (!omega.is_none()) p.angular_velocity = rows3(omega.cast<DArr>(), p.time.size(), "angular_velocity");
-             p.origin = to_vec(origin);
+             p.acceleration = vec_rows(acc, p.time.size(), "acceleration");
+             if (!omega.is_none()) p.angular_velocity = vec_rows(omega.cast<F64>(), p.time.size(), "angular_velocity");
+             p.origin = vec(origin);
              p.validate();
              return p;
            }),
            py::arg("time"), py::arg("acceleration"), py::arg("angular_velocity") = py::none(),
-           py::arg("origin") = Tuple3{0, 0, 0})
+           py::arg("origin") = Triple{0, 0, 0})
       .def(
           "evaluate",
           [](const ManeuverProfile& p, double t) {
             Vec3 a, w, wd;
             p.evaluate(t, a, w, wd);
-            return py::make_tuple(to_tuple(a), to_tuple(w), to_tuple(wd));
+            return py::make_tuple(triple(a), triple(w), triple(wd));
           },
           py::arg("t"), "Returns (acceleration, angular_velocity, angular_acceleration) at time t.");
 
@@ -356,10 +454,13 @@ PYBIND11_MODULE(CryoSPH, m) {
           "Generates wall/liquid/vapour particles for a tank (on the GPU for analytic and CSG tanks).")
       .def(
           "set_particles",
-          [](Solver& s, DArr position, DArr mass, DArr density, DArr temperature, U8Arr phase, const Tuple3& domain_lo,
-             const Tuple3& domain_hi, py::object velocity, py::object normal, py::object flags) {
-            const HostParticles hp = from_arrays(position, mass, density, temperature, phase, velocity, normal, flags);
-            s.set_particles(hp, AABB{to_vec(domain_lo), to_vec(domain_hi)});
+          [](Solver& s, py::object position, py::object mass, py::object density, py::object temperature,
+             py::object phase, const Triple& domain_lo, const Triple& domain_hi, py::object velocity,
+             py::object normal, py::object flags) {
+            const ParticleColumns cols(position, mass, density, temperature, phase, velocity, normal, flags);
+            const cryo_host_particles_t view = cols.view();
+            py::gil_scoped_release nogil;
+            s.set_particles(view, AABB{vec(domain_lo), vec(domain_hi)});
           },
           py::arg("position"), py::arg("mass"), py::arg("density"), py::arg("temperature"), py::arg("phase"),
           py::arg("domain_lo"), py::arg("domain_hi"), py::arg("velocity") = py::none(), py::arg("normal") = py::none(),
@@ -372,10 +473,10 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def("next_dt", &Solver::next_dt)
       .def("diagnostics", &Solver::diagnostics)
       .def(
-          "particles", [](const Solver& s) { return particles_dict(s.particles()); },
+          "particles", [](const Solver& s) { return state_dict(s); },
           "Copies the particle state into a dict of NumPy arrays.")
-      .def("pressure", [](const Solver& s) { return to_array(s.pressure()); })
-      .def("curvature", [](const Solver& s) { return to_array(s.curvature()); })
+      .def("pressure", [](const Solver& s) { return numpy_copy(s.pressure()); })
+      .def("curvature", [](const Solver& s) { return numpy_copy(s.curvature()); })
       .def_property_readonly("time", &Solver::time)
       .def_property_readonly("step_count", &Solver::step_count)
       .def_property_readonly("last_dt", &Solver::last_dt)
@@ -385,15 +486,15 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property_readonly("fluid", &Solver::fluid)
       .def_property_readonly("sound_speed", &Solver::sound_speed)
       .def_property_readonly("smoothing_length", &Solver::smoothing_length)
-      .def("set_gravity", [](Solver& s, const Tuple3& g) { s.set_gravity(to_vec(g)); }, py::arg("g"))
+      .def("set_gravity", [](Solver& s, const Triple& g) { s.set_gravity(vec(g)); }, py::arg("g"))
       .def("set_heater_power", &Solver::set_heater_power, py::arg("watts"))
       .def(
           "set_frame_motion",
-          [](Solver& s, const Tuple3& acc, const Tuple3& w, const Tuple3& wdot, const Tuple3& origin) {
-            s.set_frame_motion(to_vec(acc), to_vec(w), to_vec(wdot), to_vec(origin));
+          [](Solver& s, const Triple& acc, const Triple& w, const Triple& wdot, const Triple& origin) {
+            s.set_frame_motion(vec(acc), vec(w), vec(wdot), vec(origin));
           },
-          py::arg("acceleration") = Tuple3{0, 0, 0}, py::arg("angular_velocity") = Tuple3{0, 0, 0},
-          py::arg("angular_acceleration") = Tuple3{0, 0, 0}, py::arg("origin") = Tuple3{0, 0, 0},
+          py::arg("acceleration") = Triple{0, 0, 0}, py::arg("angular_velocity") = Triple{0, 0, 0},
+          py::arg("angular_acceleration") = Triple{0, 0, 0}, py::arg("origin") = Triple{0, 0, 0},
           "Constant tank-frame motion: linear acceleration of the tank, angular velocity and acceleration.")
       .def("set_maneuver", &Solver::set_maneuver, py::arg("profile"))
       .def("clear_frame_motion", &Solver::clear_frame_motion)
@@ -447,13 +548,10 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property_readonly("telemetry_mode", &Solver::telemetry_mode)
       .def(
           "probe_pressure",
-          [](Solver& s, DArr pts) {
-            if (pts.ndim() != 2 || pts.shape(1) != 3) throw std::invalid_argument("points must have shape (N, 3)");
-            std::vector<Vec3> v(static_cast<std::size_t>(pts.shape(0)));
-            auto r = pts.unchecked<2>();
-            for (py::ssize_t i = 0; i < pts.shape(0); ++i)
-              v[i] = Vec3{static_cast<real>(r(i, 0)), static_cast<real>(r(i, 1)), static_cast<real>(r(i, 2))};
-            return to_array(s.probe_pressure(v));
+          [](Solver& s, const F32& pts) {
+            if (pts.ndim() != 2 || pts.shape(1) != 3) throw std::invalid_argument("points: expected an array of shape (N, 3)");
+            const auto* p = reinterpret_cast<const Vec3*>(pts.data());
+            return numpy_copy(s.probe_pressure(std::vector<Vec3>(p, p + pts.shape(0))));
           },
           py::arg("points"), "Virtual pressure sensors: Shepard-weighted liquid pressure at each point; NaN where dry.")
       .def("request_telemetry", &Solver::request_telemetry,
@@ -472,15 +570,10 @@ PYBIND11_MODULE(CryoSPH, m) {
             return frame_dict(f);
           },
           "Waits for the pending capture and returns it as a dict (None if nothing was requested).")
-      .def(
-          "write_vtk", [](const Solver& s, const std::string& path) { write_vtk(path, s.particles(), s.pressure()); },
-          py::arg("path"))
-      .def(
-          "write_json",
-          [](const Solver& s, const std::string& path, bool include_walls) {
-            write_json_frame(path, make_frame(s.particles(), s.pressure(), s.time(), s.step_count()), include_walls);
-          },
-          py::arg("path"), py::arg("include_walls") = false)
+      .def("write_vtk", &Solver::write_vtk, py::arg("path"),
+           "Legacy binary VTK polydata of the state (payload packed on the device).")
+      .def("write_json", &Solver::write_json, py::arg("path"), py::arg("include_walls") = false,
+           "Viewer frame as JSON (walls dropped on the device unless include_walls).")
       // B200 extensions
       .def_property_readonly("stream_handle", &Solver::stream_handle, "The solver's CUDA stream (cudaStream_t).")
       .def_property_readonly(
@@ -502,7 +595,7 @@ PYBIND11_MODULE(CryoSPH, m) {
           "field",
           [](const Solver& s, int f) {
             auto v = s.field(f);
-            return to_array(v);
+            return numpy_copy(v);
           },
           py::arg("field"), "Raw per-particle field (cryosph_b200.h CRYO_F_*).");
 
@@ -548,11 +641,13 @@ PYBIND11_MODULE(CryoSPH, m) {
            "Generates the tank's particles (host generator) and cuts them into the slabs.")
       .def(
           "set_particles",
-          [](SlabSolver& s, DArr position, DArr mass, DArr density, DArr temperature, U8Arr phase,
-             const Tuple3& domain_lo, const Tuple3& domain_hi, py::object velocity, py::object normal,
-             py::object flags) {
-            const HostParticles hp = from_arrays(position, mass, density, temperature, phase, velocity, normal, flags);
-            s.set_particles(hp, AABB{to_vec(domain_lo), to_vec(domain_hi)});
+          [](SlabSolver& s, py::object position, py::object mass, py::object density, py::object temperature,
+             py::object phase, const Triple& domain_lo, const Triple& domain_hi, py::object velocity,
+             py::object normal, py::object flags) {
+            const ParticleColumns cols(position, mass, density, temperature, phase, velocity, normal, flags);
+            const cryo_host_particles_t view = cols.view();
+            py::gil_scoped_release nogil;
+            s.set_particles(view, AABB{vec(domain_lo), vec(domain_hi)});
           },
           py::arg("position"), py::arg("mass"), py::arg("density"), py::arg("temperature"), py::arg("phase"),
           py::arg("domain_lo"), py::arg("domain_hi"), py::arg("velocity") = py::none(), py::arg("normal") = py::none(),
@@ -561,7 +656,7 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def("run_steps", &SlabSolver::run_steps, py::arg("n"), py::call_guard<py::gil_scoped_release>())
       .def("diagnostics", &SlabSolver::diagnostics)
       .def(
-          "particles", [](const SlabSolver& s) { return particles_dict(s.particles()); },
+          "particles", [](const SlabSolver& s) { return state_dict(s); },
           "The whole tank's particles, in the order a Solver's arrays have.")
       .def_property_readonly("num_particles", &SlabSolver::num_particles)
       .def_property_readonly("slabs", &SlabSolver::slabs)

@@ -319,6 +319,8 @@ class Solver {
   Solver& operator=(const Solver&) = delete;
 
   void set_particles(const HostParticles& particles, const AABB& domain);
+  // the same from caller-owned arrays in the C ABI's layout (no host copy)
+  void set_particles(const cryo_host_particles_t& particles, const AABB& domain);
   // on_device: generate the lattice on the GPU where the geometry has a
   // device form (the particles are the same as the host generator's)
   void build_tank(const Geometry& geometry, const FillSpec& fill, bool on_device = true);
@@ -334,6 +336,8 @@ class Solver {
 
   Diagnostics diagnostics();
   HostParticles particles() const;
+  // particles() into caller-owned arrays (out.n >= num_particles())
+  void download(cryo_host_particles_out_t& out) const;
   std::vector<real> pressure() const;
   std::vector<real> curvature() const;
   std::vector<real> field(int cryo_field) const;
@@ -363,6 +367,11 @@ class Solver {
   bool fetch_telemetry(TelemetryFrame& out);
 
   std::vector<real> probe_pressure(const std::vector<Vec3>& points);
+
+  // write_vtk(path, particles(), pressure()) and write_json_frame(path,
+  // make_frame(...)) of the reference, with the payload packed on the device
+  void write_vtk(const std::string& path) const;
+  void write_json(const std::string& path, bool include_walls = false) const;
 
   // B200 extensions
   cryo_ctx* handle() const noexcept { return ctx_; }
@@ -440,11 +449,13 @@ class SlabSolver {
   SlabSolver& operator=(const SlabSolver&) = delete;
 
   void set_particles(const HostParticles& particles, const AABB& domain);
+  void set_particles(const cryo_host_particles_t& particles, const AABB& domain);
   void build_tank(const Geometry& geometry, const FillSpec& fill);  // the host lattice generator
   void step() { run_steps(1); }
   void run_steps(long long n);
   Diagnostics diagnostics();
   HostParticles particles() const;
+  void download(cryo_host_particles_out_t& out) const;
   std::size_t num_particles() const;
   int slabs() const noexcept { return slabs_; }
   // cell-layer boundaries (slabs + 1 entries), then per slab the particles

@@ -127,21 +127,44 @@ void Solver::check(int rc) const {
   if (rc) raise(rc, cryo_last_error(ctx_));
 }
 
-void Solver::set_particles(const HostParticles& hp, const AABB& domain) {
-  const int n = static_cast<int>(hp.size());
-  std::vector<float> x(3 * hp.size()), v(3 * hp.size()), nrm(3 * hp.size());
-  for (std::size_t i = 0; i < hp.size(); ++i) {
-    put3(x.data() + 3 * i, hp.x[i]);
-    put3(v.data() + 3 * i, hp.v[i]);
-    put3(nrm.data() + 3 * i, hp.nrm[i]);
-  }
-  cryo_host_particles_t p{n, x.data(), v.data(), nrm.data(), hp.m.data(), hp.rho.data(), hp.T.data(),
-                          hp.phase.data(), hp.flags.data(), hp.id.data()};
+// HostParticles as the C ABI's structure of arrays: Vec3 is three packed
+// floats, so the vectors are passed in place.
+static_assert(sizeof(Vec3) == 3 * sizeof(float) && sizeof(real) == sizeof(float), "Vec3 must be three floats");
+static cryo_host_particles_t soa_view(const HostParticles& hp) {
+  auto f3 = [](const std::vector<Vec3>& v) { return const_cast<float*>(reinterpret_cast<const float*>(v.data())); };
+  return cryo_host_particles_t{static_cast<int>(hp.size()),
+                               f3(hp.x),
+                               f3(hp.v),
+                               f3(hp.nrm),
+                               const_cast<float*>(hp.m.data()),
+                               const_cast<float*>(hp.rho.data()),
+                               const_cast<float*>(hp.T.data()),
+                               const_cast<std::uint8_t*>(hp.phase.data()),
+                               const_cast<std::uint8_t*>(hp.flags.data()),
+                               const_cast<std::uint32_t*>(hp.id.data())};
+}
+static void domain_floats(const AABB& d, float* lo, float* hi) {
+  put3(lo, d.lo);
+  put3(hi, d.hi);
+}
+// Resizes `h` to n particles and points `out` at its arrays.
+static cryo_host_particles_out_t soa_sink(HostParticles& h, std::size_t n) {
+  h.x.resize(n); h.v.resize(n); h.nrm.resize(n); h.m.resize(n); h.rho.resize(n); h.T.resize(n);
+  h.phase.resize(n); h.flags.resize(n); h.id.resize(n);
+  return cryo_host_particles_out_t{static_cast<int>(n), reinterpret_cast<float*>(h.x.data()),
+                                   reinterpret_cast<float*>(h.v.data()), reinterpret_cast<float*>(h.nrm.data()),
+                                   h.m.data(), h.rho.data(), h.T.data(), h.phase.data(), h.flags.data(), h.id.data()};
+}
+
+void Solver::set_particles(const HostParticles& hp, const AABB& domain) { set_particles(soa_view(hp), domain); }
+
+void Solver::set_particles(const cryo_host_particles_t& p, const AABB& domain) {
   float lo[3], hi[3];
-  put3(lo, domain.lo);
-  put3(hi, domain.hi);
+  domain_floats(domain, lo, hi);
   check(cryo_set_particles(ctx_, &p, lo, hi));
 }
+
+void Solver::download(cryo_host_particles_out_t& out) const { check(cryo_download(ctx_, &out)); }
 
 // Solver::build_tank (sph_solver.cu:430-437)
 void Solver::build_tank(const Geometry& geometry, const FillSpec& fill, bool on_device) {
@@ -227,27 +250,10 @@ Diagnostics Solver::diagnostics() {
   return to_diagnostics(d);
 }
 
-static HostParticles download(std::size_t n, const std::function<int(cryo_host_particles_out_t*)>& get) {
-  HostParticles h;
-  std::vector<float> x(3 * n), v(3 * n), nrm(3 * n);
-  h.m.resize(n); h.rho.resize(n); h.T.resize(n); h.phase.resize(n); h.flags.resize(n); h.id.resize(n);
-  cryo_host_particles_out_t o{static_cast<int>(n), x.data(), v.data(), nrm.data(), h.m.data(), h.rho.data(),
-                              h.T.data(), h.phase.data(), h.flags.data(), h.id.data()};
-  const int rc = get(&o);
-  if (rc) return h;
-  h.x.resize(n); h.v.resize(n); h.nrm.resize(n);
-  for (std::size_t i = 0; i < n; ++i) {
-    h.x[i] = get3(x.data() + 3 * i);
-    h.v[i] = get3(v.data() + 3 * i);
-    h.nrm[i] = get3(nrm.data() + 3 * i);
-  }
-  return h;
-}
-
 HostParticles Solver::particles() const {
-  int rc = 0;
-  HostParticles h = download(num_particles(), [&](cryo_host_particles_out_t* o) { return rc = cryo_download(ctx_, o); });
-  check(rc);
+  HostParticles h;
+  cryo_host_particles_out_t o = soa_sink(h, num_particles());
+  download(o);
   return h;
 }
 
@@ -492,21 +498,15 @@ void SlabSolver::check(int rc) const {
   if (rc) raise(rc, cryo_slabs_last_error(s_));
 }
 
-void SlabSolver::set_particles(const HostParticles& hp, const AABB& domain) {
-  const int n = static_cast<int>(hp.size());
-  std::vector<float> x(3 * hp.size()), v(3 * hp.size()), nrm(3 * hp.size());
-  for (std::size_t i = 0; i < hp.size(); ++i) {
-    put3(x.data() + 3 * i, hp.x[i]);
-    put3(v.data() + 3 * i, hp.v[i]);
-    put3(nrm.data() + 3 * i, hp.nrm[i]);
-  }
-  cryo_host_particles_t p{n, x.data(), v.data(), nrm.data(), hp.m.data(), hp.rho.data(), hp.T.data(),
-                          hp.phase.data(), hp.flags.data(), hp.id.data()};
+void SlabSolver::set_particles(const HostParticles& hp, const AABB& domain) { set_particles(soa_view(hp), domain); }
+
+void SlabSolver::set_particles(const cryo_host_particles_t& p, const AABB& domain) {
   float lo[3], hi[3];
-  put3(lo, domain.lo);
-  put3(hi, domain.hi);
+  domain_floats(domain, lo, hi);
   check(cryo_slabs_set_particles(s_, &p, lo, hi));
 }
+
+void SlabSolver::download(cryo_host_particles_out_t& out) const { check(cryo_slabs_download(s_, &out)); }
 
 // Solver::build_tank (sph_solver.cu:430-437) with the host generator.
 void SlabSolver::build_tank(const Geometry& geometry, const FillSpec& fill) {
@@ -533,10 +533,9 @@ std::size_t SlabSolver::num_particles() const {
 }
 
 HostParticles SlabSolver::particles() const {
-  int rc = 0;
-  HostParticles h =
-      download(num_particles(), [&](cryo_host_particles_out_t* o) { return rc = cryo_slabs_download(s_, o); });
-  check(rc);
+  HostParticles h;
+  cryo_host_particles_out_t o = soa_sink(h, num_particles());
+  download(o);
   return h;
 }
 

@@ -209,3 +209,53 @@ def test_capacity_growth_keeps_the_state(cuda_device):
     assert g.num_particles() <= cap0.value
     assert g.device_status() == 0
     assert np.isfinite(x0).all()
+
+
+def test_device_packed_frames_equal_the_host_writers(cuda_device, tmp_path):
+    """Solver.write_vtk / write_json pack the payload on the device
+    (cryo_frame_vtk, cryo_frame_viewer); the files are byte-identical to the
+    host writers' on the downloaded state (write_vtk(particles, pressure) and
+    write_json_frame(make_frame(...)), io.cpp:52-142 of the reference)."""
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    solver = cs.Solver(small_config(thermo_mode=cs.TankThermoMode.Closed), ln2)
+    fill = cs.FillSpec()
+    fill.fill_fraction = 0.5
+    solver.build_tank(cs.CylinderTank(0.02, 0.05), fill)
+    solver.run_steps(7)
+    parts, pres = solver.particles(), solver.pressure()
+    dev, host = tmp_path / "dev.vtk", tmp_path / "host.vtk"
+    solver.write_vtk(str(dev))
+    cs.write_vtk(str(host), parts, pres)
+    assert dev.read_bytes() == host.read_bytes()
+    for walls in (False, True):
+        dev, host = tmp_path / f"dev{walls}.json", tmp_path / f"host{walls}.json"
+        solver.write_json(str(dev), include_walls=walls)
+        cs.write_json_frame(str(host), cs.make_frame(parts, pres, solver.time, solver.step_count), include_walls=walls)
+        assert dev.read_text() == host.read_text()
+        d = json.loads(dev.read_text())
+        assert d["n"] == (len(parts["phase"]) if walls else int((parts["phase"] != 2).sum()))
+
+
+def test_particles_round_trip_through_the_soa_transfers(cuda_device):
+    """set_particles then particles() returns every array as given (float32
+    state; ids and flags as given; velocities, normals and flags optional)."""
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    rng = np.random.default_rng(3)
+    p = cs.tank_particles(cs.BoxTank(0.03, 0.03, 0.03), ln2, 0.003, cs.FillSpec())
+    n = len(p["mass"])
+    v = rng.standard_normal((n, 3))
+    solver = cs.Solver(small_config(dx=0.003), ln2)
+    solver.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"],
+                         domain_lo=(-0.03, -0.03, -0.03), domain_hi=(0.03, 0.03, 0.03), velocity=v,
+                         normal=p["normal"], flags=p["flags"])
+    q = solver.particles()
+    for k in ("position", "mass", "density", "temperature", "normal"):
+        assert np.array_equal(q[k], np.asarray(p[k], np.float32)), k
+    assert np.array_equal(q["velocity"], v.astype(np.float32))
+    for k in ("phase", "flags", "id"):
+        assert np.array_equal(q[k], p[k]), k
+    solver.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"],
+                         domain_lo=(-0.03, -0.03, -0.03), domain_hi=(0.03, 0.03, 0.03))
+    q = solver.particles()
+    assert not q["velocity"].any() and not q["normal"].any() and not q["flags"].any()
+    assert np.array_equal(q["id"], np.arange(n))

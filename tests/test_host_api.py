@@ -1,6 +1,7 @@
 """The CryoSPH Python module on the CPU side: the reference's public API
 (tests/python/test_bindings.py of the reference, the parts that need no
 device), and the lattice generator against the reference's own."""
+import json
 import math
 
 import numpy as np
@@ -158,3 +159,137 @@ def test_lattice_generator_bit_identical_to_reference(name, mk, nodes, dx, fillk
     lo, hi = cs.tank_domain(mk(), dx, 3)
     rlo, rhi = refpy.tank_domain(nodes, dx, 3)
     assert np.array_equal(np.float32(lo), np.float32(rlo)) and np.array_equal(np.float32(hi), np.float32(rhi))
+
+
+def _read_vtk(path):
+    """(n, points, velocity, {scalar name: values}) of a legacy binary VTK polydata file."""
+    raw = path.read_bytes()
+    assert raw.startswith(b"# vtk DataFile Version 3.0\nCryoSPH-CUDA particles\nBINARY\nDATASET POLYDATA\n")
+    at = raw.index(b"POINTS ")
+    n = int(raw[at:raw.index(b"\n", at)].split()[1])
+
+    def block(tag, words, start):
+        i = raw.index(tag, start)
+        j = raw.index(b"\n", i) + 1
+        return np.frombuffer(raw[j:j + 4 * words], dtype=">f4" if tag != b"VERTICES" else ">i4"), j + 4 * words
+
+    pts, at = block(b"POINTS", 3 * n, 0)
+    verts, at = block(b"VERTICES", 2 * n, at)
+    scal = {}
+    for name in (b"temperature", b"mass", b"density", b"phase", b"pressure"):
+        if raw.find(b"SCALARS " + name, at) < 0:
+            continue
+        i = raw.index(b"LOOKUP_TABLE default\n", raw.index(b"SCALARS " + name, at)) + len(b"LOOKUP_TABLE default\n")
+        scal[name.decode()] = np.frombuffer(raw[i:i + 4 * n], dtype=">f4")
+        at = i + 4 * n
+    vel, at = block(b"VECTORS velocity", 3 * n, at)
+    assert raw[at:] == b"\n"
+    assert np.array_equal(verts.reshape(n, 2)[:, 0], np.ones(n)) and np.array_equal(verts.reshape(n, 2)[:, 1],
+                                                                                    np.arange(n))
+    return n, pts.reshape(n, 3), vel.reshape(n, 3), scal
+
+
+def test_vtk_writer_header_and_payload(tmp_path):
+    """io test VtkHeaderAndSize (tests/test_io.cpp:21-32 of the reference),
+    plus every value read back from the binary payload."""
+    p = cs.make_block((0, 0, 0), (0.03, 0.02, 0.01), 0.01, cs.Phase.Liquid, 70.8, 20.3)
+    assert len(p["mass"]) == 6
+    p["velocity"] = np.arange(18, dtype=np.float32).reshape(6, 3) * 0.5
+    path = tmp_path / "block.vtk"
+    cs.write_vtk(str(path), p, np.full(6, 1e5))
+    text = path.read_bytes()
+    assert b"POINTS 6 float" in text and b"SCALARS pressure float 1" in text and b"VECTORS velocity float" in text
+    n, pts, vel, scal = _read_vtk(path)
+    assert n == 6
+    assert np.array_equal(pts, p["position"].astype(np.float32))
+    assert np.array_equal(vel, p["velocity"])
+    assert np.array_equal(scal["temperature"], p["temperature"]) and np.array_equal(scal["mass"], p["mass"])
+    assert np.array_equal(scal["density"], p["density"]) and np.array_equal(scal["phase"], np.zeros(6))
+    assert np.array_equal(scal["pressure"], np.full(6, 1e5, np.float32))
+    cs.write_vtk(str(path), p)  # no pressure: the section is left out
+    _, _, _, scal = _read_vtk(path)
+    assert "pressure" not in scal
+
+
+def test_json_frame_filters_walls(tmp_path):
+    """io test JsonFrameFiltersWalls (tests/test_io.cpp:34-46 of the reference)."""
+    p = cs.make_block((0, 0, 0), (0.02, 0.01, 0.01), 0.01, cs.Phase.Liquid, 1000.0, 300.0)
+    wall = {"position": [[1, 1, 1]], "mass": [1.0], "density": [1000.0], "temperature": [300.0], "phase": [2]}
+    both = {k: np.concatenate([np.asarray(p[k]), np.asarray(wall[k], dtype=np.asarray(p[k]).dtype)])
+            for k in wall}
+    fr = cs.make_frame(both, None, 0.5, 42)
+    path = tmp_path / "frame.json"
+    cs.write_json_frame(str(path), fr, include_walls=False)
+    s = path.read_text()
+    assert '"step":42' in s and '"n":2' in s and '"phase":[0,0]' in s and '"temperature":[300,300]' in s
+    d = json.loads(s)
+    assert d["time"] == 0.5 and len(d["position"]) == 6 and d["pressure"] == [0, 0]
+    cs.write_json_frame(str(path), fr, include_walls=True)
+    d = json.loads(path.read_text())
+    assert d["n"] == 3 and d["phase"] == [0, 0, 2] and d["position"][-3:] == [1, 1, 1]
+
+
+def test_json_numbers_use_six_significant_digits(tmp_path):
+    rng = np.random.default_rng(5)
+    n = 200
+    x = (rng.standard_normal((n, 3)) * 10.0 ** rng.integers(-8, 8, (n, 1))).astype(np.float32)
+    T = (rng.random(n) * 400).astype(np.float32)
+    T[3] = np.nan  # non-finite values are written as 0
+    parts = {"position": x, "mass": np.ones(n), "density": np.ones(n), "temperature": T,
+             "phase": np.zeros(n, np.uint8), "velocity": rng.standard_normal((n, 3))}
+    fr = cs.make_frame(parts, np.linspace(-1e5, 1e5, n), 1.0 / 3.0, 7)
+    path = tmp_path / "f.json"
+    cs.write_json_frame(str(path), fr)
+    d = json.loads(path.read_text())
+    assert d["time"] == float("%.9g" % (1.0 / 3.0))
+    assert d["position"] == [float("%.6g" % v) for v in x.ravel().astype(np.float64)]
+    assert d["temperature"][3] == 0 and d["temperature"][4] == float("%.6g" % float(T[4]))
+    speed = np.linalg.norm(np.asarray(parts["velocity"], np.float32), axis=1)
+    assert np.allclose(d["speed"], speed, rtol=1e-5)
+
+
+def test_particle_columns_reject_bad_shapes():
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    p = cs.make_block((0, 0, 0), (0.02, 0.01, 0.01), 0.01, cs.Phase.Liquid, 1000.0, 300.0)
+    with pytest.raises(ValueError):
+        cs.write_vtk("/dev/null", dict(p, mass=p["mass"][:-1]))
+    with pytest.raises(ValueError):
+        cs.write_vtk("/dev/null", dict(p, phase=np.full(len(p["mass"]), 7, np.uint8)))
+    with pytest.raises(ValueError):
+        cs.write_vtk("/dev/null", dict(p, position=p["position"][:, :2]))
+    assert ln2.T_sat > 0
+
+
+def test_mesh_tank_generator_matches_the_analytic_box(tmp_path):
+    """A closed triangle mesh of a box fills like the analytic BoxTank: the same
+    lattice nodes classified the same way (mesh distances from the
+    point-triangle query, the sign from the winding number)."""
+    verts = [(-1, -1, -1), (1, -1, -1), (1, 1, -1), (-1, 1, -1), (-1, -1, 1), (1, -1, 1), (1, 1, 1), (-1, 1, 1)]
+    faces = [(1, 3, 2), (1, 4, 3), (5, 6, 7), (5, 7, 8), (1, 2, 6), (1, 6, 5), (2, 3, 7), (2, 7, 6),
+             (3, 4, 8), (3, 8, 7), (4, 1, 5), (4, 5, 8)]
+    path = tmp_path / "box.obj"
+    path.write_text("# a cube\n" + "".join(f"v {a} {b} {c}\n" for a, b, c in verts) +
+                    "".join(f"f {a}/1/1 {b}/2/2 {c}/3/3\n" for a, b, c in faces))
+    mesh = cs.MeshTank(str(path), scale=0.02)
+    box = cs.BoxTank(0.04, 0.04, 0.04)
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    fill = cs.FillSpec()
+    fill.fill_fraction = 0.4
+    a = cs.tank_particles(mesh, ln2, 0.004, fill)
+    b = cs.tank_particles(box, ln2, 0.004, fill)
+    for k in ("position", "phase", "mass", "temperature", "flags", "id"):
+        assert np.array_equal(a[k], b[k]), k
+    assert np.allclose(a["normal"], b["normal"], atol=1e-6)
+    assert mesh.volume() == pytest.approx(box.volume())
+
+
+def test_obj_reader_rejects_bad_files(tmp_path):
+    p = tmp_path / "bad.obj"
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n")
+    with pytest.raises(Exception):
+        cs.MeshTank(str(p))
+    p.write_text("v 0 0 0\nv 1 0 0\n")
+    with pytest.raises(Exception):
+        cs.MeshTank(str(p))
+    p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf -4 -3 -2 -1\n")  # a quad by relative indices, fanned
+    assert cs.MeshTank(str(p)).num_triangles == 2
