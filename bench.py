@@ -362,6 +362,9 @@ def main():
                     help="c4: only the batched-ensemble comparison (64 tanks), reported as the main line")
     ap.add_argument("--dx", type=float, default=None, help="lattice spacing override (dam_break, c1, c3)")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--arith", default="fast", choices=["fast", "exact"],
+                    help="field arithmetic of the neighbour passes for the timed steps and e2e: fast (contracted, "
+                         "within 1e-5 of the reference) or exact (the reference's IEEE sequence, bit-identical)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=50)
     ap.add_argument("--batched-steps", type=int, default=100,
@@ -418,7 +421,9 @@ def main():
     device = local
 
     L = cabi.load()
+    arith = cs.FieldArithmetic.Fast if args.arith == "fast" else cs.FieldArithmetic.Exact
     solver = cs.Solver(cfg, fluid, device)
+    solver.field_arithmetic = arith
     load(solver, p, lo, hi)
     stream = torch.cuda.ExternalStream(solver.stream_handle, device=device)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=device)
@@ -452,12 +457,29 @@ def main():
     value = world * n_total * args.steps / (max_ms / 1e3)
     per_step = ctypes_int(L, "cryo_kernels_per_step", solver.handle)
 
-    e2e = roof = None
+    e2e = roof = other = None
     if rank == 0 and not args.only_timed:
         # ---- e2e through the public API with host buffers
-        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, args.steps, device, stream, flush, args.warmup)
+        e2e = e2e_run(cs, cfg, fluid, p, lo, hi, args.steps, device, stream, flush, args.warmup, arith)
         # ---- roofline of the dominant kernel (profiled run, CUDA events per kernel)
-        roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label)
+        roof = roofline(cs, cabi, L, cfg, fluid, p, lo, hi, args.profile_steps, n_fluid, n_wall, has_vapor, label,
+                        arith)
+        # ---- the same timed steps in the other field arithmetic
+        other_arith = cs.FieldArithmetic.Exact if args.arith == "fast" else cs.FieldArithmetic.Fast
+        solver.field_arithmetic = other_arith
+        solver.run_steps(args.warmup)
+        torch.cuda.synchronize()
+        ms_o = 0.0
+        with torch.cuda.stream(stream):
+            for k in range(args.steps):
+                flush.zero_()
+                starts[k].record(stream)
+                solver.step()
+                ends[k].record(stream)
+        torch.cuda.synchronize()
+        ms_o = sum(s_.elapsed_time(e_) for s_, e_ in zip(starts, ends))
+        other = {"field_arithmetic": "exact" if args.arith == "fast" else "fast",
+                 "value": n_total * args.steps / (ms_o / 1e3), "ms_per_step": ms_o / args.steps}
 
     # ---- batched ensemble (64 tanks): tanks sharded over ranks, no collective in the step
     batched = None
@@ -519,6 +541,8 @@ def main():
             "vs_baseline": None, "dtype": "f32 fields, f64 reductions", "data": "synthetic",
             "config": config_block(label, n_total, n_fluid, n_wall, world),
             "particles_after": int(n_now),
+            "field_arithmetic": args.arith,
+            "other_arithmetic": other,
             "timing": {"l2": "flushed between timed steps (256 MiB memset outside the events)",
                        "execution": "CUDA graph per step"},
             "per_gpu": value / world,
@@ -589,7 +613,7 @@ def ctypes_int(L, fn, handle):
     return v.value
 
 
-def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3):
+def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, arith=None):
     """Public-API run with host buffers: the state upload, then per step the
     frame-motion input (host->device) and the diagnostics (device->host), then
     the state download.  Device-timed per step with L2 flushed between steps.
@@ -598,6 +622,8 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3):
     the same-sized state reuses them, as a loop of runs on one Solver does."""
     import torch
     solver = cs.Solver(cfg, fluid, device)
+    if arith is not None:
+        solver.field_arithmetic = arith
     x = np.ascontiguousarray(p["position"], np.float64)
     arrays = [x, p["mass"].astype(np.float64), p["density"].astype(np.float64), p["temperature"].astype(np.float64)]
     state_in = sum(a.nbytes for a in arrays) + p["phase"].nbytes + p["normal"].nbytes + p["flags"].nbytes
@@ -867,10 +893,12 @@ def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
     }
 
 
-def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vapor, label):
+def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vapor, label, arith=None):
     import ctypes as C
     import cryo_roofline as RF
     solver = cs.Solver(cfg, fluid)
+    if arith is not None:
+        solver.field_arithmetic = arith
     load(solver, p, lo, hi)
     solver.run_steps(3)
     h = C.c_void_p(solver.handle)

@@ -320,6 +320,19 @@ int cryo_damp_velocities(cryo_ctx* ctx, float factor);
 int cryo_maneuver_evaluate(int n, const double* time, const float* acc, const float* omega, double t,
                            float* a3, float* w3, float* wdot3);
 
+/* Field arithmetic of the neighbour passes (no counterpart in the
+ * reference's API; its two builds differ exactly this way).  EXACT (the
+ * default): the reference's IEEE single-precision operation sequence, no FMA
+ * contraction, IEEE division and square root -- fields bit-identical to its
+ * CPU build.  FAST: the same passes with FMA contraction and approximate
+ * (2 ulp) division and square root, as the reference's own CUDA build
+ * contracts; every pass's fields stay within 1e-5 (normwise, relative) of
+ * EXACT.  Keys, sort and neighbour lists are bit-exact in both.  The
+ * differentiated window (cryo_adj_*) needs EXACT. */
+enum { CRYO_ARITH_EXACT = 0, CRYO_ARITH_FAST = 1 };
+int cryo_set_field_arithmetic(cryo_ctx* ctx, int mode);
+int cryo_field_arithmetic(cryo_ctx* ctx, int* mode);
+
 /* Solver::probe_pressure (sph_solver.cu:738-748): np points (np*3 floats). */
 int cryo_probe_pressure(cryo_ctx* ctx, const float* points, int np, float* out);
 

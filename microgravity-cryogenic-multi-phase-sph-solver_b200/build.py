@@ -32,6 +32,10 @@ NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
     "--extended-lambda", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I" + INCLUDE,
 ]
+# cryo_physics.cu again for the fast field arithmetic: FMA contraction and
+# approximate division / square root (denormals kept).
+FAST_FIELD_FLAGS = [f for f in NVCC_FLAGS if f != "-fmad=false"] + [
+    "-fmad=true", "-prec-div=false", "-prec-sqrt=false", "-DCRYO_FIELD_NS=fast"]
 LIB = os.path.join(HERE, "libcryosph_b200.so")
 
 
@@ -63,6 +67,12 @@ def build_lib(verbose=False):
         objs.append(o)
         if _newer(o, [s] + hdrs):
             jobs.append([NVCC] + NVCC_FLAGS + ["-c", s, "-o", o])
+    # the neighbour passes a second time, contracted (namespace cryo::fast)
+    s = os.path.join(CSRC, "cryo_physics.cu")
+    o = os.path.join(BUILD, "cryo_physics_fast.cu.o")
+    objs.append(o)
+    if _newer(o, [s] + hdrs):
+        jobs.append([NVCC] + FAST_FIELD_FLAGS + ["-c", s, "-o", o])
     with ThreadPoolExecutor(max_workers=min(8, max(1, len(jobs)))) as ex:
         for r in ex.map(_run, jobs):
             if verbose and r.stderr:

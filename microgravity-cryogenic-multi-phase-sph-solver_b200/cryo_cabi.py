@@ -17,6 +17,7 @@ LIB_NAME = "libcryosph_b200.so"
 
 # status codes
 CRYO_OK, CRYO_EINVAL, CRYO_ERANGE, CRYO_ERUNTIME, CRYO_ECUDA, CRYO_EDEVICE = range(6)
+CRYO_ARITH_EXACT, CRYO_ARITH_FAST = 0, 1
 # phases / flags
 LIQUID, VAPOR, WALL, DEAD = 0, 1, 2, 3
 FLAG_HEATED, FLAG_SOURCE, FLAG_TARGET_VAPOR, FLAG_DYING = 1, 2, 4, 8
@@ -288,6 +289,8 @@ def load(path=None):
         "cryo_load_state": (i, [vp, vp, C.c_size_t]),
         "cryo_set_graph_mode": (i, [vp, i]),
         "cryo_set_neighbor_mode": (i, [vp, i]),
+        "cryo_set_field_arithmetic": (i, [vp, i]),
+        "cryo_field_arithmetic": (i, [vp, ip]),
         "cryo_adj_forward": (i, [vp, C.c_longlong, i, vp]),
         "cryo_adj_backward": (i, [vp, vp, vp, vp]),
         "cryo_adj_seed_state": (i, [vp, i, vp, C.c_size_t]),
@@ -385,6 +388,10 @@ class Context:
 
     def set_neighbor_mode(self, use_lists):
         self.check(self.L.cryo_set_neighbor_mode(self.h, int(bool(use_lists))))
+
+    def set_field_arithmetic(self, mode):
+        """CRYO_ARITH_EXACT (0, the reference's IEEE sequence) or CRYO_ARITH_FAST (1)."""
+        self.check(self.L.cryo_set_field_arithmetic(self.h, int(mode)))
 
     def device_status(self):
         st = C.c_uint()

@@ -229,20 +229,20 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done, bool 
   const View V = view(s);
   if (maxima_reset) LAUNCH(k_begin_step, 1, 1, P, V, BEGIN_RATES);
   if (!density_done) {
-    LAUNCH(k_density, G, kBlock, P, V, 1);
+    FIELD_LAUNCH(k_density, G, kBlock, P, V, 1);
     slab_point(SLAB_HALO, s);
   }
-  LAUNCH(k_wall, G, kBlock, P, V);
+  FIELD_LAUNCH(k_wall, G, kBlock, P, V);
   slab_point(SLAB_HALO, s);
-  if (tape) LAUNCH(k_interface<1>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
-  else LAUNCH(k_interface<0>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
+  if (tape) FIELD_LAUNCH(k_interface<1>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
+  else FIELD_LAUNCH(k_interface<0>, G, kBlock, P, V, reduce(), P.thermal ? 1 : 0);
   slab_point(P.thermal ? SLAB_HEAT : SLAB_HALO, s);
   if (P.sps) {
-    LAUNCH(k_sps, G, kBlock, P, V);
+    FIELD_LAUNCH(k_sps, G, kBlock, P, V);
     slab_point(SLAB_HALO, s);
   }
   if (P.csf_active && P.csf_smooth) {
-    LAUNCH(k_smooth_normals, G, kBlock, P, V);
+    FIELD_LAUNCH(k_smooth_normals, G, kBlock, P, V);
     slab_point(SLAB_HALO, s);
   }
   const int GF = forces_blocks();
@@ -253,13 +253,13 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done, bool 
   if (P.thermal) what |= FORCE_THERMAL;
   if (tape) {  // the recomputation of a differentiated window: variants that also store their sums
     switch (what) {
-      case FORCE_BASE: LAUNCH(k_forces_t<FORCE_BASE | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
+      case FORCE_BASE: FIELD_LAUNCH(k_forces_t<FORCE_BASE | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
       case FORCE_BASE | FORCE_THERMAL:
-        LAUNCH(k_forces_t<FORCE_BASE | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
+        FIELD_LAUNCH(k_forces_t<FORCE_BASE | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
         break;
-      case FORCE_BASE | FORCE_CSF: LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
+      case FORCE_BASE | FORCE_CSF: FIELD_LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what); break;
       case FORCE_BASE | FORCE_CSF | FORCE_THERMAL:
-        LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
+        FIELD_LAUNCH(k_forces_t<FORCE_BASE | FORCE_CSF | FORCE_THERMAL | FORCE_TAPE>, GF, FORCES_BLOCK, P, V, what);
         break;
       default: throw std::runtime_error("internal: no taped force pass for this configuration");
     }
@@ -267,7 +267,7 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done, bool 
   }
   switch (what) {
 #define FORCES_CASE(W) \
-  case W: LAUNCH(k_forces_t<W>, GF, FORCES_BLOCK, P, V, W); break;
+  case W: FIELD_LAUNCH(k_forces_t<W>, GF, FORCES_BLOCK, P, V, W); break;
     FORCES_CASE(FORCE_BASE)
     FORCES_CASE(FORCE_BASE | FORCE_THERMAL)
     FORCES_CASE(FORCE_BASE | FORCE_DRHO)
@@ -281,7 +281,7 @@ void cryo_ctx::evaluate_rates(int s, bool maxima_reset, bool density_done, bool 
     FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO)
     FORCES_CASE(FORCE_BASE | FORCE_CSF | FORCE_DRHO | FORCE_THERMAL)
 #undef FORCES_CASE
-    default: LAUNCH(k_forces_t<-1>, GF, FORCES_BLOCK, P, V, what);
+    default: FIELD_LAUNCH(k_forces_t<-1>, GF, FORCES_BLOCK, P, V, what);
   }
   slab_point(SLAB_FORCES, s);
 }
@@ -320,9 +320,9 @@ void cryo_ctx::enqueue_step(int s, const StepTape* tape) {
   LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   slab_point(SLAB_HALO, d);
   if (P.shift_strength > 0.0f) {
-    LAUNCH(k_shift_compute, G, kBlock, P, V);
+    FIELD_LAUNCH(k_shift_compute, G, kBlock, P, V);
     slab_point(SLAB_HALO, d);
-    LAUNCH(k_shift_apply, G, kBlock, P, V);
+    FIELD_LAUNCH(k_shift_apply, G, kBlock, P, V);
     slab_point(SLAB_HALO, d);
     // the phase-change passes search around the shifted positions
     // (old cell table), as for_each_neighbor does in the reference
@@ -402,7 +402,7 @@ void cryo_ctx::ensure_initialized() {
   slab_point(SLAB_SORTED, cur);
   const int G = grid_blocks();
   if (cfg.normalize_initial_masses) {
-    LAUNCH(k_normalize_masses, G, kBlock, P, view(cur));
+    FIELD_LAUNCH(k_normalize_masses, G, kBlock, P, view(cur));
     slab_point(SLAB_HALO, cur);
   }
   evaluate_rates(cur, true, false);
@@ -1284,7 +1284,7 @@ int cryo_probe_pressure(cryo_ctx* c, const float* pts, int np, float* out) {
     CK(cudaMallocAsync(&d, (size_t)np * 4 * sizeof(float), c->stream));
     CK(cudaMemcpyAsync(d, pts, (size_t)np * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     const int blocks = std::max(1, std::min((np + 127) / 128, c->sm_count * 8));
-    k_probe<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
+    FIELD_KERNEL(c, k_probe)<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
     LAUNCH_CHECK();
     CK(cudaMemcpyAsync(out, d + 3 * (size_t)np, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaFreeAsync(d, c->stream));
@@ -1347,7 +1347,7 @@ int cryo_probe_pressure_noalloc(cryo_ctx* c, const float* pts, int np, float* ou
     }
     CK(cudaMemcpyAsync(d, pts, (size_t)np * 3 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
     const int blocks = std::max(1, std::min((np + 127) / 128, c->sm_count * 8));
-    k_probe<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
+    FIELD_KERNEL(c, k_probe)<<<blocks, 128, 0, c->stream>>>(c->P, c->view(c->cur), d, np, d + 3 * (size_t)np);
     LAUNCH_CHECK();
     CK(cudaMemcpyAsync(out, d + 3 * (size_t)np, (size_t)np * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     c->sync();
@@ -1382,7 +1382,7 @@ int cryo_pass(cryo_ctx* c, int pass) {
     switch (pass) {  // passes that read View::aux get it from the current fields
       case CRYO_PASS_INTERFACE: case CRYO_PASS_TRANSPORT: case CRYO_PASS_SPS: case CRYO_PASS_MOMENTUM:
       case CRYO_PASS_CSF: case CRYO_PASS_AKINCI: case CRYO_PASS_DENSITY_RATE: case CRYO_PASS_THERMAL:
-        k_aux<<<G, kBlock, 0, st>>>(P, V);
+        FIELD_KERNEL(c, k_aux)<<<G, kBlock, 0, st>>>(P, V);
         LAUNCH_CHECK();
         break;
       default: break;
@@ -1395,33 +1395,33 @@ int cryo_pass(cryo_ctx* c, int pass) {
         c->grid_build(c->cur);
         c->cur = 1 - c->cur;
         break;
-      case CRYO_PASS_DENSITY: k_density<<<G, kBlock, 0, st>>>(P, V, 0); break;
-      case CRYO_PASS_NORMALIZE_MASSES: k_normalize_masses<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_EOS: k_eos<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_WALL_BOUNDARY: k_wall<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_INTERFACE: k_interface<0><<<G, kBlock, 0, st>>>(P, V, R, 0); break;
-      case CRYO_PASS_TRANSPORT: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_TRANSPORT); break;
-      case CRYO_PASS_SPS: k_sps<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_MOMENTUM: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_MOMENTUM); break;
-      case CRYO_PASS_SMOOTH_NORMALS: k_smooth_normals<<<G, kBlock, 0, st>>>(P, V); break;
-      case CRYO_PASS_CSF: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_CSF); break;
-      case CRYO_PASS_AKINCI: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_AKINCI); break;
-      case CRYO_PASS_DENSITY_RATE: k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_DRHO); break;
+      case CRYO_PASS_DENSITY: FIELD_KERNEL(c, k_density)<<<G, kBlock, 0, st>>>(P, V, 0); break;
+      case CRYO_PASS_NORMALIZE_MASSES: FIELD_KERNEL(c, k_normalize_masses)<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_EOS: FIELD_KERNEL(c, k_eos)<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_WALL_BOUNDARY: FIELD_KERNEL(c, k_wall)<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_INTERFACE: FIELD_KERNEL(c, k_interface<0>)<<<G, kBlock, 0, st>>>(P, V, R, 0); break;
+      case CRYO_PASS_TRANSPORT: FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_TRANSPORT); break;
+      case CRYO_PASS_SPS: FIELD_KERNEL(c, k_sps)<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_MOMENTUM: FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_MOMENTUM); break;
+      case CRYO_PASS_SMOOTH_NORMALS: FIELD_KERNEL(c, k_smooth_normals)<<<G, kBlock, 0, st>>>(P, V); break;
+      case CRYO_PASS_CSF: FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_CSF); break;
+      case CRYO_PASS_AKINCI: FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_AKINCI); break;
+      case CRYO_PASS_DENSITY_RATE: FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_DRHO); break;
       case CRYO_PASS_THERMAL:
         k_heat_norm<<<G, kBlock, 0, st>>>(P, V, R);
         LAUNCH_CHECK();
-        k_forces_t<-1><<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
+        FIELD_KERNEL(c, k_forces_t<-1>)<<<c->forces_blocks(), FORCES_BLOCK, 0, st>>>(P, V, FORCE_THERMAL_ALWAYS);
         break;
       case CRYO_PASS_MAXIMA:
         k_begin_step<<<1, 1, 0, st>>>(P, V, BEGIN_RATES);
         LAUNCH_CHECK();
-        k_maxima<<<G, kBlock, 0, st>>>(P, V);
+        FIELD_KERNEL(c, k_maxima)<<<G, kBlock, 0, st>>>(P, V);
         break;
       case CRYO_PASS_KICK: k_kick<<<G, kBlock, 0, st>>>(P, V, 0); break;
       case CRYO_PASS_SHIFTING:
-        k_shift_compute<<<G, kBlock, 0, st>>>(P, V);
+        FIELD_KERNEL(c, k_shift_compute)<<<G, kBlock, 0, st>>>(P, V);
         LAUNCH_CHECK();
-        k_shift_apply<<<G, kBlock, 0, st>>>(P, V);
+        FIELD_KERNEL(c, k_shift_apply)<<<G, kBlock, 0, st>>>(P, V);
         LAUNCH_CHECK();
         if (P.use_lists) k_build_lists<<<G, kBlock, 0, st>>>(P, V, R, LISTS_ONLY);
         break;
@@ -1753,6 +1753,20 @@ int cryo_set_graph_mode(cryo_ctx* c, int enable) {
     c->graph_mode = enable != 0;
     c->invalidate_graphs();
   });
+}
+
+int cryo_set_field_arithmetic(cryo_ctx* c, int mode) {
+  return guard(c, [&] {
+    if (mode != CRYO_ARITH_EXACT && mode != CRYO_ARITH_FAST)
+      throw std::invalid_argument("cryo_set_field_arithmetic: mode must be CRYO_ARITH_EXACT or CRYO_ARITH_FAST");
+    c->sync();
+    c->fast_fields = mode == CRYO_ARITH_FAST;
+    c->invalidate_graphs();
+  });
+}
+
+int cryo_field_arithmetic(cryo_ctx* c, int* mode) {
+  return guard(c, [&] { *mode = c->fast_fields ? CRYO_ARITH_FAST : CRYO_ARITH_EXACT; });
 }
 
 int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {

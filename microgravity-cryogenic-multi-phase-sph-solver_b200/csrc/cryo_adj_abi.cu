@@ -97,6 +97,7 @@ void adj_check_config(const cryo_ctx* c) {
   const cryo_config_t& g = c->cfg;
   const Params& P = c->P;
   auto no = [](const char* what) { throw std::invalid_argument(std::string("adjoint: not supported: ") + what); };
+  if (c->fast_fields) no("the fast field arithmetic (the reverse passes differentiate the exact sequence)");
   if (!(P.fixed_dt > 0.0f)) no("adaptive time step (set fixed_dt)");
   if (!(g.sound_speed > 0 || g.velocity_scale > 0)) no("sound speed derived from the surface tension (set sound_speed)");
   if (P.density_mode != CRYO_DENSITY_SUMMATION) no("continuity density");

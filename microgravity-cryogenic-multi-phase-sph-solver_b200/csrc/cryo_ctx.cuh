@@ -51,6 +51,17 @@ struct CudaError : std::runtime_error {
     this->after_launch();                        \
   } while (0)
 
+// A kernel of cryo_physics.cu in the context's field arithmetic (exact: the
+// reference's IEEE sequence; fast: contracted, see cryo_kernels.cuh).
+#define FIELD_KERNEL(ctx, K) ((ctx)->fast_fields ? &fast::K : &exact::K)
+#define FIELD_LAUNCH(K, G, B, ...)                  \
+  do {                                              \
+    if (this->fast_fields)                          \
+      LAUNCH(fast::K, G, B, __VA_ARGS__);           \
+    else                                            \
+      LAUNCH(exact::K, G, B, __VA_ARGS__);          \
+  } while (0)
+
 struct Persist {
   float4 *xp = nullptr, *vT = nullptr, *vt = nullptr, *nrm = nullptr, *mrps = nullptr;
   uint32_t* id = nullptr;
@@ -201,6 +212,7 @@ struct cryo_ctx {
   bool graph_valid[2] = {false, false};
   cudaGraphExec_t graph[2] = {nullptr, nullptr};
   bool use_lists = true;
+  bool fast_fields = false;  // field arithmetic of the neighbour passes (cryo_set_field_arithmetic)
 
   // launch accounting / profiling
   long long launch_counter = 0;
@@ -255,6 +267,8 @@ struct cryo_ctx {
     std::string name(raw);
     const size_t lt = name.find('<');
     if (lt != std::string::npos) name = name.substr(0, lt);
+    const size_t ns = name.rfind("::");
+    if (ns != std::string::npos) name = name.substr(ns + 2);
     if (name == "k_forces_t") name = "k_forces";
     int k = 0;
     while (k < (int)prof_names.size() && prof_names[k] != name) ++k;

@@ -140,24 +140,41 @@ __global__ void k_build_lists(Params P, View V, Reduce R, int mode);
 __global__ void k_nbr_count(Params P, View V, int* counts);
 __global__ void k_nbr_fill(Params P, View V, const long long* offsets, int* list);
 
-// physics (cryo_physics.cu)
-__global__ void k_density(Params P, View V, int fuse_eos);
-__global__ void k_aux(Params P, View V);
-__global__ void k_normalize_masses(Params P, View V);
-__global__ void k_eos(Params P, View V);
-__global__ void k_wall(Params P, View V);
-// heat_sum: 0 none, 1 when thermal is on (step), 2 always (operator call)
-// TAPE: also store the sums into V.tape (the recomputation of a differentiated window).
-template <int TAPE>
-__global__ void k_interface(Params P, View V, Reduce R, int heat_sum);
-__global__ void k_sps(Params P, View V);
-__global__ void k_smooth_normals(Params P, View V);
-// Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
+// physics (cryo_physics.cu).  Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
 enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8, FORCE_DRHO = 16,
        FORCE_THERMAL = 32, FORCE_MAXIMA = 64, FORCE_THERMAL_ALWAYS = 128,
        FORCE_TAPE = 256 };  // compile-time only: also store the sums into V.tape
-template <int WHAT>
-__global__ void k_forces_t(Params P, View V, int what_rt);
+// cryo_physics.cu is compiled twice.  namespace exact: the reference's IEEE
+// single-precision operation sequence (no FMA contraction, IEEE division and
+// square root), bit-identical to its CPU build.  namespace fast: the same
+// source with FMA contraction and the approximate (2 ulp) division and square
+// root, as the reference's own CUDA build contracts; fields then agree with
+// the exact sequence to ~1e-6 relative per pass.  The neighbour lists, keys
+// and sort are not in that file, so they stay bit-exact in both.
+#define CRYO_FIELD_KERNELS                                                           \
+  __global__ void k_density(Params P, View V, int fuse_eos);                        \
+  __global__ void k_aux(Params P, View V);                                          \
+  __global__ void k_normalize_masses(Params P, View V);                             \
+  __global__ void k_eos(Params P, View V);                                          \
+  __global__ void k_wall(Params P, View V);                                         \
+  template <int TAPE>                                                               \
+  __global__ void k_interface(Params P, View V, Reduce R, int heat_sum);            \
+  __global__ void k_sps(Params P, View V);                                          \
+  __global__ void k_smooth_normals(Params P, View V);                               \
+  template <int WHAT>                                                               \
+  __global__ void k_forces_t(Params P, View V, int what_rt);                        \
+  __global__ void k_maxima(Params P, View V);                                       \
+  __global__ void k_shift_compute(Params P, View V);                                \
+  __global__ void k_shift_apply(Params P, View V);                                  \
+  __global__ void k_probe(Params P, View V, const float* pts, int np, float* out);
+namespace exact {
+CRYO_FIELD_KERNELS
+}
+namespace fast {
+CRYO_FIELD_KERNELS
+}
+// heat_sum of k_interface: 0 none, 1 when thermal is on (step), 2 always (operator call)
+// TAPE: also store the sums into V.tape (the recomputation of a differentiated window).
 constexpr int FORCE_BASE = FORCE_TRANSPORT | FORCE_MOMENTUM | FORCE_MAXIMA;
 // Block shape of the force pass.  The pass is bound by the latency of each
 // particle's neighbour chain, so what matters is how many particles are in
@@ -194,9 +211,6 @@ constexpr int forces_min_blocks(int what) {
 #ifndef LIST_MIN_BLOCKS
 #define LIST_MIN_BLOCKS 4
 #endif
-__global__ void k_shift_compute(Params P, View V);
-__global__ void k_shift_apply(Params P, View V);
-__global__ void k_probe(Params P, View V, const float* pts, int np, float* out);
 
 // integrator + phase change (cryo_phase.cu)
 __global__ void k_kick_drift(Params P, View V, int continuity, int tvf);
@@ -216,7 +230,6 @@ __global__ void k_scale_velocities(View V, float factor, int scale_vmax);
 enum { BEGIN_STEP = 0, BEGIN_RATES = 1 };
 __global__ void k_begin_step(Params P, View V, int mode);
 __global__ void k_heat_norm(Params P, View V, Reduce R);
-__global__ void k_maxima(Params P, View V);
 // The ullage pressure and saturation temperature from the phase sums
 // (sph_solver.cu:586-607).
 __device__ inline void saturation_update(const Params& P, DynState* d, bool closed, double m_liq, double m_vap,

@@ -4,7 +4,13 @@
 // 27-cell order (for_each_neighbor in cryo_common.cuh).
 #include "cryo_kernels.cuh"
 
+// exact (default) or fast: see CRYO_FIELD_KERNELS in cryo_kernels.cuh
+#ifndef CRYO_FIELD_NS
+#define CRYO_FIELD_NS exact
+#endif
+
 namespace cryo {
+namespace CRYO_FIELD_NS {
 
 #define PARTICLE_LOOP(i, n) \
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < (n); i += gridDim.x * blockDim.x)
@@ -815,4 +821,5 @@ __global__ void k_probe(Params P, View V, const float* __restrict__ pts, int np,
   }
 }
 
+}  // namespace CRYO_FIELD_NS
 }  // namespace cryo

@@ -215,6 +215,9 @@ PYBIND11_MODULE(CryoSPH, m) {
       .value("NormalRotation", WettingModel::NormalRotation)
       .value("ContactLineForce", WettingModel::ContactLineForce)
       .value("Both", WettingModel::Both);
+  py::enum_<FieldArithmetic>(m, "FieldArithmetic")
+      .value("Exact", FieldArithmetic::Exact)
+      .value("Fast", FieldArithmetic::Fast);
   py::enum_<TelemetryMode>(m, "TelemetryMode")
       .value("AsyncCopy", TelemetryMode::AsyncCopy)
       .value("ZeroCopy", TelemetryMode::ZeroCopy);
@@ -579,6 +582,9 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property_readonly(
           "handle", [](const Solver& s) { return reinterpret_cast<std::uintptr_t>(s.handle()); },
           "The cryo_ctx* behind this solver, for direct C-ABI calls (include/cryosph_b200.h).")
+      .def_property("field_arithmetic", &Solver::field_arithmetic, &Solver::set_field_arithmetic,
+                    "Exact (default): the reference's IEEE operation sequence in the neighbour passes, bit-identical "
+                    "to its CPU build; Fast: FMA contraction and approximate division / square root, within 1e-5.")
       .def("set_graph_mode", &Solver::set_graph_mode, py::arg("enabled"),
            "Replay each step as a captured CUDA graph (default) or launch kernels one by one.")
       .def(

@@ -284,6 +284,7 @@ void load_obj(const std::string& path, std::vector<std::array<double, 3>>& verti
               std::vector<std::array<int, 3>>& triangles);
 
 enum class FillMode : int { Settled = 0, CentralBubble = 1, Full = 2 };
+enum class FieldArithmetic : int { Exact = CRYO_ARITH_EXACT, Fast = CRYO_ARITH_FAST };
 
 struct FillSpec {
   FillMode mode = FillMode::Settled;
@@ -377,6 +378,10 @@ class Solver {
   cryo_ctx* handle() const noexcept { return ctx_; }
   std::uintptr_t stream_handle() const;
   void set_graph_mode(bool on);
+  // Exact: the reference's IEEE operation sequence in the neighbour passes
+  // (bit-identical to its CPU build); Fast: contracted, within 1e-5 of it.
+  void set_field_arithmetic(FieldArithmetic mode);
+  FieldArithmetic field_arithmetic() const;
   std::vector<std::uint8_t> save_state() const;
   void load_state(const std::vector<std::uint8_t>& blob);
 

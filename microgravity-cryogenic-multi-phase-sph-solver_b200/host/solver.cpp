@@ -402,6 +402,12 @@ std::vector<real> Solver::probe_pressure(const std::vector<Vec3>& points) {
 
 std::uintptr_t Solver::stream_handle() const { return cryo_stream(ctx_); }
 void Solver::set_graph_mode(bool on) { check(cryo_set_graph_mode(ctx_, on ? 1 : 0)); }
+void Solver::set_field_arithmetic(FieldArithmetic mode) { check(cryo_set_field_arithmetic(ctx_, static_cast<int>(mode))); }
+FieldArithmetic Solver::field_arithmetic() const {
+  int m = 0;
+  check(cryo_field_arithmetic(ctx_, &m));
+  return static_cast<FieldArithmetic>(m);
+}
 
 std::vector<std::uint8_t> Solver::save_state() const {
   std::size_t bytes = 0;
