@@ -373,6 +373,9 @@ def main():
     ap.add_argument("--adjoint-steps", type=int, default=400,
                     help="steps of the differentiated LN2 boil-off window (0 = skip the adjoint leg)")
     ap.add_argument("--adjoint-every", type=int, default=20, help="checkpoint interval of the adjoint window")
+    ap.add_argument("--adjoint-fd64", type=int, default=0,
+                    help="run only the FP64 finite-difference check of the adjoint over a window of this many steps "
+                         "from the boil-off tank's initial lattice, and print its record")
     ap.add_argument("--only-adjoint", action="store_true",
                     help="run only the adjoint leg (LN2 boil-off window) and print its record; for profiler launch lists")
     ap.add_argument("--slabs", type=int, default=0,
@@ -380,6 +383,11 @@ def main():
     ap.add_argument("--slab-devices", default=None,
                     help="comma-separated device per slab (default: every slab on this rank's device)")
     ap.add_argument("--slab-steps", type=int, default=50, help="timed steps of the slab leg")
+    ap.add_argument("--side-force-steps", type=int, default=0,
+                    help="with --workload c3: steps of the manoeuvre run (side force against -M a; 0 = skip)")
+    ap.add_argument("--probe-steps", type=int, default=1000,
+                    help="steps of the dam break's probe-pressure series against the FP64 reference (0 = skip)")
+    ap.add_argument("--probe-dx", type=float, default=0.04, help="lattice spacing of the probe-series dam break")
     ap.add_argument("--only-timed", action="store_true",
                     help="run the timed steps only (no e2e, roofline or CPU legs); for profiler launch lists")
     args = ap.parse_args()
@@ -396,6 +404,11 @@ def main():
 
     import CryoSPH as cs
 
+    if args.adjoint_fd64 > 0:
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps({"adjoint_fd64": adjoint_fd64_run(cs, local, args.adjoint_fd64, args.adjoint_every)}))
+        return 0
     if args.only_adjoint:
         import torch
         torch.cuda.set_device(local)
@@ -489,7 +502,7 @@ def main():
         torch.cuda.empty_cache()
         all_tanks = c4_tanks(cs, count=args.batched_tanks)
         mine = cryo_shard.shard_of([tk["n"] for tk in all_tanks], rank, world)
-        b = batched_run(cs, [all_tanks[t] for t in mine], args.batched_steps, args.warmup, device)
+        b = batched_run(cs, [all_tanks[t] for t in mine], args.batched_steps, args.warmup, device, arith=arith)
         agg = torch.tensor([b["ms_per_step"], b["back_to_back_ms_per_step"], 0.0 if b["diagnostics_bit_identical"] else 1.0],
                            dtype=torch.float64, device=device)
         if dist:
@@ -528,6 +541,15 @@ def main():
         devs = [int(d) for d in args.slab_devices.split(",")] if args.slab_devices else [device] * args.slabs
         slabs = slab_run(cs, cfg, fluid, p, lo, hi, args.slabs, devs, args.slab_steps, label)
 
+    side = None
+    if rank == 0 and args.workload == "c3" and args.side_force_steps > 0:
+        side = side_force_run(cs, device, args.side_force_steps, arith, args.dx)
+
+    # the dam break's probe-pressure series against the reference's FP64 build
+    probes = None
+    if rank == 0 and world == 1 and args.probe_steps > 0 and not args.only_timed and args.workload == "dam_break":
+        probes = probe_series_run(cs, device, args.probe_dx, args.probe_steps, arith)
+
     # the adjoint leg last: its window holds several GB until it is released
     adjoint = None
     if rank == 0 and args.adjoint_steps > 0 and not args.only_timed:
@@ -555,6 +577,8 @@ def main():
             "batched": batched,
             "adjoint": adjoint,
             "slabs": slabs,
+            "probe_series": probes,
+            "side_force": side,
         }
         print(json.dumps(line))
     if dist:
@@ -579,7 +603,8 @@ def batched_main(args, cs, rank, world, local):
     if dist:
         dist.barrier()
     with Clocks(local) as clk:
-        b = batched_run(cs, [all_tanks[t] for t in mine], args.steps, args.warmup, local)
+        arith = cs.FieldArithmetic.Fast if args.arith == "fast" else cs.FieldArithmetic.Exact
+        b = batched_run(cs, [all_tanks[t] for t in mine], args.steps, args.warmup, local, arith=arith)
     agg = torch.tensor([b["ms_per_step"], b["back_to_back_ms_per_step"], 0.0 if b["diagnostics_bit_identical"] else 1.0],
                        dtype=torch.float64, device=local)
     if dist:
@@ -674,6 +699,119 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, a
             "steps": steps, "host_wall_ms": {k: round(v, 3) for k, v in host.items()},
             "timing": "CUDA events per step (host work inside), L2 flushed between steps; one untimed run of the "
                       "same sequence first"}
+
+
+# SPHERIC Test 2 pressure sensors (validation/spheric_test2/run.py:30-33,69-73
+# of the reference): four on the obstacle's front face, four on its top.
+def spheric_sensors(dx):
+    x_front, box_h, y = 0.744, 0.161, 0.403 / 2 - 0.176
+    offs = (0.021, 0.061, 0.101, 0.141)
+    return np.array([(x_front + 0.5 * dx, y, z) for z in offs] + [(x_front - o, y, box_h + 0.5 * dx) for o in offs],
+                    np.float32)
+
+
+def probe_series_run(cs, device, dx, steps, arith):
+    """The dam break's probe-pressure time series at the eight SPHERIC sensors,
+    every step, against the reference's FP64 build on the same inputs (and its
+    FP32 build, the single-precision noise floor).  The FP64 run's own time
+    steps differ, so its series is interpolated linearly to this run's step
+    times; a sample counts where both runs read the sensor wet.  Error per
+    sensor: max |p - p64| / max |p64| over the wet samples."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refpy
+    if not refpy.ref_available(fp64=True):
+        return None
+    label, cfg, fluid, p, lo, hi = workload("dam_break", cs, dx)
+    s = cs.Solver(cfg, fluid, device)
+    s.field_arithmetic = arith
+    load(s, p, lo, hi)
+    _, rcfg, rfluid, rp, rlo, rhi = ref_workload("dam_break", dx)
+    refs = {}
+    for name, fp64 in (("fp64", True), ("fp32", False)):
+        r = refpy.Ref(rcfg, rfluid, fp64=fp64)
+        r.set_threads(os.cpu_count() or 1)
+        r.set_particles(rp, rlo, rhi)
+        refs[name] = r
+    pts = spheric_sensors(dx)
+    series = {"ours": ([], []), "fp64": ([], []), "fp32": ([], [])}
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        s.step()
+        series["ours"][0].append(s.time)
+        series["ours"][1].append(s.probe_pressure(pts))
+        for name, r in refs.items():
+            r.step(1)
+            series[name][0].append(r.time()[0])
+            series[name][1].append(r.probe_pressure(pts))
+    wall = time.perf_counter() - t0
+
+    def err(name):
+        t, v = np.asarray(series[name][0]), np.asarray(series[name][1], np.float64)
+        t64, v64 = np.asarray(series["fp64"][0]), np.asarray(series["fp64"][1], np.float64)
+        out = []
+        for k in range(len(pts)):
+            ref_k = np.interp(t, t64, np.nan_to_num(v64[:, k], nan=np.inf))
+            wet = np.isfinite(v[:, k]) & np.isfinite(ref_k) & (t <= t64[-1])
+            if not wet.any():
+                out.append(None)
+                continue
+            scale = max(float(np.abs(ref_k[wet]).max()), 1e-30)
+            out.append(float(np.abs(v[wet, k] - ref_k[wet]).max() / scale))
+        return out
+
+    wet = np.isfinite(np.asarray(series["ours"][1])).mean(axis=0)
+    return {"workload": label, "steps": steps, "sensors": "P1-P4 front face, P5-P8 top (run.py:69-73)",
+            "field_arithmetic": "fast" if arith == cs.FieldArithmetic.Fast else "exact",
+            "t_end": float(series["ours"][0][-1]), "wet_fraction": [float(w) for w in wet],
+            "error_vs_fp64": err("ours"), "reference_fp32_error_vs_fp64": err("fp32"),
+            "peak_pressure_fp64": [float(np.nanmax(np.asarray(series["fp64"][1])[:, k]))
+                                   if np.isfinite(np.asarray(series["fp64"][1])[:, k]).any() else None
+                                   for k in range(len(pts))],
+            "wall_s": wall,
+            "note": "error = max |p - p_fp64| / max |p_fp64| over the samples where both read the sensor wet; "
+                    "the FP64 series interpolated to this run's step times"}
+
+
+def side_force_run(cs, device, steps, arith, dx=None):
+    """The LH2 sphere under its manoeuvre: a lateral (x) acceleration pulse of
+    0.05 m/s^2 over the first 0.5 s, then a slew ramped to 5 deg/s about the
+    tank centre (pitch, the y axis) over the next 0.5 s.  Every step the
+    diagnostics give the slosh force; over the pulse the impulse on the tank
+    is compared with -M a t (M the fluid mass), raw and corrected by the
+    liquid's own momentum change in the tank frame (impulse balance: the walls
+    take -M a t less what the liquid keeps as relative momentum)."""
+    label, cfg, fluid, p, lo, hi = workload("c3", cs, dx)
+    s = cs.Solver(cfg, fluid, device)
+    s.field_arithmetic = arith
+    load(s, p, lo, hi)
+    a, t_pulse = 0.05, 0.5
+    w = 5.0 * math.pi / 180.0
+    times = [0.0, t_pulse, t_pulse + 1e-6, 2 * t_pulse]
+    acc = np.array([[a, 0, 0], [a, 0, 0], [0, 0, 0], [0, 0, 0]], np.float64)
+    omega = np.array([[0, 0, 0], [0, 0, 0], [0, 0, 0], [0, w, 0]], np.float64)
+    s.set_maneuver(cs.ManeuverProfile(times, acc, omega, origin=(0.0, 0.0, 0.0)))
+    d0 = s.diagnostics()
+    M = d0.mass_liquid + d0.mass_vapor
+    p0 = d0.liquid_momentum[0]
+    impulse, t_in, p_in = 0.0, 0.0, p0
+    rows = []
+    t0 = time.perf_counter()
+    for k in range(steps):
+        s.step()
+        d = s.diagnostics()
+        if d.time <= t_pulse:
+            impulse += d.dt * d.slosh_force[0]
+            t_in, p_in = d.time, d.liquid_momentum[0]
+        if k % max(1, steps // 50) == 0 or k == steps - 1:
+            rows.append([round(d.time, 6), d.slosh_force[0], d.slosh_force[2], d.slosh_moment[1]])
+    wall = time.perf_counter() - t0
+    expect = -M * a * t_in
+    return {"workload": label, "particles": int(s.num_particles), "steps": steps, "t_end": float(rows[-1][0]),
+            "field_arithmetic": "fast" if arith == cs.FieldArithmetic.Fast else "exact",
+            "fluid_mass": M, "pulse": {"a_x": a, "t": t_in, "impulse_x": impulse, "minus_M_a_t": expect,
+                                       "ratio": impulse / expect,
+                                       "ratio_momentum_corrected": (impulse + (p_in - p0)) / expect},
+            "slew_deg_s": 5.0, "series_t_Fx_Fz_My": rows, "wall_s": wall}
 
 
 def c5_solver(cs, device, dx=0.0034):
@@ -832,7 +970,93 @@ def adjoint_run(cs, device, steps, every, knots=16):
     return res
 
 
-def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
+def _ref_structs(cs_cfg, fluid):
+    """The reference driver's config and fluid structs from module objects."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_abi
+    kw = {}
+    for name, _ in ref_abi.Config._fields_:
+        v = getattr(cs_cfg, name)
+        kw[name] = tuple(v) if name == "gravity" else (int(v.value) if hasattr(v, "value") else
+                                                      (int(v) if isinstance(v, bool) else v))
+    f = ref_abi.Fluid()
+    for k, _ in ref_abi.Fluid._fields_:
+        setattr(f, k, getattr(fluid, k))
+    return ref_abi.config(**kw), f
+
+
+def adjoint_fd64_run(cs, device, steps, every, knots=4):
+    """The LN2 boil-off window from its initial lattice: this library's adjoint
+    gradients (FP32 forward, hand-written reverse passes) against central
+    differences of the same loss through the reference's FP64 forward
+    (oracle/_ref/libcryoref64.so, every host thread), for the contact angle,
+    the Lee coefficient and the first manoeuvre knot.  The FP64 forward has no
+    single-precision noise, so a small step (1e-3 relative; 1e-4 m/s^2 for the
+    knot) gives a clean difference quotient."""
+    import torch
+    import cryo_adjoint as ca
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refpy
+    if not refpy.ref_available(fp64=True):
+        return None
+    s, fluid = c5_solver(cs, device)
+    p = s.particles()
+    lo, hi = cs.tank_domain(cs.CylinderTank(0.1, 0.25), float(s.config.dx), 3)
+    dt = float(s.config.fixed_dt)
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    kn = np.zeros((knots, 3))
+    kn[:, 0] = rng.uniform(-0.05, 0.05, knots)
+    times, _ = ca.knot_schedule(0.0, dt, steps, knots)
+    weights = np.array([1.0, 1.0, 1.0, 1.0, 1.0, 1.0, 1e-4])
+    theta0, lee0 = float(s.config.contact_angle_deg), 5.0
+    # adjoint
+    th = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    le = torch.tensor(lee0, dtype=torch.float64, requires_grad=True)
+    kt = torch.tensor(kn, dtype=torch.float64, requires_grad=True)
+    t0 = time.perf_counter()
+    out = ca.slosh_window(s, float(fluid.sigma), th, le, kt, steps, every)
+    (out * torch.tensor(weights)).sum().backward()
+    t_adj = time.perf_counter() - t0
+    ad = {"contact_angle_deg": float(th.grad), "lee": float(le.grad), "knot0_x": float(kt.grad[0, 0])}
+    base_cfg, base_fluid = _ref_structs(s.config, fluid)
+    arrays = {"x": p["position"], "v": p["velocity"], "m": p["mass"], "rho": p["density"], "T": p["temperature"],
+              "phase": p["phase"], "nrm": p["normal"], "flags": p["flags"]}
+
+    def loss64(theta=theta0, lee=lee0, knot0=kn[0, 0]):
+        cfg = type(base_cfg).from_buffer_copy(base_cfg)
+        cfg.contact_angle_deg = theta
+        cfg.lee_evaporation = cfg.lee_condensation = lee
+        r = refpy.Ref(cfg, base_fluid, fp64=True)
+        r.set_threads(os.cpu_count() or 1)
+        r.set_particles(arrays, lo, hi)
+        k = kn.copy()
+        k[0, 0] = knot0
+        r.set_maneuver(times, np.repeat(k, 2, axis=0))
+        obj = np.zeros(7)
+        for _ in range(steps):
+            r.step(1)
+            d = r.diagnostics()
+            obj[:3] += dt * np.asarray(d.slosh_force, np.float64)
+            obj[3:6] += dt * np.asarray(d.slosh_moment, np.float64)
+        obj[6] = r.diagnostics().p_ullage
+        r.close()
+        return float(obj @ weights)
+
+    t0 = time.perf_counter()
+    check = {}
+    for name, base, h, call in (("contact_angle_deg", theta0, 1e-3 * theta0, lambda v: loss64(theta=v)),
+                                ("lee", lee0, 1e-3 * lee0, lambda v: loss64(lee=v)),
+                                ("knot0_x", float(kn[0, 0]), 1e-4, lambda v: loss64(knot0=v))):
+        fd = (call(base + h) - call(base - h)) / (2 * h)
+        check[name] = {"adjoint": ad[name], "fd64": fd, "rel": abs(ad[name] - fd) / max(abs(fd), 1e-300)}
+    s.adjoint_release()
+    return {"workload": "c5_ln2_boiloff_cylinder_dx0.0034", "window_steps": steps, "checkpoint_every": every,
+            "knots": knots, "start": "initial lattice (t = 0)", "fd_check_fp64": check,
+            "loss": "sum of int F, int M (N s, N m s) + 1e-4 p_ullage (Pa)",
+            "adjoint_s": t_adj, "fd64_s": time.perf_counter() - t0}
+
+
+def batched_run(cs, tanks, steps, warmup, device, tune_steps=3, arith=None):
     """The 64-tank ensemble: the tanks advanced together by one cs.Ensemble (one
     graph launch per ensemble step, branch count autotuned) against the same
     tanks stepped back to back by plain Solvers.  Both sides take the same
@@ -846,6 +1070,8 @@ def batched_run(cs, tanks, steps, warmup, device, tune_steps=3):
         out = []
         for tk in tanks:
             sv = cs.Solver(tk["cfg"], tk["fluid"], device)
+            if arith is not None:
+                sv.field_arithmetic = arith
             load(sv, tk["p"], tk["lo"], tk["hi"])
             sv.set_maneuver(tk["maneuver"])
             out.append(sv)

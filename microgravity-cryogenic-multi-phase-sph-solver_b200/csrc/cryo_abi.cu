@@ -420,11 +420,15 @@ void cryo_ctx::check_capacity() {
 
 void cryo_ctx::run_steps(long long n) {
   ensure_initialized();
+  // Particles appear (splits) or leave (merges, deaths) only through the
+  // phase change; without it the count is fixed, so the steps return without
+  // a round trip and the host mirror is refreshed by the next call that reads it.
+  const bool count_can_change = P.cfg_phase_change != 0;
   for (long long k = 0; k < n; ++k) {
     launch_step();
-    if ((k & 15) == 15) check_capacity();
+    if (count_can_change && (k & 15) == 15) check_capacity();
   }
-  check_capacity();
+  if (count_can_change) check_capacity();
 }
 
 // Solver::run_until (sph_solver.cu:540-543): the steps are issued in batches

@@ -321,7 +321,10 @@ __device__ inline float eos_pressure(const Params& P, int ph, float rho, float T
   if (ph == kVapor) {
     p = rho * P.gas_R * T + (P.p_bg - P.vapor_K);
   } else {
-    const float ratio = rho / P.rho0[0];
+    // IEEE division in either field arithmetic: the Tait form takes 1 off
+    // ratio^7, so a last-place error of the ratio would be amplified by
+    // 7 / (ratio^7 - 1) in the pressure of a liquid near rest
+    const float ratio = __fdiv_rn(rho, P.rho0[0]);
     float r_g;
     if (P.tait_gamma == 7.0f) {
       const float r2 = ratio * ratio;
