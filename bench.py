@@ -385,7 +385,7 @@ def main():
     ap.add_argument("--slab-steps", type=int, default=50, help="timed steps of the slab leg")
     ap.add_argument("--side-force-steps", type=int, default=0,
                     help="with --workload c3: steps of the manoeuvre run (side force against -M a; 0 = skip)")
-    ap.add_argument("--probe-steps", type=int, default=1000,
+    ap.add_argument("--probe-steps", type=int, default=1500,
                     help="steps of the dam break's probe-pressure series against the FP64 reference (0 = skip)")
     ap.add_argument("--probe-dx", type=float, default=0.04, help="lattice spacing of the probe-series dam break")
     ap.add_argument("--only-timed", action="store_true",
@@ -702,12 +702,16 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, a
 
 
 # SPHERIC Test 2 pressure sensors (validation/spheric_test2/run.py:30-33,69-73
-# of the reference): four on the obstacle's front face, four on its top.
-def spheric_sensors(dx):
+# of the reference): four on the obstacle's front face, four on its top; then
+# four on the floor along the column's path (x = 2.8, 2.2 under the column,
+# 1.8, 1.6 where the front arrives), which the series reaches sooner.
+def spheric_sensors(dx, floor=True):
     x_front, box_h, y = 0.744, 0.161, 0.403 / 2 - 0.176
     offs = (0.021, 0.061, 0.101, 0.141)
-    return np.array([(x_front + 0.5 * dx, y, z) for z in offs] + [(x_front - o, y, box_h + 0.5 * dx) for o in offs],
-                    np.float32)
+    pts = [(x_front + 0.5 * dx, y, z) for z in offs] + [(x_front - o, y, box_h + 0.5 * dx) for o in offs]
+    if floor:
+        pts += [(x, 0.0, 0.5 * dx) for x in (2.8, 2.2, 1.8, 1.6)]
+    return np.array(pts, np.float32)
 
 
 def probe_series_run(cs, device, dx, steps, arith):
@@ -760,7 +764,9 @@ def probe_series_run(cs, device, dx, steps, arith):
         return out
 
     wet = np.isfinite(np.asarray(series["ours"][1])).mean(axis=0)
-    return {"workload": label, "steps": steps, "sensors": "P1-P4 front face, P5-P8 top (run.py:69-73)",
+    return {"workload": label, "steps": steps,
+            "sensors": "P1-P4 obstacle front face, P5-P8 obstacle top (run.py:69-73), F1-F4 floor at x = 2.8, 2.2, "
+                       "1.8, 1.6 m",
             "field_arithmetic": "fast" if arith == cs.FieldArithmetic.Fast else "exact",
             "t_end": float(series["ours"][0][-1]), "wet_fraction": [float(w) for w in wet],
             "error_vs_fp64": err("ours"), "reference_fp32_error_vs_fp64": err("fp32"),
@@ -1002,6 +1008,10 @@ def adjoint_fd64_run(cs, device, steps, every, knots=4):
     s, fluid = c5_solver(cs, device)
     p = s.particles()
     lo, hi = cs.tank_domain(cs.CylinderTank(0.1, 0.25), float(s.config.dx), 3)
+    # Initialise with the base parameters (the initial rate evaluation, whose
+    # accelerations the first half-kick uses, is not part of the window);
+    # the reference below is initialised the same way before its perturbation.
+    s.next_dt()
     dt = float(s.config.fixed_dt)
     rng = np.random.Generator(np.random.PCG64(SEED))
     kn = np.zeros((knots, 3))
@@ -1024,11 +1034,12 @@ def adjoint_fd64_run(cs, device, steps, every, knots=4):
 
     def loss64(theta=theta0, lee=lee0, knot0=kn[0, 0]):
         cfg = type(base_cfg).from_buffer_copy(base_cfg)
-        cfg.contact_angle_deg = theta
-        cfg.lee_evaporation = cfg.lee_condensation = lee
+        cfg.lee_evaporation = cfg.lee_condensation = lee  # not read by the initialisation
         r = refpy.Ref(cfg, base_fluid, fp64=True)
         r.set_threads(os.cpu_count() or 1)
         r.set_particles(arrays, lo, hi)
+        r.next_dt()  # initialised with the base contact angle and no frame motion
+        r.set_contact_angle(theta)
         k = kn.copy()
         k[0, 0] = knot0
         r.set_maneuver(times, np.repeat(k, 2, axis=0))
@@ -1051,7 +1062,8 @@ def adjoint_fd64_run(cs, device, steps, every, knots=4):
         check[name] = {"adjoint": ad[name], "fd64": fd, "rel": abs(ad[name] - fd) / max(abs(fd), 1e-300)}
     s.adjoint_release()
     return {"workload": "c5_ln2_boiloff_cylinder_dx0.0034", "window_steps": steps, "checkpoint_every": every,
-            "knots": knots, "start": "initial lattice (t = 0)", "fd_check_fp64": check,
+            "knots": knots, "start": "initial lattice (t = 0), initialised with the base parameters",
+            "fd_check_fp64": check,
             "loss": "sum of int F, int M (N s, N m s) + 1e-4 p_ullage (Pa)",
             "adjoint_s": t_adj, "fd64_s": time.perf_counter() - t0}
 

@@ -30,7 +30,7 @@ CU_SOURCES = ["cryo_grid.cu", "cryo_physics.cu", "cryo_phase.cu", "cryo_control.
 # reference's IEEE operation sequence (see csrc/cryo_common.cuh).
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
-    "--extended-lambda", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2", "-I" + INCLUDE,
+    "--extended-lambda", "-Xcompiler", "-fPIC,-ffp-contract=off,-O2,-fopenmp", "-I" + INCLUDE,
 ]
 # cryo_physics.cu again for the fast field arithmetic: FMA contraction and
 # approximate division / square root (denormals kept).
@@ -78,7 +78,7 @@ def build_lib(verbose=False):
             if verbose and r.stderr:
                 print(r.stderr)
     if _newer(LIB, objs):
-        _run([NVCC, "-shared", "-o", LIB] + objs + ["-lcudart"])
+        _run([NVCC, "-shared", "-o", LIB] + objs + ["-lcudart", "-Xcompiler", "-fopenmp"])
     return LIB
 
 

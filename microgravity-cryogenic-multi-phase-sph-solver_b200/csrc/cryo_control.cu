@@ -224,9 +224,11 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
     __syncthreads();
   }
   if (last_block(R.ticket)) {
-    for (int v = 0; v < 23; ++v) {
-      const double s = block_sum_partials(R, v, nch);
-      if (threadIdx.x == 0) out[v] = s;
+    // the 23 sums spread over the block's warps, one warp per value
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int v = warp; v < 23; v += kBlock / 32) {
+      const double s = warp_sum_partials(R, v, nch);
+      if (lane == 0) out[v] = s;
     }
     __shared__ float wm[2][kBlock / 32];
     for (int v = 23; v < 25; ++v) {

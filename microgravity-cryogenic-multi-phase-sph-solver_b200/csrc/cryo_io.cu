@@ -180,6 +180,37 @@ __global__ void __launch_bounds__(kBlock) k_frame_viewer(int n, View V, Reduce R
 }  // namespace cryo
 
 // ------------------------------------------------------------- host side
+namespace {
+
+// Host copies between the caller's arrays and the pinned transfer buffer,
+// cut into pieces of at most 1 MiB and spread over up to 8 host threads
+// (one thread copies a few GB/s; the DMA engine moves far more).
+struct HostCopy {
+  void* dst;
+  const void* src;
+  size_t bytes;
+};
+void copy_all(const std::vector<HostCopy>& jobs) {
+  constexpr size_t kPiece = size_t(1) << 20;
+  std::vector<HostCopy> pieces;
+  size_t total = 0;
+  for (const HostCopy& j : jobs) {
+    total += j.bytes;
+    for (size_t o = 0; o < j.bytes; o += kPiece)
+      pieces.push_back({static_cast<char*>(j.dst) + o, static_cast<const char*>(j.src) + o,
+                        std::min(kPiece, j.bytes - o)});
+  }
+  const int np = static_cast<int>(pieces.size());
+  if (total < (size_t(4) << 20)) {
+    for (const HostCopy& p : pieces) std::memcpy(p.dst, p.src, p.bytes);
+    return;
+  }
+#pragma omp parallel for schedule(dynamic, 1) num_threads(8)
+  for (int k = 0; k < np; ++k) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+}
+
+}  // namespace
+
 void cryo_ctx::io_reserve(size_t bytes) {
   if (bytes <= io_cap) return;
   sync();
@@ -215,16 +246,15 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
     const IoLayout L = io_layout((size_t)n);
     c->io_reserve(L.bytes);
     char* h = c->io_host;
+    const size_t N = (size_t)n;
     int have = 0;
-    std::memcpy(h + L.x, p->x, 12 * (size_t)n);
-    std::memcpy(h + L.m, p->m, 4 * (size_t)n);
-    std::memcpy(h + L.rho, p->rho, 4 * (size_t)n);
-    std::memcpy(h + L.T, p->T, 4 * (size_t)n);
-    std::memcpy(h + L.phase, p->phase, (size_t)n);
-    if (p->v) { std::memcpy(h + L.v, p->v, 12 * (size_t)n); have |= IO_V; }
-    if (p->nrm) { std::memcpy(h + L.nrm, p->nrm, 12 * (size_t)n); have |= IO_NRM; }
-    if (p->flags) { std::memcpy(h + L.flags, p->flags, (size_t)n); have |= IO_FLAGS; }
-    if (p->id) { std::memcpy(h + L.id, p->id, 4 * (size_t)n); have |= IO_ID; }
+    std::vector<HostCopy> jobs = {{h + L.x, p->x, 12 * N}, {h + L.m, p->m, 4 * N}, {h + L.rho, p->rho, 4 * N},
+                                  {h + L.T, p->T, 4 * N}, {h + L.phase, p->phase, N}};
+    if (p->v) { jobs.push_back({h + L.v, p->v, 12 * N}); have |= IO_V; }
+    if (p->nrm) { jobs.push_back({h + L.nrm, p->nrm, 12 * N}); have |= IO_NRM; }
+    if (p->flags) { jobs.push_back({h + L.flags, p->flags, N}); have |= IO_FLAGS; }
+    if (p->id) { jobs.push_back({h + L.id, p->id, 4 * N}); have |= IO_ID; }
+    copy_all(jobs);
     CK(cudaMemcpyAsync(c->io_dev, h, L.bytes, cudaMemcpyHostToDevice, c->stream));
     const int G = std::max(1, std::min((n + kBlock - 1) / kBlock, c->sm_count * 8));
     k_load_pack<<<G, kBlock, 0, c->stream>>>(n, io_arrays(c->io_dev, L), have, c->view(0));
@@ -253,15 +283,18 @@ int cryo_download(cryo_ctx* c, cryo_host_particles_out_t* o) {
     CK(cudaMemcpyAsync(c->io_host, c->io_dev, L.bytes, cudaMemcpyDeviceToHost, c->stream));
     c->sync();
     const char* h = c->io_host;
-    if (o->x) std::memcpy(o->x, h + L.x, 12 * (size_t)n);
-    if (o->v) std::memcpy(o->v, h + L.v, 12 * (size_t)n);
-    if (o->nrm) std::memcpy(o->nrm, h + L.nrm, 12 * (size_t)n);
-    if (o->m) std::memcpy(o->m, h + L.m, 4 * (size_t)n);
-    if (o->rho) std::memcpy(o->rho, h + L.rho, 4 * (size_t)n);
-    if (o->T) std::memcpy(o->T, h + L.T, 4 * (size_t)n);
-    if (o->id) std::memcpy(o->id, h + L.id, 4 * (size_t)n);
-    if (o->phase) std::memcpy(o->phase, h + L.phase, (size_t)n);
-    if (o->flags) std::memcpy(o->flags, h + L.flags, (size_t)n);
+    const size_t N = (size_t)n;
+    std::vector<HostCopy> jobs;
+    if (o->x) jobs.push_back({o->x, h + L.x, 12 * N});
+    if (o->v) jobs.push_back({o->v, h + L.v, 12 * N});
+    if (o->nrm) jobs.push_back({o->nrm, h + L.nrm, 12 * N});
+    if (o->m) jobs.push_back({o->m, h + L.m, 4 * N});
+    if (o->rho) jobs.push_back({o->rho, h + L.rho, 4 * N});
+    if (o->T) jobs.push_back({o->T, h + L.T, 4 * N});
+    if (o->id) jobs.push_back({o->id, h + L.id, 4 * N});
+    if (o->phase) jobs.push_back({o->phase, h + L.phase, N});
+    if (o->flags) jobs.push_back({o->flags, h + L.flags, N});
+    copy_all(jobs);
   });
 }
 

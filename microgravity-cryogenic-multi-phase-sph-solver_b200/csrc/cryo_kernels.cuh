@@ -77,6 +77,22 @@ __device__ inline double block_sum_partials(const Reduce& R, int v, int nchunks)
   __syncthreads();
   return r;
 }
+// Sum of value v over chunks [0, nchunks) by one warp, in a fixed order that
+// depends on nothing but nchunks: lane l sums chunks l, l + 32, ...
+// (compensated), then a fixed down-shift tree.  The result is valid in lane 0.
+// Several warps of a block can each take their own values at once.
+__device__ inline double warp_sum_partials(const Reduce& R, int v, int nchunks) {
+  const int lane = threadIdx.x & 31;
+  double s = 0, c = 0;
+  const double* p = R.partials + (size_t)v * R.max_chunks;
+  for (int k = lane; k < nchunks; k += 32) neumaier(s, c, __ldcg(p + k));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const double s2 = __shfl_down_sync(0xffffffffu, s, o), c2 = __shfl_down_sync(0xffffffffu, c, o);
+    neumaier_pair(s, c, s2, c2);
+  }
+  return s + c;
+}
 // In-place exclusive scan of the (integral) chunk values of row v by the whole
 // block; returns the total (all threads).  Integral doubles add exactly, so
 // the parallel order gives the serial result.
