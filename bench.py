@@ -1094,7 +1094,7 @@ def batched_run(cs, tanks, steps, warmup, device, tune_steps=3, arith=None):
     for sv in ens_tanks:
         ens.add(sv)
     cands = sorted({k for k in (len(tanks), 32, 16, 8, 4) if 1 <= k <= len(tanks)}, reverse=True)
-    branches, per_launch, _ = ens.tune(cands, [1, 2, 4], tune_steps)
+    branches, per_launch, _ = ens.tune(cands, [1, 2, 4], tune_steps, [1, 2, 4])
     ens.run_steps(warmup)
     before = ens_tanks[0].step_count
     ms_ens = ens.step_time(steps)
@@ -1102,6 +1102,7 @@ def batched_run(cs, tanks, steps, warmup, device, tune_steps=3, arith=None):
     total_steps = ens_tanks[0].step_count
     n_total = sum(tk["n"] for tk in tanks)
     launches = ens.launches_per_step
+    tile = ens.tile
     d_ens = [d.as_dict() for d in ens.diagnostics()]
     del ens
 
@@ -1125,7 +1126,7 @@ def batched_run(cs, tanks, steps, warmup, device, tune_steps=3, arith=None):
         "ms_per_step": ms_ens, "back_to_back": n_total * timed_steps / (ms_solo / 1e3),
         "back_to_back_ms_per_step": ms_solo / timed_steps,
         "speedup": (ms_solo / timed_steps) / ms_ens if ms_ens > 0 else None, "branches": branches,
-        "steps_per_launch": per_launch,
+        "steps_per_launch": per_launch, "tile": tile,
         "gpu_launches_per_step": launches, "diagnostics_bit_identical": bool(same),
         "execution": "CUDA graph launches of steps_per_launch ensemble steps (every tank's kernels as concurrent branches)",
     }

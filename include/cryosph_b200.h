@@ -446,6 +446,17 @@ int cryo_ensemble_step_time(cryo_ensemble* ens, int steps, float* ms_per_step);
 int cryo_ensemble_tune(cryo_ensemble* ens, const int* chain_candidates, int nchain, const int* launch_candidates,
                        int nlaunch, int steps, int* best_chains, int* best_steps_per_launch,
                        float* best_ms_per_step);
+/* The members' tile: particles per thread of their grid-stride kernels
+ * inside the ensemble's graphs (1 to 64; 1 = one thread per particle, as a
+ * member stepped alone).  Results do not depend on it.  cryo_ensemble_tune_tiles
+ * runs cryo_ensemble_tune for every tile candidate (NULL: the current tile)
+ * and keeps the fastest branch count, steps per launch and tile. */
+int cryo_ensemble_set_tile(cryo_ensemble* ens, int particles_per_thread);
+int cryo_ensemble_tile(cryo_ensemble* ens, int* particles_per_thread);
+int cryo_ensemble_tune_tiles(cryo_ensemble* ens, const int* chain_candidates, int nchain,
+                             const int* launch_candidates, int nlaunch, const int* tile_candidates, int ntile,
+                             int steps, int* best_chains, int* best_steps_per_launch, int* best_tile,
+                             float* best_ms_per_step);
 /* Kernel launches per ensemble step inside the step graphs. */
 int cryo_ensemble_launches_per_step(cryo_ensemble* ens, int* launches);
 int cryo_ensemble_synchronize(cryo_ensemble* ens);

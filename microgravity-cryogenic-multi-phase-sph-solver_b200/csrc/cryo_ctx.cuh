@@ -378,13 +378,21 @@ struct cryo_ctx {
   // the particle count last read plus head-room for splits; check_capacity
   // drops the graphs when the count outgrows it
   void size_grids() { grid_span = std::max(1, std::min(capacity, hdyn->n + hdyn->n / 8 + 1024)); }
+  // Particles per thread of the grid-stride kernels (1: one thread per
+  // particle).  Any value gives the same results; an ensemble's autotuner
+  // picks it for the members' kernels (coarser grids of many small tanks
+  // running side by side).
+  int grid_tile = 1;
   int grid_blocks() const {
-    const int need = (span() + kBlock - 1) / kBlock;
+    const int per_block = kBlock * grid_tile;
+    const int need = (span() + per_block - 1) / per_block;
     return std::max(1, std::min(need, sm_count * 8));
   }
-  // force pass: one thread per particle up to two full-occupancy waves
+  // force pass: one thread per particle (times the tile) up to two
+  // full-occupancy waves
   int forces_blocks() const {
-    const int need = (span() + FORCES_BLOCK - 1) / FORCES_BLOCK;
+    const int per_block = FORCES_BLOCK * grid_tile;
+    const int need = (span() + per_block - 1) / per_block;
     return std::max(1, std::min(need, sm_count * (2048 / FORCES_BLOCK) * 2));
   }
   void invalidate_graphs() {

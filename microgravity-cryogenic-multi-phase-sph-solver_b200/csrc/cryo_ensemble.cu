@@ -32,6 +32,8 @@ struct cryo_ensemble {
   std::vector<cryo_ctx*> tanks;
   int chains = 0;      // 0: one branch per tank
   int per_launch = 1;  // steps per graph launch (divides 16)
+  int tile = 1;        // particles per thread of the members' grid-stride kernels
+  int built_tile = 0;
   Graphs multi, single;
   std::vector<int> built_cur;  // each tank's ping-pong parity when the graphs were built
   std::vector<unsigned long long> built_gen;
@@ -59,7 +61,7 @@ struct cryo_ensemble {
     return chains <= 0 ? t : std::min(chains, t);
   }
   bool valid() const {
-    if (built_chains != branches() || multi.steps != per_launch) return false;
+    if (built_chains != branches() || multi.steps != per_launch || built_tile != tile) return false;
     for (size_t t = 0; t < tanks.size(); ++t)
       if (tanks[t]->generation != built_gen[t] || tanks[t]->cur != ((built_cur[t] + phase) & 1)) return false;
     return true;
@@ -94,6 +96,13 @@ struct cryo_ensemble {
         for (int t : br) {
           cryo_ctx* c = tanks[t];
           CK(cudaStreamWaitEvent(c->stream, prev, 0));
+          // the member's kernels at the ensemble's tile (its own step graphs keep theirs)
+          struct TileScope {
+            cryo_ctx* c;
+            int saved;
+            ~TileScope() { c->grid_tile = saved; }
+          } scope{c, c->grid_tile};
+          c->grid_tile = tile;
           for (int k = 0; k < steps; ++k) {
             const long long c0 = c->launch_counter;
             c->enqueue_step((built_cur[t] + q + k) & 1);
@@ -141,6 +150,7 @@ struct cryo_ensemble {
     build_shape(multi, per_launch, pl);
     if (per_launch > 1) build_shape(single, 1, pl);
     built_chains = branches();
+    built_tile = tile;
   }
   // tank streams -> ensemble stream, and back
   void enter() {
@@ -322,6 +332,53 @@ int cryo_ensemble_step_time(cryo_ensemble* e, int steps, float* ms_per_step) {
   return eguard(e, [&] {
     if (steps <= 0) throw std::invalid_argument("ensemble: steps must be > 0");
     *ms_per_step = e->tanks.empty() ? 0.0f : e->time_steps(steps);
+  });
+}
+
+int cryo_ensemble_set_tile(cryo_ensemble* e, int particles_per_thread) {
+  return eguard(e, [&] {
+    if (particles_per_thread < 1 || particles_per_thread > 64)
+      throw std::invalid_argument("ensemble: the tile must be 1 to 64 particles per thread");
+    e->tile = particles_per_thread;
+  });
+}
+
+int cryo_ensemble_tile(cryo_ensemble* e, int* particles_per_thread) {
+  return eguard(e, [&] { *particles_per_thread = e->tile; });
+}
+
+// The tuner of cryo_ensemble_tune over a third axis: the members' tile
+// (particles per thread of their grid-stride kernels).
+int cryo_ensemble_tune_tiles(cryo_ensemble* e, const int* chain_candidates, int nchain, const int* launch_candidates,
+                             int nlaunch, const int* tile_candidates, int ntile, int steps, int* best_chains,
+                             int* best_steps_per_launch, int* best_tile, float* best_ms) {
+  return eguard(e, [&] {
+    std::vector<int> tc;
+    if (tile_candidates && ntile > 0) tc.assign(tile_candidates, tile_candidates + ntile);
+    else tc.push_back(e->tile);
+    for (int k : tc)
+      if (k < 1 || k > 64) throw std::invalid_argument("ensemble: tiles must be 1 to 64 particles per thread");
+    int bc = 0, bl = 1, bt = tc[0];
+    float bm = 0.0f;
+    bool any = false;
+    for (int k : tc) {
+      e->tile = k;
+      int c = 0, l = 1;
+      float ms = 0.0f;
+      const int rc = cryo_ensemble_tune(e, chain_candidates, nchain, launch_candidates, nlaunch, steps, &c, &l, &ms);
+      if (rc != CRYO_OK) throw std::runtime_error(e->err);
+      if (!any || ms < bm) {
+        any = true;
+        bc = c; bl = l; bt = k; bm = ms;
+      }
+    }
+    e->chains = bc;
+    e->per_launch = bl;
+    e->tile = bt;
+    if (best_chains) *best_chains = bc;
+    if (best_steps_per_launch) *best_steps_per_launch = bl;
+    if (best_tile) *best_tile = bt;
+    if (best_ms) *best_ms = bm;
   });
 }
 

@@ -623,14 +623,19 @@ PYBIND11_MODULE(CryoSPH, m) {
                     "Ensemble steps per graph launch (1, 2, 4, 8 or 16).")
       .def(
           "tune",
-          [](Ensemble& e, std::vector<int> chains, std::vector<int> steps_per_launch, int steps) {
+          [](Ensemble& e, std::vector<int> chains, std::vector<int> steps_per_launch, int steps,
+             std::vector<int> tiles) {
             py::gil_scoped_release nogil;
-            return e.tune(chains, steps_per_launch, steps);
+            return e.tune(chains, steps_per_launch, steps, tiles);
           },
           py::arg("chains") = std::vector<int>{}, py::arg("steps_per_launch") = std::vector<int>{},
-          py::arg("steps") = 3,
-          "Autotunes branch count and steps per launch by timing `steps` steps per candidate pair (these steps "
-          "advance the members); returns (branches, steps per launch, ms per step).")
+          py::arg("steps") = 3, py::arg("tiles") = std::vector<int>{},
+          "Autotunes branch count, steps per launch and the members' tile (particles per thread) by timing "
+          "`steps` steps per candidate (these steps advance the members); returns (branches, steps per launch, "
+          "ms per step).")
+      .def_property("tile", &Ensemble::tile, &Ensemble::set_tile,
+                    "Particles per thread of the members' grid-stride kernels inside the ensemble (results do not "
+                    "depend on it).")
       .def("step_time", &Ensemble::step_time, py::arg("steps"), py::call_guard<py::gil_scoped_release>(),
            "Device ms per ensemble step over `steps` steps (which advance the members).")
       .def_property_readonly("launches_per_step", &Ensemble::launches_per_step)

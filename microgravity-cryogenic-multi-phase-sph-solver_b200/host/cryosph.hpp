@@ -428,8 +428,12 @@ class Ensemble {
   // Times `steps` steps per (branch count, steps per launch) candidate and
   // keeps the fastest; returns (branches, steps per launch, ms per step).
   // The timed steps advance the members.
+  // Times `steps` steps per (branch count, steps per launch, tile) candidate
+  // and keeps the fastest; returns (branches, steps per launch, ms per step).
   std::tuple<int, int, float> tune(const std::vector<int>& chain_candidates, const std::vector<int>& launch_candidates,
-                                   int steps);
+                                   int steps, const std::vector<int>& tile_candidates = {});
+  void set_tile(int particles_per_thread);  // particles per thread of the members' kernels (1..64)
+  int tile() const;
   float step_time(int steps);
   int launches_per_step() const;
   std::uintptr_t stream_handle() const;

@@ -452,14 +452,22 @@ int Ensemble::steps_per_launch() const {
   return k;
 }
 std::tuple<int, int, float> Ensemble::tune(const std::vector<int>& chain_candidates,
-                                           const std::vector<int>& launch_candidates, int steps) {
-  int best = 0, per = 0;
+                                           const std::vector<int>& launch_candidates, int steps,
+                                           const std::vector<int>& tile_candidates) {
+  int best = 0, per = 0, tile = 0;
   float ms = 0.0f;
-  check(cryo_ensemble_tune(e_, chain_candidates.empty() ? nullptr : chain_candidates.data(),
-                           static_cast<int>(chain_candidates.size()),
-                           launch_candidates.empty() ? nullptr : launch_candidates.data(),
-                           static_cast<int>(launch_candidates.size()), steps, &best, &per, &ms));
+  auto ptr = [](const std::vector<int>& v) { return v.empty() ? nullptr : v.data(); };
+  check(cryo_ensemble_tune_tiles(e_, ptr(chain_candidates), static_cast<int>(chain_candidates.size()),
+                                 ptr(launch_candidates), static_cast<int>(launch_candidates.size()),
+                                 ptr(tile_candidates), static_cast<int>(tile_candidates.size()), steps, &best, &per,
+                                 &tile, &ms));
   return {best, per, ms};
+}
+void Ensemble::set_tile(int particles_per_thread) { check(cryo_ensemble_set_tile(e_, particles_per_thread)); }
+int Ensemble::tile() const {
+  int k = 0;
+  check(cryo_ensemble_tile(e_, &k));
+  return k;
 }
 float Ensemble::step_time(int steps) {
   float ms = 0.0f;
