@@ -140,3 +140,27 @@ def test_bad_members_are_refused(cuda_device, tanks):
         ens.chains = -1
     with pytest.raises(ValueError):
         ens.steps_per_launch = 3
+
+
+@pytest.mark.parametrize("tile", [2, 4])
+def test_member_tiles_keep_bit_identity(cuda_device, tanks, tile):
+    """The members' tile (particles per thread of their grid-stride kernels)
+    changes launch grids only: results equal the solo steps bit for bit,
+    and the tuner's tile axis picks one of its candidates."""
+    ens_s, solo = solvers(tanks), solvers(tanks)
+    ens = cs.Ensemble(0)
+    for s in ens_s:
+        ens.add(s)
+    ens.tile = tile
+    assert ens.tile == tile
+    ens.run_steps(6)
+    best, per, ms = ens.tune([len(tanks)], [1], 2, [1, tile])
+    assert ens.tile in (1, tile) and ms > 0
+    ens.run_steps(3)
+    total = ens_s[0].step_count
+    for s in solo:
+        s.run_steps(total)
+    for k, (a, b) in enumerate(zip(ens_s, solo)):
+        assert same_state(a, b) is None, (k, same_state(a, b))
+    with pytest.raises(ValueError):
+        ens.tile = 0
