@@ -255,6 +255,15 @@ int cryo_set_particles(cryo_ctx* ctx, const cryo_host_particles_t* p, const floa
 int cryo_build_tank(cryo_ctx* ctx, const cryo_geom_node_t* nodes, int n_nodes, const cryo_fill_t* fill,
                     const float* bounds_lo, const float* bounds_hi);
 
+/* Seeded jitter of the fluid lattice on the device (no counterpart in the
+ * reference, whose inputs are jittered on the host): before the first step,
+ * every liquid and vapour coordinate moves by amplitude * (2u - 1) with u a
+ * 24-bit uniform in [0, 1) drawn from (seed, particle id, axis) by the
+ * SplitMix64 output function, so the result does not depend on particle
+ * order and can be restated on the host bit for bit; walls stay on the
+ * lattice.  CRYO_EINVAL once the solver has stepped. */
+int cryo_jitter_fluid(cryo_ctx* ctx, float amplitude, unsigned long long seed);
+
 /* Solver::step / run_steps / run_until / relax / next_dt (sph_solver.cu:506-543,707-736). */
 int cryo_step(cryo_ctx* ctx);
 int cryo_run_steps(cryo_ctx* ctx, long long n);

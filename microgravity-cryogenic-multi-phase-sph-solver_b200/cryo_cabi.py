@@ -290,6 +290,7 @@ def load(path=None):
         "cryo_set_graph_mode": (i, [vp, i]),
         "cryo_set_neighbor_mode": (i, [vp, i]),
         "cryo_set_field_arithmetic": (i, [vp, i]),
+        "cryo_jitter_fluid": (i, [vp, f, C.c_ulonglong]),
         "cryo_field_arithmetic": (i, [vp, ip]),
         "cryo_adj_forward": (i, [vp, C.c_longlong, i, vp]),
         "cryo_adj_backward": (i, [vp, vp, vp, vp]),
@@ -337,6 +338,22 @@ def fluid_preset(which, lib=None):
 
 def vec3(v):
     return (C.c_float * 3)(*[float(a) for a in v])
+
+
+def jitter_offsets(ids, seed, amplitude):
+    """The offsets cryo_jitter_fluid adds on the device, restated on the host:
+    (n, 3) float32, amplitude * (2u - 1) with u = the top 24 bits of the
+    SplitMix64 output function of seed + (3 id + axis + 1) * 0x9E3779B97F4A7C15,
+    scaled by 2^-24.  Apply them to liquid and vapour particles only."""
+    ids = np.asarray(ids, np.uint64)
+    with np.errstate(over="ignore"):
+        k = (np.uint64(3) * ids)[:, None] + np.arange(1, 4, dtype=np.uint64)[None, :]
+        z = np.uint64(seed) + k * np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    u = (z >> np.uint64(40)).astype(np.float32) * np.float32(1.0 / 16777216.0)
+    return np.float32(amplitude) * (np.float32(2.0) * u - np.float32(1.0))
 
 
 class Context:
@@ -388,6 +405,9 @@ class Context:
 
     def set_neighbor_mode(self, use_lists):
         self.check(self.L.cryo_set_neighbor_mode(self.h, int(bool(use_lists))))
+
+    def jitter_fluid(self, amplitude, seed):
+        self.check(self.L.cryo_jitter_fluid(self.h, float(amplitude), int(seed)))
 
     def set_field_arithmetic(self, mode):
         """CRYO_ARITH_EXACT (0, the reference's IEEE sequence) or CRYO_ARITH_FAST (1)."""

@@ -716,6 +716,26 @@ void cryo_ctx::finish_load(int n, uint32_t next_id) {
   c->initialized = false;
 }
 
+// Seeded jitter of the loaded fluid lattice on the device (k_jitter_fluid):
+// before the first step, every liquid and vapour coordinate moves by a
+// uniform offset in [-amplitude, amplitude) drawn from (seed, id, axis).
+int cryo_jitter_fluid(cryo_ctx* c, float amplitude, unsigned long long seed) {
+  return guard(c, [&] {
+    if (!c->has_particles) throw std::invalid_argument("cryo_jitter_fluid: no particles loaded");
+    if (c->initialized)
+      throw std::invalid_argument("cryo_jitter_fluid: the solver has stepped; jitter the lattice before the first step");
+    if (!(amplitude >= 0.0f) || !std::isfinite(amplitude))
+      throw std::invalid_argument("cryo_jitter_fluid: the amplitude must be finite and >= 0");
+    c->pull();
+    const int n = c->hdyn->n;
+    if (n == 0 || amplitude == 0.0f) return;
+    const int G = std::max(1, std::min((n + kBlock - 1) / kBlock, c->sm_count * 8));
+    k_jitter_fluid<<<G, kBlock, 0, c->stream>>>(c->view(c->cur), n, amplitude, (uint64_t)seed);
+    LAUNCH_CHECK();
+    c->sync();
+  });
+}
+
 // Solver::build_tank with the lattice generated on the device (see
 // cryo_setup.cu).  The lattice range, the liquid cut and the particle
 // constants follow build_tank_particles (geometry.cpp:242-330) operation for

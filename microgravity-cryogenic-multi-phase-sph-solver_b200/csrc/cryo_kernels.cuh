@@ -328,6 +328,7 @@ __global__ void k_fill_split(Lattice L, FillDev F, const long long* fluid_nodes,
                              uint32_t* cnt_keep, uint32_t* cnt_liq);
 __global__ void k_emit_walls(const GeomNode* G, int ng, Lattice L, FillDev F, const long long* wall_nodes, int nw,
                              View V);
+__global__ void k_jitter_fluid(View V, int n, float amplitude, uint64_t seed);
 __global__ void k_emit_fluid(Lattice L, FillDev F, const long long* fluid_nodes, int nf, const uint8_t* liquid,
                              const uint32_t* off_keep, int nw, View V);
 

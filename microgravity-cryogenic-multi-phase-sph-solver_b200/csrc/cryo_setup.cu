@@ -264,4 +264,31 @@ __global__ void __launch_bounds__(kBlock) k_emit_fluid(Lattice L, FillDev F, con
   V.id[o] = (uint32_t)o;
 }
 
+// Seeded jitter of the fluid lattice (liquid and vapour; walls stay on the
+// lattice): every coordinate moves by amplitude * (2u - 1), u uniform in
+// [0, 1) with 24 bits, drawn by a counter-based generator from (seed,
+// particle id, axis): the SplitMix64 output function (S. Vigna, "Further
+// scramblings of Marsaglia's xorshift generators", 2017) of
+// seed + (3 id + axis + 1) * 0x9E3779B97F4A7C15.  The draw depends on the
+// id, not on the slot, so it is the same whatever order the particles are in,
+// and a host restatement (cryo_cabi.jitter_offsets) reproduces it bit for bit.
+__device__ inline float jitter_unit(uint64_t seed, uint32_t id, int axis) {
+  uint64_t z = seed + (3ull * id + (uint64_t)axis + 1ull) * 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  z = z ^ (z >> 31);
+  return (float)(uint32_t)(z >> 40) * (1.0f / 16777216.0f);
+}
+__global__ void __launch_bounds__(kBlock) k_jitter_fluid(View V, int n, float amplitude, uint64_t seed) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 xp = V.xp[i];
+    if (!is_fluid(ph_of(xp))) continue;
+    const uint32_t id = V.id[i];
+    xp.x = xp.x + amplitude * (2.0f * jitter_unit(seed, id, 0) - 1.0f);
+    xp.y = xp.y + amplitude * (2.0f * jitter_unit(seed, id, 1) - 1.0f);
+    xp.z = xp.z + amplitude * (2.0f * jitter_unit(seed, id, 2) - 1.0f);
+    V.xp[i] = xp;
+  }
+}
+
 }  // namespace cryo

@@ -585,6 +585,9 @@ PYBIND11_MODULE(CryoSPH, m) {
       .def_property("field_arithmetic", &Solver::field_arithmetic, &Solver::set_field_arithmetic,
                     "Exact (default): the reference's IEEE operation sequence in the neighbour passes, bit-identical "
                     "to its CPU build; Fast: FMA contraction and approximate division / square root, within 1e-5.")
+      .def("jitter_fluid", &Solver::jitter_fluid, py::arg("amplitude"), py::arg("seed"),
+           "Moves every liquid and vapour particle by a seeded uniform offset in [-amplitude, amplitude) per axis, "
+           "on the device, before the first step (cryo_cabi.jitter_offsets restates it on the host).")
       .def("set_graph_mode", &Solver::set_graph_mode, py::arg("enabled"),
            "Replay each step as a captured CUDA graph (default) or launch kernels one by one.")
       .def(

@@ -378,6 +378,9 @@ class Solver {
   cryo_ctx* handle() const noexcept { return ctx_; }
   std::uintptr_t stream_handle() const;
   void set_graph_mode(bool on);
+  // Seeded uniform jitter of the fluid lattice on the device, before the
+  // first step (walls stay on the lattice; cryo_jitter_fluid).
+  void jitter_fluid(real amplitude, std::uint64_t seed);
   // Exact: the reference's IEEE operation sequence in the neighbour passes
   // (bit-identical to its CPU build); Fast: contracted, within 1e-5 of it.
   void set_field_arithmetic(FieldArithmetic mode);

@@ -402,6 +402,9 @@ std::vector<real> Solver::probe_pressure(const std::vector<Vec3>& points) {
 
 std::uintptr_t Solver::stream_handle() const { return cryo_stream(ctx_); }
 void Solver::set_graph_mode(bool on) { check(cryo_set_graph_mode(ctx_, on ? 1 : 0)); }
+void Solver::jitter_fluid(real amplitude, std::uint64_t seed) {
+  check(cryo_jitter_fluid(ctx_, amplitude, static_cast<unsigned long long>(seed)));
+}
 void Solver::set_field_arithmetic(FieldArithmetic mode) { check(cryo_set_field_arithmetic(ctx_, static_cast<int>(mode))); }
 FieldArithmetic Solver::field_arithmetic() const {
   int m = 0;

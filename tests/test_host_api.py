@@ -293,3 +293,20 @@ def test_obj_reader_rejects_bad_files(tmp_path):
         cs.MeshTank(str(p))
     p.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf -4 -3 -2 -1\n")  # a quad by relative indices, fanned
     assert cs.MeshTank(str(p)).num_triangles == 2
+
+
+def test_jitter_offsets_are_a_function_of_seed_and_id():
+    """The host restatement of the device jitter: bounded by the amplitude,
+    fixed by (seed, id, axis) whatever the order, different for another seed,
+    and 24-bit uniform draws (mean near 0, variance near amp^2 / 3)."""
+    ids = np.arange(200_000, dtype=np.uint32)
+    a = cabi.jitter_offsets(ids, 2002, 1e-4)
+    assert a.shape == (len(ids), 3) and a.dtype == np.float32
+    assert np.abs(a).max() <= 1e-4
+    perm = np.random.default_rng(1).permutation(len(ids))
+    assert np.array_equal(cabi.jitter_offsets(ids[perm], 2002, 1e-4), a[perm])
+    assert not np.array_equal(cabi.jitter_offsets(ids, 2003, 1e-4), a)
+    assert abs(float(a.mean())) < 2e-7
+    assert abs(float(a.var()) / (1e-4 ** 2 / 3.0) - 1.0) < 0.01
+    # the three axes are not copies of one another
+    assert abs(float(np.corrcoef(a[:, 0], a[:, 1])[0, 1])) < 0.01

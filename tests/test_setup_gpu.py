@@ -92,3 +92,33 @@ def test_device_lattice_timing_large_sphere(cuda_device):
     assert dev.num_particles == host.num_particles
     for k in ("position", "phase", "normal"):
         assert np.array_equal(np.asarray(dev.particles()[k]), np.asarray(host.particles()[k])), k
+
+
+def test_device_jitter_equals_its_host_restatement(cuda_device):
+    """Solver.jitter_fluid moves the fluid lattice on the device; the same
+    offsets from cryo_cabi.jitter_offsets (by particle id) applied to the host
+    generator's particles give the same positions bit for bit; walls stay."""
+    import cryo_cabi as cabi
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    cfg = cs.SolverConfig()
+    cfg.dx = 0.004
+    fill = cs.FillSpec()
+    fill.fill_fraction = 0.4
+    geo = cs.SphereTank(0.05)
+    s = cs.Solver(cfg, ln2)
+    s.build_tank(geo, fill)
+    amp, seed = 0.05 * 0.004, 2002
+    s.jitter_fluid(amp, seed)
+    got = s.particles()
+    host = cs.tank_particles(geo, ln2, 0.004, fill)
+    off = cabi.jitter_offsets(host["id"], seed, amp)
+    fl = host["phase"] != 2
+    want = host["position"].astype(np.float32).copy()
+    want[fl] = want[fl] + off[fl]
+    order = np.argsort(got["id"])
+    assert np.array_equal(got["id"][order], host["id"])
+    assert np.array_equal(got["position"][order].view(np.uint32), want.view(np.uint32))
+    assert np.abs(off).max() <= amp and off[fl].std() > 0.4 * amp
+    s.run_steps(1)
+    with pytest.raises(ValueError):
+        s.jitter_fluid(amp, seed)
