@@ -183,12 +183,23 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
       const float4 vT = V.vT[i];
       const double m = V.mrps[i].x;
       if (ph == kLiquid || ph == kVapor) {
-        const int k = ph;
-        s[k] = 1.0;
-        s[3 + k] = m;
-        s[5 + k] = 0.5 * m * (double)norm2(xyz(vT));
-        s[7 + k] = m * (double)specific_enthalpy(P, ph, vT.w);
-        s[9 + k] = m * vT.w;
+        // per-phase slots chosen by selects, not by a run-time index, so the
+        // 23 sums stay in registers (an indexed store would put them in
+        // local memory)
+        const bool liq = ph == kLiquid;
+        const double ke = 0.5 * m * (double)norm2(xyz(vT));
+        const double H = m * (double)specific_enthalpy(P, ph, vT.w);
+        const double mT = m * vT.w;
+        s[0] = liq ? 1.0 : 0.0;
+        s[1] = liq ? 0.0 : 1.0;
+        s[3] = liq ? m : 0.0;
+        s[4] = liq ? 0.0 : m;
+        s[5] = liq ? ke : 0.0;
+        s[6] = liq ? 0.0 : ke;
+        s[7] = liq ? H : 0.0;
+        s[8] = liq ? 0.0 : H;
+        s[9] = liq ? mT : 0.0;
+        s[10] = liq ? 0.0 : mT;
         const float4 fw = V.fw[i], mw = V.mw[i];
         s[17] = fw.x; s[18] = fw.y; s[19] = fw.z;
         s[20] = mw.x; s[21] = mw.y; s[22] = mw.z;

@@ -434,14 +434,17 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
     // evaluated once per particle when it does not vary per neighbour
     // (0 where eta_i + eta_j = 0: that term is skipped, and a zero term
     // added to a sum leaves it unchanged)
-    float eta_pair[2] = {0.0f, 0.0f};
+    // (two scalars picked by a select per pair: a small array indexed by the
+    // neighbour's phase would live in local memory, a load on every pair's
+    // dependent chain)
+    float eta_pair0 = 0.0f, eta_pair1 = 0.0f;
     if (!P.sps) {
-#pragma unroll
-      for (int q = 0; q < 2; ++q) {
-        const float etaj = P.mu[q] + 0.0f;
+      auto harmonic = [&](float etaj) {
         const float eta_sum = etai + etaj;
-        eta_pair[q] = eta_sum > 0.0f ? 2.0f * etai * etaj / eta_sum : 0.0f;
-      }
+        return eta_sum > 0.0f ? 2.0f * etai * etaj / eta_sum : 0.0f;
+      };
+      eta_pair0 = harmonic(P.mu[0] + 0.0f);
+      eta_pair1 = harmonic(P.mu[1] + 0.0f);
     }
 
     // transport (SPH_kernels.cu:61-74)
@@ -477,9 +480,8 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
     // thermal: the harmonic conductivity per neighbour phase
     // (phase_change.cu:57-61), evaluated once per particle
     const float ki = P.k[pi_idx];
-    float k_pair[2];
-#pragma unroll
-    for (int qq = 0; qq < 2; ++qq) k_pair[qq] = 4.0f * ki * P.k[qq] / (ki + P.k[qq]);
+    const float k_pair0 = 4.0f * ki * P.k[0] / (ki + P.k[0]);
+    const float k_pair1 = 4.0f * ki * P.k[1] / (ki + P.k[1]);
     float q = 0.0f;
 
     constexpr int kUnroll = (FORCES_UNROLL_HEAVY > 1 && WHAT >= 0 && (WHAT & (FORCE_CSF | FORCE_THERMAL)))
@@ -572,8 +574,9 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
             const float eta_ij = 2.0f * etai * etaj / eta_sum;
             force += vij * (vsum * eta_ij * dW / r);
           }
-        } else if (eta_pair[phase_index(phj)] != 0.0f && separated) {
-          force += vij * (vsum * eta_pair[phase_index(phj)] * dW / r);
+        } else {
+          const float eta_ij = phj == kVapor ? eta_pair1 : eta_pair0;
+          if (eta_ij != 0.0f && separated) force += vij * (vsum * eta_ij * dW / r);
         }
         if (alpha_i > 0.0f && phj == ph) {
           const float vr = dot(vij, rij);
@@ -611,7 +614,7 @@ __global__ void __launch_bounds__(FORCES_BLOCK, forces_min_blocks(WHAT)) k_force
       }
       // equal temperatures give a zero term that leaves q as it is
       if (thermal && Ti != vTj.w) {
-        const float kij = k_pair[phase_index(phj)];
+        const float kij = phj == kVapor ? k_pair1 : k_pair0;
         const float rgw = r * dW;
         q += Vi * Vj * kij * (Ti - vTj.w) * rgw / (r2 + eta2);
       }
