@@ -377,6 +377,11 @@ int cryo_grid_tables(cryo_ctx* ctx, uint32_t* keys, uint32_t* perm, int32_t* cel
  * (spatial_hash.hpp:37-56 filtered by r^2 < (2h)^2, self included):
  * counts[n], and the indices concatenated into list (capacity `cap`). */
 int cryo_neighbor_lists(cryo_ctx* ctx, int32_t* counts, int32_t* list, long long cap, long long* total);
+/* The same from the stored neighbour lists the passes walk (the last grid
+ * build's): fluid particles' lists as above, walls' lists hold their fluid
+ * neighbours only.  EINVAL when lists are off or no grid build ran since the
+ * load. */
+int cryo_stored_neighbor_lists(cryo_ctx* ctx, int32_t* counts, int32_t* list, long long cap, long long* total);
 /* Sets the step size used by the next pass calls (SimParams::dt). */
 int cryo_set_pass_dt(cryo_ctx* ctx, float dt);
 /* Device guard word (CRYO_DEV_* bits), cleared on read. */

@@ -282,6 +282,7 @@ def load(path=None):
         "cryo_grid_info": (i, [vp, ip, ip, ip, ip, fp, fp]),
         "cryo_grid_tables": (i, [vp, vp, vp, vp, vp]),
         "cryo_neighbor_lists": (i, [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
+        "cryo_stored_neighbor_lists": (i, [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]),
         "cryo_set_pass_dt": (i, [vp, f]),
         "cryo_device_status": (i, [vp, C.POINTER(C.c_uint)]),
         "cryo_state_size": (i, [vp, C.POINTER(C.c_size_t)]),
@@ -468,13 +469,16 @@ class Context:
         self.check(self.L.cryo_grid_tables(self.h, _ptr(keys), _ptr(perm), _ptr(cs), _ptr(ce)))
         return keys, perm, cs, ce
 
-    def neighbor_lists(self):
+    def neighbor_lists(self, stored=False):
+        """(counts, concatenated lists) in reference order.  stored=True reads
+        the stored lists the passes walk (walls: fluid neighbours only)."""
+        fn = self.L.cryo_stored_neighbor_lists if stored else self.L.cryo_neighbor_lists
         n = self.num_particles()
         counts = np.empty(n, np.int32)
         total = C.c_longlong()
-        self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), None, 0, C.byref(total)))
+        self.check(fn(self.h, _ptr(counts), None, 0, C.byref(total)))
         lst = np.empty(max(total.value, 1), np.int32)
-        self.check(self.L.cryo_neighbor_lists(self.h, _ptr(counts), _ptr(lst), total.value, C.byref(total)))
+        self.check(fn(self.h, _ptr(counts), _ptr(lst), total.value, C.byref(total)))
         return counts, lst[: total.value]
 
     def probe_pressure(self, pts):

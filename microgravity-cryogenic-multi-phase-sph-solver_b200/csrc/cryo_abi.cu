@@ -219,7 +219,10 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
   LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
   if (P.use_lists) CK(cudaMemsetAsync(cell_fluid, 0, (size_t)P.num_cells, stream));
   LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce());
-  if (P.use_lists) LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
+  if (P.use_lists) {
+    LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
+    lists_built = true;
+  }
 }
 
 // Solver::evaluate_rates (sph_solver.cu:449-480) on set s.  density_done:
@@ -646,6 +649,7 @@ void cryo_ctx::begin_load(int n, bool vap, const float* lo, const float* hi) {
   const int* old_cells = cell_begin;
   const int old_n = loaded_n;
   has_vapor = vap;
+  lists_built = false;
   const float ex = hi[0] - lo[0], ey = hi[1] - lo[1], ez = hi[2] - lo[2];
   float cl = ex;
   if (cl < ey) cl = ey;
@@ -1506,37 +1510,47 @@ int cryo_grid_tables(cryo_ctx* c, uint32_t* keys, uint32_t* perm, int32_t* cs, i
   });
 }
 
-int cryo_neighbor_lists(cryo_ctx* c, int32_t* counts, int32_t* list, long long cap, long long* total) {
-  return guard(c, [&] {
-    c->pull();
-    const int n = c->hdyn->n;
-    int* dcount = nullptr;
-    CK(cudaMallocAsync(&dcount, (size_t)std::max(n, 1) * sizeof(int), c->stream));
-    k_nbr_count<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), dcount);
+static void neighbor_dump(cryo_ctx* c, int stored, int32_t* counts, int32_t* list, long long cap, long long* total) {
+  c->pull();
+  const int n = c->hdyn->n;
+  int* dcount = nullptr;
+  CK(cudaMallocAsync(&dcount, (size_t)std::max(n, 1) * sizeof(int), c->stream));
+  k_nbr_count<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), stored, dcount);
+  LAUNCH_CHECK();
+  CK(cudaMemcpyAsync(counts, dcount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  c->sync();
+  std::vector<long long> off(n);
+  long long t = 0;
+  for (int i = 0; i < n; ++i) {
+    off[i] = t;
+    t += counts[i];
+  }
+  *total = t;
+  if (list && cap >= t && t > 0) {
+    long long* doff = nullptr;
+    int* dlist = nullptr;
+    CK(cudaMallocAsync(&doff, (size_t)n * sizeof(long long), c->stream));
+    CK(cudaMallocAsync(&dlist, (size_t)t * sizeof(int), c->stream));
+    CK(cudaMemcpyAsync(doff, off.data(), (size_t)n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+    k_nbr_fill<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), stored, doff, dlist);
     LAUNCH_CHECK();
-    CK(cudaMemcpyAsync(counts, dcount, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    c->sync();
-    std::vector<long long> off(n);
-    long long t = 0;
-    for (int i = 0; i < n; ++i) {
-      off[i] = t;
-      t += counts[i];
-    }
-    *total = t;
-    if (list && cap >= t && t > 0) {
-      long long* doff = nullptr;
-      int* dlist = nullptr;
-      CK(cudaMallocAsync(&doff, (size_t)n * sizeof(long long), c->stream));
-      CK(cudaMallocAsync(&dlist, (size_t)t * sizeof(int), c->stream));
-      CK(cudaMemcpyAsync(doff, off.data(), (size_t)n * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-      k_nbr_fill<<<c->grid_blocks(), kBlock, 0, c->stream>>>(c->P, c->view(c->cur), doff, dlist);
-      LAUNCH_CHECK();
-      CK(cudaMemcpyAsync(list, dlist, (size_t)t * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaFreeAsync(doff, c->stream));
-      CK(cudaFreeAsync(dlist, c->stream));
-    }
-    CK(cudaFreeAsync(dcount, c->stream));
-    c->sync();
+    CK(cudaMemcpyAsync(list, dlist, (size_t)t * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaFreeAsync(doff, c->stream));
+    CK(cudaFreeAsync(dlist, c->stream));
+  }
+  CK(cudaFreeAsync(dcount, c->stream));
+  c->sync();
+}
+
+int cryo_neighbor_lists(cryo_ctx* c, int32_t* counts, int32_t* list, long long cap, long long* total) {
+  return guard(c, [&] { neighbor_dump(c, 0, counts, list, cap, total); });
+}
+
+int cryo_stored_neighbor_lists(cryo_ctx* c, int32_t* counts, int32_t* list, long long cap, long long* total) {
+  return guard(c, [&] {
+    if (!c->P.use_lists || !c->lists_built)
+      throw std::invalid_argument("no neighbour lists: lists are off or no grid build ran since the load");
+    neighbor_dump(c, 1, counts, list, cap, total);
   });
 }
 
@@ -1630,6 +1644,7 @@ int cryo_load_state(cryo_ctx* c, const void* blob, size_t bytes) {
     c->push();
     c->initialized = h.initialized != 0;
     c->has_vapor = h.has_vapor != 0;
+    c->lists_built = false;
     CK(cudaMemcpyAsync(c->cell_begin, p, cells, cudaMemcpyHostToDevice, c->stream));
     c->sync();
   });
@@ -1798,6 +1813,7 @@ int cryo_set_neighbor_mode(cryo_ctx* c, int use_lists) {
     c->sync();
     c->use_lists = use_lists != 0;
     c->P.use_lists = c->use_lists ? 1 : 0;
+    c->lists_built = false;
     c->invalidate_graphs();
   });
 }

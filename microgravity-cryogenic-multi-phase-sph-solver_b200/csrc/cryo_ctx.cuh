@@ -190,6 +190,7 @@ struct cryo_ctx {
 
   // solver state on the host side
   bool has_particles = false, initialized = false, has_vapor = false;
+  bool lists_built = false;  // the neighbour lists of the current particles exist
   int loaded_n = -1;  // particle count of the last set_particles / build_tank
   float char_length = 0;
   float pass_dt = 0;
@@ -482,6 +483,7 @@ struct cryo_ctx {
     keys_a = nka; keys_b = nkb; vals_a = nva; vals_b = nvb; split_flag = nsf;
     hist = nhist; partials = npart; max_chunks = nchunks; diag_out = ndiag; ticket = ntick;
     nbr = nnbr; nbr_cnt = nnc; fluid_idx = nfi; wall_idx = nwi;
+    lists_built = false;
     sorted_keys = nullptr;
     sorted_perm = nullptr;
     capacity = cap;

@@ -334,19 +334,24 @@ __global__ void __launch_bounds__(kBlock, LIST_MIN_BLOCKS) k_build_lists(Params 
 }
 
 // Neighbour list dump (test hook): counts, then the lists at given offsets.
-__global__ void k_nbr_count(Params P, View V, int* __restrict__ counts) {
+// stored = 0: the cell scan (every neighbour); 1: the lists of the last
+// build, as the passes walk them (walls: their fluid neighbours only).
+__global__ void k_nbr_count(Params P, View V, int stored, int* __restrict__ counts) {
   const int n = V.dyn->n;
+  P.use_lists = stored;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     int c = 0;
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(V.xp[i]), [&](int, float4, V3, float) { ++c; });
+    for_each_nbr(P, V, i, xyz(V.xp[i]), [&](int, float4, V3, float) { ++c; });
     counts[i] = c;
   }
 }
-__global__ void k_nbr_fill(Params P, View V, const long long* __restrict__ offsets, int* __restrict__ list) {
+__global__ void k_nbr_fill(Params P, View V, int stored, const long long* __restrict__ offsets,
+                           int* __restrict__ list) {
   const int n = V.dyn->n;
+  P.use_lists = stored;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     long long o = offsets[i];
-    for_each_neighbor(P, V.cell_begin, V.xp, xyz(V.xp[i]), [&](int j, float4, V3, float) { list[o++] = j; });
+    for_each_nbr(P, V, i, xyz(V.xp[i]), [&](int j, float4, V3, float) { list[o++] = j; });
   }
 }
 

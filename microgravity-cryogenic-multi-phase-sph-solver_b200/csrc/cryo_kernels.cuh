@@ -153,8 +153,8 @@ __global__ void k_cells(Params P, const uint32_t* keys, DynState* dyn, int* cell
 __global__ void k_gather(Params P, View src, View dst, const uint32_t* perm, Reduce R);
 enum { LISTS_ONLY = 0, LISTS_PHASE = 1 };
 __global__ void k_build_lists(Params P, View V, Reduce R, int mode);
-__global__ void k_nbr_count(Params P, View V, int* counts);
-__global__ void k_nbr_fill(Params P, View V, const long long* offsets, int* list);
+__global__ void k_nbr_count(Params P, View V, int stored, int* counts);
+__global__ void k_nbr_fill(Params P, View V, int stored, const long long* offsets, int* list);
 
 // physics (cryo_physics.cu).  Fused rate pass; `what` selects the sub-passes (FORCE_* bits).
 enum { FORCE_TRANSPORT = 1, FORCE_MOMENTUM = 2, FORCE_CSF = 4, FORCE_AKINCI = 8, FORCE_DRHO = 16,

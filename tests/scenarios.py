@@ -160,3 +160,16 @@ def normwise(a, b):
     if scale == 0.0:
         return float(err)
     return float(err / scale)
+
+
+def assert_stored_lists(g, oc, ol, phase):
+    """The stored neighbour lists the CUDA passes walk equal the oracle's
+    lists (counts oc, concatenated lists ol), a wall's restricted to its
+    fluid neighbours (phase <= 1)."""
+    sc, sl = g.neighbor_lists(stored=True)
+    parts = np.split(ol, np.cumsum(oc)[:-1]) if len(oc) else []
+    want = [lst if phase[i] != 2 else lst[phase[lst] <= 1] for i, lst in enumerate(parts)]
+    wc = np.array([len(w) for w in want], np.int32)
+    assert np.array_equal(sc, wc), "stored neighbour list counts differ"
+    if want:
+        assert np.array_equal(sl, np.concatenate(want)), "stored neighbour lists differ (membership or order)"

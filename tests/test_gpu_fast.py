@@ -101,6 +101,7 @@ def test_fast_dam_break_at_bench_size(cuda_device):
     gc, gl = g.neighbor_lists()
     oc, ol = o.neighbor_lists()
     assert np.array_equal(gc, oc) and np.array_equal(gl, ol)
+    S.assert_stored_lists(g, oc, ol, o.field("phase"))
     g2 = cabi.Context(cfg, fl)
     g2.set_field_arithmetic(cabi.CRYO_ARITH_FAST)
     o2 = refpy.Oracle(cfg, fl)

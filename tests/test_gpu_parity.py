@@ -84,6 +84,8 @@ def test_grid_build_and_neighbor_lists_bit_exact(cuda_device, name):
     oc, ol = o.neighbor_lists()
     assert np.array_equal(gc, oc), "neighbour counts differ"
     assert np.array_equal(gl, ol), "neighbour lists differ (membership or order)"
+    # the stored lists the passes walk
+    S.assert_stored_lists(g, oc, ol, o.field("phase"))
 
 
 def pass_plan(cfg, has_vapor):

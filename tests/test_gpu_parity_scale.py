@@ -75,6 +75,7 @@ def assert_grid_bit_exact(g, o):
     oc, ol = o.neighbor_lists()
     assert np.array_equal(gc, oc), "neighbour counts differ"
     assert np.array_equal(gl, ol), "neighbour lists differ (membership or order)"
+    S.assert_stored_lists(g, oc, ol, o.field("phase"))
     return len(gl)
 
 
