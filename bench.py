@@ -848,31 +848,41 @@ def c5_solver(cs, device, dx=0.0034):
 def slab_run(cs, cfg, fluid, p, lo, hi, nslabs, devices, steps, label):
     """The workload as one tank cut along z into `nslabs` slabs of cell layers
     (CryoSPH.SlabSolver), against one Solver on the same inputs: wall clock
-    per step with the device synchronised (the slab steps meet on the host
-    between passes and run without step graphs), particle states compared
-    bit for bit after the timed steps."""
+    per step with the device synchronised, the slab steps once as the
+    captured group graph (the default) and once enqueued by host threads
+    meeting at the exchange points; particle states compared bit for bit
+    after the timed steps."""
     import torch
     one = cs.Solver(cfg, fluid, devices[0])
     load(one, p, lo, hi)
-    sl = cs.SlabSolver(cfg, fluid, slabs=nslabs, devices=devices)
-    sl.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"], domain_lo=lo,
-                     domain_hi=hi, normal=p["normal"], flags=p["flags"])
+    runs = {"one_context": one}
+    for name, graph in (("slabs", True), ("slabs_host_threads", False)):
+        sl = cs.SlabSolver(cfg, fluid, slabs=nslabs, devices=devices)
+        sl.graph_mode = graph
+        sl.set_particles(p["position"], p["mass"], p["density"], p["temperature"], p["phase"], domain_lo=lo,
+                         domain_hi=hi, normal=p["normal"], flags=p["flags"])
+        runs[name] = sl
     times = {}
-    for name, obj in (("one_context", one), ("slabs", sl)):
+    for name, obj in runs.items():
         obj.run_steps(3)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         obj.run_steps(steps)
         torch.cuda.synchronize()
         times[name] = (time.perf_counter() - t0) / steps * 1e3
-    a, b = one.particles(), sl.particles()
-    same = all(np.array_equal(np.asarray(a[k]), np.asarray(b[k])) for k in a)
+    a = one.particles()
+    same = {name: all(np.array_equal(np.asarray(a[k]), np.asarray(b[k])) for k in a)
+            for name, b in ((n, runs[n].particles()) for n in ("slabs", "slabs_host_threads"))}
+    sl = runs["slabs"]
     lay = sl.layout()
     return {"workload": label, "slabs": nslabs, "devices": devices, "steps": steps,
-            "ms_per_step": times["slabs"], "one_context_ms_per_step": times["one_context"],
+            "ms_per_step": times["slabs"], "graph_mode": sl.graph_mode,
+            "host_threads_ms_per_step": times["slabs_host_threads"],
+            "one_context_ms_per_step": times["one_context"],
             "z_begin": list(lay["z_begin"]), "owned": list(lay["owned"]), "held": list(lay["held"]),
             "ghost_fraction": sum(lay["held"]) / max(sum(lay["owned"]), 1) - 1.0,
-            "bit_identical": bool(same), "timing": "wall clock, device synchronised"}
+            "bit_identical": bool(same["slabs"] and same["slabs_host_threads"]),
+            "timing": "wall clock, device synchronised"}
 
 
 def adjoint_run(cs, device, steps, every, knots=16):

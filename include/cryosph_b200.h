@@ -502,6 +502,15 @@ const char* cryo_slabs_last_error(const cryo_slabs* s);
 int cryo_slabs_count(cryo_slabs* s, int* nslabs);
 /* Solver::set_particles of the whole tank (sph_solver.cu:407-428). */
 int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, const float* lo, const float* hi);
+/* Graph mode (default 1): the group's step (every slab's refresh and step,
+ * their exchange points as graph edges) is captured once as one CUDA graph
+ * rooted on slab 0's stream and replayed, with no host barrier inside a
+ * step; 0: one host thread per slab enqueues every step.  cryo_slabs_graph_mode
+ * reports 0 (off), 1 (steps replay the graph) or 2 (on, but the runtime
+ * refused the capture, e.g. across devices that cannot share a graph: the
+ * steps run as in mode 0). */
+int cryo_slabs_set_graph_mode(cryo_slabs* s, int enable);
+int cryo_slabs_graph_mode(cryo_slabs* s, int* mode);
 /* Solver::run_steps (sph_solver.cu:535-538) of the whole tank. */
 int cryo_slabs_run_steps(cryo_slabs* s, long long n);
 int cryo_slabs_num_particles(cryo_slabs* s, int* n);

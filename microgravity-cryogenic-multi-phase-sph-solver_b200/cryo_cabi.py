@@ -308,6 +308,8 @@ def load(path=None):
         "cryo_slabs_count": (i, [vp, ip]),
         "cryo_slabs_set_particles": (i, [vp, C.POINTER(HostParticles), fp, fp]),
         "cryo_slabs_run_steps": (i, [vp, C.c_longlong]),
+        "cryo_slabs_set_graph_mode": (i, [vp, i]),
+        "cryo_slabs_graph_mode": (i, [vp, ip]),
         "cryo_slabs_num_particles": (i, [vp, ip]),
         "cryo_slabs_download": (i, [vp, C.POINTER(HostParticlesOut)]),
         "cryo_slabs_diagnostics": (i, [vp, C.POINTER(Diagnostics)]),
@@ -593,6 +595,15 @@ class Slabs:
 
     def step(self, n=1):
         self.check(self.L.cryo_slabs_run_steps(self.h, int(n)))
+
+    def set_graph_mode(self, on):
+        self.check(self.L.cryo_slabs_set_graph_mode(self.h, 1 if on else 0))
+
+    def graph_mode(self):
+        """0 off, 1 the steps replay the group graph, 2 on but the capture was refused."""
+        m = C.c_int()
+        self.check(self.L.cryo_slabs_graph_mode(self.h, C.byref(m)))
+        return m.value
 
     def num_particles(self):
         n = C.c_int()

@@ -11,6 +11,13 @@
 // barrier), so each slab's stream can wait on its neighbours' events before
 // it reads their memory, and they wait on its events before they overwrite
 // what it read.  No kernel waits on another slab's kernel.
+//
+// In graph mode (the default) that enqueue runs once, under stream capture:
+// slab 0's stream forks into every other slab's stream, the exchange points
+// become graph edges between the slabs' kernels, and every stream joins back
+// into slab 0's.  The steps then replay that one graph, with no host thread
+// or barrier inside a step.  A group whose capture the runtime refuses (for
+// instance across devices that cannot share one graph) steps without it.
 namespace {
 
 class HostBarrier {
@@ -64,6 +71,15 @@ struct SlabGroup {
   std::vector<float4*> spare;         // per slab: a4 / ab4 of a refresh (2 x capacity)
   std::vector<int> spare_cap;
   HostBarrier barrier;
+  // the captured group step (graph mode)
+  bool graph_mode = true;
+  bool graph_refused = false;  // the runtime refused the capture: eager steps
+  cudaGraphExec_t gexec = nullptr;
+  cudaEvent_t ev_fork = nullptr;
+  std::vector<cudaEvent_t> ev_join;
+  std::vector<unsigned long long> graph_gen;  // each slab's graph generation at capture
+  std::vector<float4*> graph_spare;
+  std::vector<int> graph_cur;
 
   explicit SlabGroup(int n) : barrier(n) {}
   int count() const { return (int)slabs.size(); }
@@ -129,9 +145,10 @@ struct SlabGroup {
   }
 
   // Runs body(r) for every slab in its own thread; the first failure is
-  // rethrown after every thread has ended.
+  // rethrown after every thread has ended.  sync: wait for the streams
+  // afterwards (not while they are being captured).
   template <class F>
-  void lockstep(F&& body) {
+  void lockstep(F&& body, bool sync = true) {
     barrier.reset();
     const int R = count();
     std::vector<std::exception_ptr> errs(R);
@@ -148,7 +165,8 @@ struct SlabGroup {
         }
       });
     for (auto& t : th) t.join();
-    for (cryo_ctx* c : slabs) cudaStreamSynchronize(c->stream);
+    if (sync)
+      for (cryo_ctx* c : slabs) cudaStreamSynchronize(c->stream);
     // a real error first, not another thread's "another slab failed"
     for (int pass = 0; pass < 2; ++pass)
       for (int r = 0; r < R; ++r) {
@@ -198,16 +216,113 @@ struct SlabGroup {
     check();
   }
 
+  void drop_graph() {
+    if (gexec) cudaGraphExecDestroy(gexec);
+    gexec = nullptr;
+  }
+  // The captured step is valid while no slab re-allocated or re-sized its
+  // grids (its graph generation) and the spare arrays and buffer parities
+  // are those of the capture.
+  bool graph_current() const {
+    if (!gexec) return false;
+    for (int r = 0; r < count(); ++r)
+      if (slabs[r]->generation != graph_gen[r] || spare[r] != graph_spare[r] || slabs[r]->cur != graph_cur[r])
+        return false;
+    return true;
+  }
+  // One step of every slab (refresh + step) captured into one graph rooted
+  // on slab 0's stream.  Returns false when the runtime refused the capture.
+  bool capture() {
+    drop_graph();
+    const int R = count();
+    for (cryo_ctx* c : slabs) c->size_grids();
+    if (!ev_fork) CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    if ((int)ev_join.size() != R) {
+      ev_join.assign(R, nullptr);
+      for (int r = 0; r < R; ++r) {
+        CK(cudaSetDevice(slabs[r]->device));
+        CK(cudaEventCreateWithFlags(&ev_join[r], cudaEventDisableTiming));
+      }
+    }
+    std::vector<unsigned long long> gen(R);
+    std::vector<int> cur(R);
+    for (int r = 0; r < R; ++r) {
+      gen[r] = slabs[r]->generation;
+      cur[r] = slabs[r]->cur;
+    }
+    cryo_ctx* c0 = slabs[0];
+    CK(cudaSetDevice(c0->device));
+    CK(cudaStreamSynchronize(c0->stream));
+    CK(cudaStreamBeginCapture(c0->stream, cudaStreamCaptureModeRelaxed));
+    cudaGraph_t g = nullptr;
+    try {
+      CK(cudaEventRecord(ev_fork, c0->stream));
+      for (int r = 1; r < R; ++r) {
+        CK(cudaSetDevice(slabs[r]->device));
+        CK(cudaStreamWaitEvent(slabs[r]->stream, ev_fork, 0));
+      }
+      lockstep([&](int r) {
+        refresh(r);
+        slabs[r]->launch_step();
+      }, false);
+      for (int r = 1; r < R; ++r) {
+        CK(cudaSetDevice(slabs[r]->device));
+        CK(cudaEventRecord(ev_join[r], slabs[r]->stream));
+        CK(cudaSetDevice(c0->device));
+        CK(cudaStreamWaitEvent(c0->stream, ev_join[r], 0));
+      }
+      CK(cudaSetDevice(c0->device));
+      CK(cudaStreamEndCapture(c0->stream, &g));
+      CK(cudaGraphInstantiate(&gexec, g, 0));
+      CK(cudaGraphDestroy(g));
+    } catch (...) {
+      cudaSetDevice(c0->device);
+      cudaGraph_t bad = nullptr;
+      cudaStreamEndCapture(c0->stream, &bad);
+      if (bad) cudaGraphDestroy(bad);
+      if (g) cudaGraphDestroy(g);
+      gexec = nullptr;
+      (void)cudaGetLastError();
+      // the capture enqueued nothing; the host side of the step (buffer
+      // parities) is put back
+      for (int r = 0; r < R; ++r) slabs[r]->cur = cur[r];
+      try {
+        throw;
+      } catch (const CudaError&) {
+        return false;  // refused by the runtime: the group steps without a graph
+      }
+    }
+    // the capture only recorded the step: the parities it flipped are the
+    // ones the replay flips, and every step returns them to these values
+    for (int r = 0; r < R; ++r) slabs[r]->cur = cur[r];
+    graph_gen = gen;
+    graph_spare = spare;
+    graph_cur = cur;
+    return true;
+  }
+
   void run(long long n) {
     initialize();
     while (n > 0) {
       const int k = (int)std::min<long long>(n, 16);
-      lockstep([&](int r) {
-        for (int q = 0; q < k; ++q) {
-          refresh(r);
-          slabs[r]->launch_step();
+      bool done = false;
+      if (graph_mode && !graph_refused) {
+        if (!graph_current() && !capture()) graph_refused = true;
+        if (!graph_refused) {
+          cryo_ctx* c0 = slabs[0];
+          CK(cudaSetDevice(c0->device));
+          for (int q = 0; q < k; ++q) CK(cudaGraphLaunch(gexec, c0->stream));
+          CK(cudaStreamSynchronize(c0->stream));
+          done = true;
         }
-      });
+      }
+      if (!done)
+        lockstep([&](int r) {
+          for (int q = 0; q < k; ++q) {
+            refresh(r);
+            slabs[r]->launch_step();
+          }
+        });
       check();
       n -= k;
     }
@@ -216,6 +331,10 @@ struct SlabGroup {
   ~SlabGroup() {  // also after a failed create: slabs not made yet are null
     for (cryo_ctx* c : slabs)
       if (c && c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph();
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    for (cudaEvent_t e : ev_join)
+      if (e) cudaEventDestroy(e);
     for (size_t r = 0; r < slabs.size(); ++r) {
       if (r < spare.size() && spare[r]) cudaFree(spare[r]);
       if (r < dyn_table.size() && dyn_table[r]) cudaFree(dyn_table[r]);
@@ -370,6 +489,7 @@ int cryo_slabs_count(cryo_slabs* s, int* nslabs) {
 int cryo_slabs_set_particles(cryo_slabs* s, const cryo_host_particles_t* p, const float* lo, const float* hi) {
   return slab_guard(s, [&] {
     SlabGroup& G = *s->g;
+    G.drop_graph();
     const int n = p->n;
     if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
     bool vap = false;
@@ -451,6 +571,26 @@ int cryo_slabs_layout(cryo_slabs* s, int* z_begin, int* owned, int* held) {
       if (owned) owned[r] = (d.own_hi - d.own_lo) + (d.n - d.n_sorted);
       if (held) held[r] = d.n;
     }
+  });
+}
+
+int cryo_slabs_set_graph_mode(cryo_slabs* s, int enable) {
+  return slab_guard(s, [&] {
+    SlabGroup& G = *s->g;
+    for (cryo_ctx* c : G.slabs) {
+      CK(cudaSetDevice(c->device));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    G.graph_mode = enable != 0;
+    G.graph_refused = false;
+    G.drop_graph();
+  });
+}
+
+int cryo_slabs_graph_mode(cryo_slabs* s, int* mode) {
+  return slab_guard(s, [&] {
+    const SlabGroup& G = *s->g;
+    *mode = !G.graph_mode ? 0 : (G.graph_refused ? 2 : 1);
   });
 }
 

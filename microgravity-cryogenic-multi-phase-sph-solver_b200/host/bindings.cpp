@@ -674,6 +674,10 @@ PYBIND11_MODULE(CryoSPH, m) {
           "The whole tank's particles, in the order a Solver's arrays have.")
       .def_property_readonly("num_particles", &SlabSolver::num_particles)
       .def_property_readonly("slabs", &SlabSolver::slabs)
+      .def_property(
+          "graph_mode", &SlabSolver::graph_mode, [](SlabSolver& s, bool on) { s.set_graph_mode(on); },
+          "True (default): every step replays one captured CUDA graph of all slabs; False: host threads per slab. "
+          "Reads 0 (off), 1 (graph) or 2 (on, but the capture was refused and the steps run without it).")
       .def(
           "layout",
           [](const SlabSolver& s) {

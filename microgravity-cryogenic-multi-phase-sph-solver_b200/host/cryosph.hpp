@@ -470,6 +470,10 @@ class SlabSolver {
   void download(cryo_host_particles_out_t& out) const;
   std::size_t num_particles() const;
   int slabs() const noexcept { return slabs_; }
+  // 1 (default): the group's step is one captured CUDA graph; 0: host
+  // threads per slab.  graph_mode() reports 0, 1, or 2 (on, capture refused).
+  void set_graph_mode(bool on);
+  int graph_mode() const;
   // cell-layer boundaries (slabs + 1 entries), then per slab the particles
   // it owns and the particles its context holds (owned + ghost copies)
   std::tuple<std::vector<int>, std::vector<int>, std::vector<int>> layout() const;

@@ -537,6 +537,14 @@ void SlabSolver::build_tank(const Geometry& geometry, const FillSpec& fill) {
 
 void SlabSolver::run_steps(long long n) { check(cryo_slabs_run_steps(s_, n)); }
 
+void SlabSolver::set_graph_mode(bool on) { check(cryo_slabs_set_graph_mode(s_, on ? 1 : 0)); }
+
+int SlabSolver::graph_mode() const {
+  int m = 0;
+  check(cryo_slabs_graph_mode(s_, &m));
+  return m;
+}
+
 Diagnostics SlabSolver::diagnostics() {
   cryo_diagnostics_t d{};
   check(cryo_slabs_diagnostics(s_, &d));

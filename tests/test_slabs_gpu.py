@@ -74,8 +74,30 @@ def test_slabs_equal_one_context(cuda_device, name, nslabs):
     zb, owned, held = s.layout()
     print(f"\n[{name} x{nslabs}] layers {zb.tolist()} owned {owned.tolist()} held {held.tolist()}")
     assert owned.sum() == len(ref["x"])
+    assert s.graph_mode() == 1, "the slab steps should replay the captured group graph"
     assert_same(ref, got, f"{name} x{nslabs}")
     assert_diag_close(d_ref, d_got, f"{name} x{nslabs}")
+
+
+def test_slab_graph_and_host_threads_agree(cuda_device):
+    """The captured group step (graph mode, the default) and the same steps
+    enqueued by one host thread per slab meeting at barriers give the same
+    particles bit for bit, with splits inside the window and steps issued in
+    several calls (re-captures after capacity changes included)."""
+    cfg, fl, parts, lo, hi = S.ln2_boiloff()
+    cfg.update(split_ratio=1.02, lee_evaporation=200.0)
+    runs = []
+    for graph in (True, False):
+        s = cabi.Slabs(cfg, fl, 3)
+        s.set_graph_mode(graph)
+        s.set_particles(parts, lo, hi)
+        for k in (1, 7, 16, 6):
+            s.step(k)
+        assert s.graph_mode() == (1 if graph else 0)
+        runs.append((s.particles(), s.diagnostics()))
+    assert runs[0][1].splits > 0, "the case should split particles"
+    assert_same(runs[1][0], runs[0][0], "graph vs host threads")
+    assert_diag_close(runs[1][1], runs[0][1], "graph vs host threads")
 
 
 def test_slabs_with_splits(cuda_device):
@@ -140,3 +162,6 @@ def test_slab_solver_python_api(cuda_device):
     lay = sl.layout()
     assert len(lay["z_begin"]) == 4 and sum(lay["owned"]) == one.num_particles
     assert sl.diagnostics().step == one.diagnostics().step == 10
+    assert sl.graph_mode == 1
+    sl.graph_mode = False
+    assert sl.graph_mode == 0
