@@ -242,16 +242,58 @@ def load(solver, p, lo, hi):
 
 # ---------------------------------------------------------------- clocks
 class Clocks:
+    """SM clock and clock-event reasons sampled while the timed steps run.
+    NVML is read every ~1 ms from a background thread (the timed region of a
+    short run lasts a few milliseconds); where NVML cannot be opened,
+    nvidia-smi samples every 200 ms."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"))
 
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.path = None
+        self.nvml = None
+        self.rows = []
+
+    def _open_nvml(self):
+        import threading
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        prop = torch.cuda.get_device_properties(self.device)
+        bus = f"{prop.pci_domain_id:08x}:{prop.pci_bus_id:02x}:{prop.pci_device_id:02x}.0"
+        h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(h, pynvml.NVML_CLOCK_SM))
+        self.bits = {name: getattr(pynvml, attr) for name, attr in self.REASONS}
+
+        def sample():
+            self.rows.append((float(pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)),
+                              int(pynvml.nvmlDeviceGetCurrentClocksEventReasons(h))))
+
+        sample()
+        self.stop = threading.Event()
+
+        def run():
+            while not self.stop.is_set():
+                sample()
+                time.sleep(0.001)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        self.nvml = pynvml
 
     def __enter__(self):
+        try:
+            self._open_nvml()
+            return self
+        except Exception:
+            self.nvml = None
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
         try:
@@ -263,6 +305,13 @@ class Clocks:
         return self
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -271,6 +320,13 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
+        if self.nvml:
+            rows = list(self.rows)
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+            reasons = sorted({name for _, r in rows for name, bit in self.bits.items() if r & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": self.max_mhz,
+                    "reasons": reasons, "samples": len(rows), "source": "NVML, every ~1 ms"}
         rows = []
         try:
             with open(self.path) as fh:
@@ -278,7 +334,7 @@ class Clocks:
                     parts = [s.strip() for s in line.split(",")]
                     if len(parts) >= 9:
                         rows.append(parts)
-        except OSError:
+        except (OSError, TypeError):
             pass
         finally:
             if self.path and os.path.exists(self.path):
@@ -290,7 +346,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, every 200 ms"}
 
 
 # ------------------------------------------------------------- reference arm
@@ -569,7 +625,7 @@ def main():
                        "execution": "CUDA graph per step"},
             "per_gpu": value / world,
             "gpu_launches": per_step * args.steps,
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": {k: clocks.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples", "source")},
             "e2e": e2e,
             "roofline": roof,
             "cpu_baseline": cpu,
@@ -623,7 +679,7 @@ def batched_main(args, cs, rank, world, local):
             "back_to_back": n_all / (ms_s / 1e3), "back_to_back_ms_per_step": ms_s, "speedup": ms_s / ms_e,
             "branches": b["branches"], "steps_per_launch": b["steps_per_launch"],
             "gpu_launches": b["gpu_launches_per_step"] * b["steps"], "diagnostics_bit_identical": differs == 0.0,
-            "clocks": {"sm_mhz": clocks["sm_mhz"], "sm_max_mhz": clocks["sm_max_mhz"], "reasons": clocks["reasons"]},
+            "clocks": {k: clocks.get(k) for k in ("sm_mhz", "sm_max_mhz", "reasons", "samples", "source")},
         }))
     if dist:
         dist.barrier()
