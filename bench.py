@@ -696,11 +696,15 @@ def ctypes_int(L, fn, handle):
 
 def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, arith=None):
     """Public-API run with host buffers: the state upload, then per step the
-    frame-motion input (host->device) and the diagnostics (device->host), then
-    the state download.  Device-timed per step with L2 flushed between steps.
-    The same sequence runs once untimed first (`warmup` steps): the solver's
-    device storage and step graphs are then in place, and the timed upload of
-    the same-sized state reuses them, as a loop of runs on one Solver does."""
+    frame-motion input (host->device) and the step's diagnostics
+    (device->host), then the state download.  The diagnostics go through
+    request_diagnostics / fetch_diagnostics as a control loop reads them: each
+    step's record is requested after the step and read while the next step
+    runs (the last one at the end of the last step).  Device-timed per step
+    with L2 flushed between steps.  The same sequence runs once untimed first
+    (`warmup` steps): the solver's device storage and step graphs are then in
+    place, and the timed upload of the same-sized state reuses them, as a loop
+    of runs on one Solver does."""
     import torch
     solver = cs.Solver(cfg, fluid, device)
     if arith is not None:
@@ -723,8 +727,11 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, a
             a = 0.01 * math.sin(0.01 * k)
             solver.set_frame_motion(acceleration=(a, 0.0, 0.0))
             solver.step()
-            d = solver.diagnostics()
-            _ = d.slosh_force
+            solver.request_diagnostics()
+            if k > 0:  # the previous step's record
+                _ = solver.fetch_diagnostics().slosh_force
+            if k == k_steps - 1:  # and this one's, at the end
+                _ = solver.fetch_diagnostics().slosh_force
             t2 = time.perf_counter()
             if k == k_steps - 1:
                 parts = solver.particles()
@@ -754,7 +761,9 @@ def e2e_run(cs, cfg, fluid, p, lo, hi, steps, device, stream, flush, warmup=3, a
             "h2d_bytes_per_step": int(state_in / steps + ctl), "d2h_bytes_per_step": int(diag + state_out / steps),
             "steps": steps, "host_wall_ms": {k: round(v, 3) for k, v in host.items()},
             "timing": "CUDA events per step (host work inside), L2 flushed between steps; one untimed run of the "
-                      "same sequence first"}
+                      "same sequence first",
+            "diagnostics": "every step's record read on the host: requested after the step, fetched while the next "
+                           "step runs (request_diagnostics / fetch_diagnostics)"}
 
 
 # SPHERIC Test 2 pressure sensors (validation/spheric_test2/run.py:30-33,69-73

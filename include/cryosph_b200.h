@@ -280,6 +280,15 @@ int cryo_capacity(cryo_ctx* ctx, int* capacity);
 
 /* Solver::diagnostics (sph_solver.cu:609-653). */
 int cryo_diagnostics(cryo_ctx* ctx, cryo_diagnostics_t* out);
+/* The same record without blocking the caller (no counterpart in the
+ * reference): request enqueues the reduction of the current state and its
+ * copy into a pinned slot on the solver's stream; fetch returns the oldest
+ * pending result in request order (*got = 1), waiting for it when wait != 0,
+ * else *got = 0 while it is not ready or nothing is pending.  At most 8
+ * requests pending (EINVAL beyond).  A control loop requests after each step
+ * and fetches the previous step's record while the next step runs. */
+int cryo_diagnostics_request(cryo_ctx* ctx);
+int cryo_diagnostics_fetch(cryo_ctx* ctx, cryo_diagnostics_t* out, int wait, int* got);
 
 /* Solver::particles (persistent arrays).  out->n must be >= the particle count;
  * on return out->n holds the count. */

@@ -263,6 +263,8 @@ def load(path=None):
         "cryo_num_particles": (i, [vp, ip]),
         "cryo_capacity": (i, [vp, ip]),
         "cryo_diagnostics": (i, [vp, C.POINTER(Diagnostics)]),
+        "cryo_diagnostics_request": (i, [vp]),
+        "cryo_diagnostics_fetch": (i, [vp, C.POINTER(Diagnostics), i, ip]),
         "cryo_download": (i, [vp, vp]),
         "cryo_get_field": (i, [vp, i, vp, C.c_size_t]),
         "cryo_set_field": (i, [vp, i, vp, C.c_size_t]),
@@ -448,6 +450,15 @@ class Context:
         d = Diagnostics()
         self.check(self.L.cryo_diagnostics(self.h, C.byref(d)))
         return d
+
+    def request_diagnostics(self):
+        self.check(self.L.cryo_diagnostics_request(self.h))
+
+    def fetch_diagnostics(self, wait=True):
+        """The oldest requested Diagnostics, or None (not ready / none pending)."""
+        d, got = Diagnostics(), C.c_int()
+        self.check(self.L.cryo_diagnostics_fetch(self.h, C.byref(d), 1 if wait else 0, C.byref(got)))
+        return d if got.value else None
 
     def time(self):
         t, s, dt = C.c_double(), C.c_longlong(), C.c_double()

@@ -1050,6 +1050,49 @@ int cryo_diagnostics(cryo_ctx* c, cryo_diagnostics_t* o) {
   });
 }
 
+int cryo_diagnostics_request(cryo_ctx* c) {
+  return guard(c, [&] {
+    c->ensure_initialized();
+    if (c->diag_head - c->diag_tail >= cryo_ctx::kDiagSlots)
+      throw std::invalid_argument("cryo_diagnostics_request: " + std::to_string(cryo_ctx::kDiagSlots) +
+                                  " requests are pending; fetch one first");
+    if (!c->diag_ring) {
+      CK(cudaMallocHost(&c->diag_ring, (size_t)cryo_ctx::kDiagSlots * 64 * sizeof(double)));
+      for (int k = 0; k < cryo_ctx::kDiagSlots; ++k)
+        CK(cudaEventCreateWithFlags(&c->diag_ev[k], cudaEventDisableTiming));
+    }
+    const int slot = (int)(c->diag_head % cryo_ctx::kDiagSlots);
+    const int G = c->grid_blocks();
+    k_diagnostics<<<G, kBlock, 0, c->stream>>>(c->P, c->view(c->cur), c->reduce(), c->diag_out);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(c->diag_ring + (size_t)slot * 64, c->diag_out, 44 * sizeof(double), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaEventRecord(c->diag_ev[slot], c->stream));
+    ++c->diag_head;
+  });
+}
+
+int cryo_diagnostics_fetch(cryo_ctx* c, cryo_diagnostics_t* o, int wait, int* got) {
+  return guard(c, [&] {
+    *got = 0;
+    if (c->diag_tail == c->diag_head) return;
+    const int slot = (int)(c->diag_tail % cryo_ctx::kDiagSlots);
+    if (wait) {
+      CK(cudaEventSynchronize(c->diag_ev[slot]));
+    } else {
+      const cudaError_t e = cudaEventQuery(c->diag_ev[slot]);
+      if (e == cudaErrorNotReady) {
+        (void)cudaGetLastError();
+        return;
+      }
+      CK(e);
+    }
+    diag_fill(c->diag_ring + (size_t)slot * 64, o);
+    ++c->diag_tail;
+    *got = 1;
+  });
+}
+
 // The Diagnostics record from the k_diagnostics output row.
 }  // extern "C"
 void cryo::diag_fill(const double* v, cryo_diagnostics_t* o) {

@@ -170,6 +170,12 @@ struct cryo_ctx {
   DynState* dyn = nullptr;   // device
   DynState* hdyn = nullptr;  // pinned host mirror
   double* diag_host = nullptr;  // pinned, 64 doubles
+  // Non-blocking diagnostics (cryo_diagnostics_request / _fetch): a FIFO of
+  // pinned result rows, each completed by an event on the stream.
+  static constexpr int kDiagSlots = 8;
+  double* diag_ring = nullptr;  // pinned, kDiagSlots rows of 64 doubles (made on first request)
+  cudaEvent_t diag_ev[kDiagSlots] = {};
+  long long diag_head = 0, diag_tail = 0;  // requests made, results fetched
   // Host-owned frame state (authoritative unless a manoeuvre table drives the
   // frame on the device); updates go out through a ring of pinned slots.
   DynState::Frame hframe{};
@@ -337,6 +343,9 @@ struct cryo_ctx {
     if (dyn) cudaFree(dyn);
     if (hdyn) cudaFreeHost(hdyn);
     if (diag_host) cudaFreeHost(diag_host);
+    if (diag_ring) cudaFreeHost(diag_ring);
+    for (cudaEvent_t e : diag_ev)
+      if (e) cudaEventDestroy(e);
     if (frame_ring) cudaFreeHost(frame_ring);
     for (cudaEvent_t e : frame_ev)
       if (e) cudaEventDestroy(e);

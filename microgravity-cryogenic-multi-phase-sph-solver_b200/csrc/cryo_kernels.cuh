@@ -52,11 +52,28 @@ __device__ inline void neumaier_pair(double& s, double& c, double s2, double c2)
 // t, t + blockDim, ... (compensated), the 32 lanes of a warp combine in a
 // fixed down-shift tree, and thread 0 combines the warps in order.  Every
 // thread of the block must call it; the result is valid in thread 0.
+// Compensated sum of p[k] for k = k0, k0 + step, ... below n, in that order;
+// the loads go out kBatch at a time ahead of the additions, so a thread
+// waits on one round trip per batch instead of one per element.
+__device__ inline void strided_neumaier(const double* p, int k0, int step, int n, double& s, double& c) {
+  constexpr int kBatch = 8;
+  for (int kb = k0; kb < n; kb += kBatch * step) {
+    double x[kBatch];
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u) {
+      const int k = kb + u * step;
+      x[u] = k < n ? __ldcg(p + k) : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < kBatch; ++u)
+      if (kb + u * step < n) neumaier(s, c, x[u]);
+  }
+}
 __device__ inline double block_sum_partials(const Reduce& R, int v, int nchunks) {
   __shared__ double ws[kBlock / 32], wc[kBlock / 32];
   double s = 0, c = 0;
   const double* p = R.partials + (size_t)v * R.max_chunks;
-  for (int k = threadIdx.x; k < nchunks; k += blockDim.x) neumaier(s, c, __ldcg(p + k));
+  strided_neumaier(p, threadIdx.x, blockDim.x, nchunks, s, c);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double s2 = __shfl_down_sync(0xffffffffu, s, o), c2 = __shfl_down_sync(0xffffffffu, c, o);
@@ -85,7 +102,7 @@ __device__ inline double warp_sum_partials(const Reduce& R, int v, int nchunks) 
   const int lane = threadIdx.x & 31;
   double s = 0, c = 0;
   const double* p = R.partials + (size_t)v * R.max_chunks;
-  for (int k = lane; k < nchunks; k += 32) neumaier(s, c, __ldcg(p + k));
+  strided_neumaier(p, lane, 32, nchunks, s, c);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     const double s2 = __shfl_down_sync(0xffffffffu, s, o), c2 = __shfl_down_sync(0xffffffffu, c, o);

@@ -475,6 +475,22 @@ PYBIND11_MODULE(CryoSPH, m) {
            py::call_guard<py::gil_scoped_release>())
       .def("next_dt", &Solver::next_dt)
       .def("diagnostics", &Solver::diagnostics)
+      .def("request_diagnostics", &Solver::request_diagnostics,
+           "Enqueues the diagnostics of the current state without waiting (fetch them with fetch_diagnostics).")
+      .def(
+          "fetch_diagnostics",
+          [](Solver& s, bool wait) -> py::object {
+            Diagnostics d;
+            bool got;
+            {
+              py::gil_scoped_release nogil;
+              got = s.fetch_diagnostics(d, wait);
+            }
+            return got ? py::cast(d) : py::none();
+          },
+          py::arg("wait") = true,
+          "The oldest requested diagnostics, in request order; None while not ready (wait=False) or when none is "
+          "pending.")
       .def(
           "particles", [](const Solver& s) { return state_dict(s); },
           "Copies the particle state into a dict of NumPy arrays.")

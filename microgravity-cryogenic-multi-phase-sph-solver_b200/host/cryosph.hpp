@@ -336,6 +336,11 @@ class Solver {
   double next_dt();
 
   Diagnostics diagnostics();
+  // Non-blocking diagnostics: request after a step, fetch in request order
+  // (false while the oldest result is not ready and wait is false, or when
+  // nothing is pending).
+  void request_diagnostics();
+  bool fetch_diagnostics(Diagnostics& out, bool wait = true);
   HostParticles particles() const;
   // particles() into caller-owned arrays (out.n >= num_particles())
   void download(cryo_host_particles_out_t& out) const;

@@ -250,6 +250,16 @@ Diagnostics Solver::diagnostics() {
   return to_diagnostics(d);
 }
 
+void Solver::request_diagnostics() { check(cryo_diagnostics_request(ctx_)); }
+
+bool Solver::fetch_diagnostics(Diagnostics& out, bool wait) {
+  cryo_diagnostics_t d{};
+  int got = 0;
+  check(cryo_diagnostics_fetch(ctx_, &d, wait ? 1 : 0, &got));
+  if (got) out = to_diagnostics(d);
+  return got != 0;
+}
+
 HostParticles Solver::particles() const {
   HostParticles h;
   cryo_host_particles_out_t o = soa_sink(h, num_particles());

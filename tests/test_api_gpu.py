@@ -259,3 +259,45 @@ def test_particles_round_trip_through_the_soa_transfers(cuda_device):
     q = solver.particles()
     assert not q["velocity"].any() and not q["normal"].any() and not q["flags"].any()
     assert np.array_equal(q["id"], np.arange(n))
+
+
+def test_diagnostics_requested_without_blocking_equal_the_blocking_ones(cuda_device):
+    """request_diagnostics after each step and fetch_diagnostics later (in
+    request order) give the records a twin solver's blocking diagnostics()
+    gives after the same steps; nothing pending gives None; at most 8
+    requests may be pending."""
+    ln2 = cs.FluidProperties.liquid_nitrogen()
+    cfg = small_config(dx=0.004, gravity=(0.0, 0.0, -9.81e-4), heater_power=5.0)
+    fill = cs.FillSpec()
+    fill.fill_fraction = 0.5
+    geo = cs.CylinderTank(0.03, 0.06)
+    a, b = cs.Solver(cfg, ln2), cs.Solver(cfg, ln2)
+    a.build_tank(geo, fill)
+    b.build_tank(geo, fill)
+    assert a.fetch_diagnostics() is None
+    want = []
+    for k in range(6):
+        a.set_frame_motion(acceleration=(0.02 * k, 0.0, 0.0))
+        b.set_frame_motion(acceleration=(0.02 * k, 0.0, 0.0))
+        a.step()
+        b.step()
+        a.request_diagnostics()
+        want.append(b.diagnostics())
+        if k >= 1:  # the previous step's record, while this one may still run
+            got = a.fetch_diagnostics()
+            ref = want[k - 1]
+            for f in ("time", "step", "dt", "mass_total", "kinetic_energy", "enthalpy", "p_ullage", "T_sat",
+                      "heat_input", "max_speed"):
+                assert getattr(got, f) == getattr(ref, f), f
+            assert tuple(got.slosh_force) == tuple(ref.slosh_force)
+    last = a.fetch_diagnostics(wait=True)
+    assert last.step == want[-1].step and last.kinetic_energy == want[-1].kinetic_energy
+    assert a.fetch_diagnostics(wait=False) is None
+    for _ in range(8):
+        a.request_diagnostics()
+    with pytest.raises(Exception):
+        a.request_diagnostics()
+    n = 0
+    while a.fetch_diagnostics() is not None:
+        n += 1
+    assert n == 8
