@@ -1249,7 +1249,12 @@ def roofline(cs, cabi, L, cfg, fluid, p, lo, hi, steps, n_fluid, n_wall, has_vap
     achieved = alg / (avg_ms / 1e3) / 1e9
     traffic = ncu_traffic(top[0], label)
     return {"kernel": top[0], "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "ncu_utilisation": ncu_utilisation(top[0], label),
+            "frac": achieved / peak, "traffic": traffic,
+            "traffic_cold": ncu_traffic(top[0], label, cold=True),
+            "traffic_note": "DRAM bytes per launch from one ncu launch list of this command with the L2 as the timed "
+                            "steps leave it (--cache-control none; flushed between steps only); traffic_cold: the "
+                            "same with the L2 flushed before the kernel",
+            "ncu_utilisation": ncu_utilisation(top[0], label),
             "algorithmic_bytes": alg, "avg_launch_ms": avg_ms,
             "share": top[1] / total if total else None, "peak_source": "measured" if peaks else "fallback",
             "kernels": {r[0]: {"ms_per_step": r[1] / steps, "launches": r[2]} for r in sorted(rows, key=lambda r: -r[1])}}
@@ -1275,13 +1280,14 @@ def ncu_utilisation(kernel, label):
         return None
 
 
-def ncu_traffic(kernel, label):
-    """DRAM bytes per launch of `kernel` from the committed ncu summary (null if absent)."""
+def ncu_traffic(kernel, label, cold=False):
+    """DRAM bytes per launch of `kernel` in the step (L2 as the timed steps leave it; cold=True: L2 flushed
+    before the kernel) from the committed ncu launch list (null if absent)."""
     path = os.path.join(REPO, "profiles", "ncu_dram.json")
     try:
         with open(path) as fh:
             d = json.load(fh)
-        e = d.get(label, {}).get(kernel)
+        e = (d.get("cold", {}) if cold else d).get(label, {}).get(kernel)
         return None if e is None else float(e)
     except (OSError, ValueError):
         return None
