@@ -243,6 +243,28 @@ uintptr_t cryo_stream(const cryo_ctx* ctx);
 /* Solver::set_particles (sph_solver.cu:407-428).  domain_lo/hi: float[3]. */
 int cryo_set_particles(cryo_ctx* ctx, const cryo_host_particles_t* p, const float* domain_lo,
                        const float* domain_hi);
+/* The same particle set with each float column given as float or as double
+ * (no counterpart in the reference, whose upload takes one element type).
+ * Callers holding double-precision arrays (NumPy's default) pass them as
+ * they are: each value is rounded to float, as a C cast rounds it, while the
+ * copy threads move it into the transfer buffer, so no converted copy of the
+ * caller's arrays is made.  x / v / nrm hold n*3 values, m / rho / T n values;
+ * the matching *_f64 flag is 1 for double, 0 for float. */
+typedef struct cryo_host_columns {
+  int n;
+  const void* x;
+  const void* v;
+  const void* nrm;
+  const void* m;
+  const void* rho;
+  const void* T;
+  int x_f64, v_f64, nrm_f64, m_f64, rho_f64, T_f64;
+  const uint8_t* phase;
+  const uint8_t* flags;
+  const uint32_t* id;
+} cryo_host_columns_t;
+int cryo_set_particles_columns(cryo_ctx* ctx, const cryo_host_columns_t* p, const float* domain_lo,
+                               const float* domain_hi);
 
 /* Solver::build_tank (sph_solver.cu:430-437) with the lattice generated on
  * the device: build_tank_particles (geometry.cpp:242-330) evaluated per

@@ -183,30 +183,44 @@ __global__ void __launch_bounds__(kBlock) k_frame_viewer(int n, View V, Reduce R
 namespace {
 
 // Host copies between the caller's arrays and the pinned transfer buffer,
-// cut into pieces of at most 1 MiB and spread over up to 8 host threads
-// (one thread copies a few GB/s; the DMA engine moves far more).
+// cut into pieces of at most 1 MiB (of the destination) and spread over up to
+// 8 host threads (one thread copies a few GB/s; the DMA engine moves far
+// more).  A job with f64 set reads doubles and writes them rounded to float
+// (bytes counts the float destination).
 struct HostCopy {
   void* dst;
   const void* src;
   size_t bytes;
+  bool f64 = false;
 };
+void copy_piece(const HostCopy& p) {
+  if (!p.f64) {
+    std::memcpy(p.dst, p.src, p.bytes);
+    return;
+  }
+  float* d = static_cast<float*>(p.dst);
+  const double* s = static_cast<const double*>(p.src);
+  const size_t n = p.bytes / sizeof(float);
+  for (size_t i = 0; i < n; ++i) d[i] = static_cast<float>(s[i]);
+}
 void copy_all(const std::vector<HostCopy>& jobs) {
   constexpr size_t kPiece = size_t(1) << 20;
   std::vector<HostCopy> pieces;
   size_t total = 0;
   for (const HostCopy& j : jobs) {
-    total += j.bytes;
+    total += j.f64 ? 2 * j.bytes : j.bytes;
+    const size_t scale = j.f64 ? 2 : 1;
     for (size_t o = 0; o < j.bytes; o += kPiece)
-      pieces.push_back({static_cast<char*>(j.dst) + o, static_cast<const char*>(j.src) + o,
-                        std::min(kPiece, j.bytes - o)});
+      pieces.push_back({static_cast<char*>(j.dst) + o, static_cast<const char*>(j.src) + scale * o,
+                        std::min(kPiece, j.bytes - o), j.f64});
   }
   const int np = static_cast<int>(pieces.size());
   if (total < (size_t(4) << 20)) {
-    for (const HostCopy& p : pieces) std::memcpy(p.dst, p.src, p.bytes);
+    for (const HostCopy& p : pieces) copy_piece(p);
     return;
   }
 #pragma omp parallel for schedule(dynamic, 1) num_threads(8)
-  for (int k = 0; k < np; ++k) std::memcpy(pieces[k].dst, pieces[k].src, pieces[k].bytes);
+  for (int k = 0; k < np; ++k) copy_piece(pieces[k]);
 }
 
 }  // namespace
@@ -228,8 +242,8 @@ void cryo_ctx::io_reserve(size_t bytes) {
 extern "C" {
 
 // Solver::set_particles (sph_solver.cu:407-428) + ParticleSystem::upload
-// (particle_system.cpp:73-93).
-int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float* lo, const float* hi) {
+// (particle_system.cpp:73-93), from columns of floats or doubles.
+int cryo_set_particles_columns(cryo_ctx* c, const cryo_host_columns_t* p, const float* lo, const float* hi) {
   return guard(c, [&] {
     const int n = p->n;
     if (n <= 0) throw std::invalid_argument("Solver::set_particles: no particles");
@@ -248,10 +262,13 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
     char* h = c->io_host;
     const size_t N = (size_t)n;
     int have = 0;
-    std::vector<HostCopy> jobs = {{h + L.x, p->x, 12 * N}, {h + L.m, p->m, 4 * N}, {h + L.rho, p->rho, 4 * N},
-                                  {h + L.T, p->T, 4 * N}, {h + L.phase, p->phase, N}};
-    if (p->v) { jobs.push_back({h + L.v, p->v, 12 * N}); have |= IO_V; }
-    if (p->nrm) { jobs.push_back({h + L.nrm, p->nrm, 12 * N}); have |= IO_NRM; }
+    std::vector<HostCopy> jobs = {{h + L.x, p->x, 12 * N, p->x_f64 != 0},
+                                  {h + L.m, p->m, 4 * N, p->m_f64 != 0},
+                                  {h + L.rho, p->rho, 4 * N, p->rho_f64 != 0},
+                                  {h + L.T, p->T, 4 * N, p->T_f64 != 0},
+                                  {h + L.phase, p->phase, N}};
+    if (p->v) { jobs.push_back({h + L.v, p->v, 12 * N, p->v_f64 != 0}); have |= IO_V; }
+    if (p->nrm) { jobs.push_back({h + L.nrm, p->nrm, 12 * N, p->nrm_f64 != 0}); have |= IO_NRM; }
     if (p->flags) { jobs.push_back({h + L.flags, p->flags, N}); have |= IO_FLAGS; }
     if (p->id) { jobs.push_back({h + L.id, p->id, 4 * N}); have |= IO_ID; }
     copy_all(jobs);
@@ -261,6 +278,12 @@ int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float*
     LAUNCH_CHECK();
     c->finish_load(n, next_id);  // synchronises: the pinned buffer is free again
   });
+}
+
+int cryo_set_particles(cryo_ctx* c, const cryo_host_particles_t* p, const float* lo, const float* hi) {
+  const cryo_host_columns_t cols{p->n, p->x, p->v, p->nrm, p->m, p->rho, p->T, 0, 0, 0, 0, 0, 0,
+                                 p->phase, p->flags, p->id};
+  return cryo_set_particles_columns(c, &cols, lo, hi);
 }
 
 // Solver::particles (particle_system.cpp:95-101): the arrays the caller

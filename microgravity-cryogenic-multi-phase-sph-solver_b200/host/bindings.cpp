@@ -51,34 +51,71 @@ Arr column(py::handle src, py::ssize_t n, int width, const char* name) {
   return a;
 }
 
-// The particle set a caller hands over, held in the solver's element types;
-// view() gives the C ABI's structure of arrays over it (absent columns null).
+// One float column of a particle set: a C-contiguous float64 array is kept
+// as it is (the upload rounds each value while copying it into the transfer
+// buffer), anything else becomes float32 through NumPy.
+struct FloatColumn {
+  py::array arr;
+  bool f64 = false;
+  bool present = false;
+};
+FloatColumn float_column(py::handle src, py::ssize_t n, int width, const char* name) {
+  FloatColumn c;
+  c.present = true;
+  if (py::isinstance<py::array_t<double, py::array::c_style>>(src)) {
+    c.arr = py::reinterpret_borrow<py::array>(src);
+    c.f64 = true;
+  } else {
+    c.arr = py::cast<F32>(src);
+  }
+  const bool ok = width == 3 ? (c.arr.ndim() == 2 && (n < 0 || c.arr.shape(0) == n) && c.arr.shape(1) == 3)
+                             : c.arr.size() == n;
+  if (!ok)
+    throw std::invalid_argument(std::string(name) + (width == 3 ? ": expected an array of shape (N, 3)"
+                                                                : ": expected N values (one per particle)"));
+  return c;
+}
+
+// The particle set a caller hands over; columns() gives the C ABI's typed
+// columns over it (float or double per column, absent columns null), view()
+// the all-float structure of arrays (double columns converted by NumPy).
 struct ParticleColumns {
-  F32 x, v, nrm, m, rho, T;
+  FloatColumn x, v, nrm, m, rho, T;
   U8 phase, flags;
-  bool has_v = false, has_nrm = false, has_flags = false;
+  bool has_flags = false;
   py::ssize_t n = 0;
+  mutable std::vector<F32> f32_copies;
 
   ParticleColumns(py::handle position, py::handle mass, py::handle density, py::handle temperature,
                   py::handle phase_in, py::handle velocity, py::handle normal, py::handle flags_in) {
-    x = py::cast<F32>(position);
-    if (x.ndim() != 2 || x.shape(1) != 3) throw std::invalid_argument("position: expected an array of shape (N, 3)");
-    n = x.shape(0);
-    m = column<F32>(mass, n, 1, "mass");
-    rho = column<F32>(density, n, 1, "density");
-    T = column<F32>(temperature, n, 1, "temperature");
+    x = float_column(position, -1, 3, "position");
+    n = x.arr.shape(0);
+    m = float_column(mass, n, 1, "mass");
+    rho = float_column(density, n, 1, "density");
+    T = float_column(temperature, n, 1, "temperature");
     phase = column<U8>(phase_in, n, 1, "phase");
     const std::uint8_t* ph = phase.data();
     for (py::ssize_t i = 0; i < n; ++i)
       if (ph[i] > kWall) throw std::invalid_argument("phase: values must be 0 (liquid), 1 (vapour) or 2 (wall)");
-    if ((has_v = !velocity.is_none())) v = column<F32>(velocity, n, 3, "velocity");
-    if ((has_nrm = !normal.is_none())) nrm = column<F32>(normal, n, 3, "normal");
+    if (!velocity.is_none()) v = float_column(velocity, n, 3, "velocity");
+    if (!normal.is_none()) nrm = float_column(normal, n, 3, "normal");
     if ((has_flags = !flags_in.is_none())) flags = column<U8>(flags_in, n, 1, "flags");
   }
+  cryo_host_columns_t columns() const {
+    auto d = [](const FloatColumn& c) { return c.present ? c.arr.data() : nullptr; };
+    return cryo_host_columns_t{static_cast<int>(n), d(x), d(v), d(nrm), d(m), d(rho), d(T),
+                               x.f64, v.f64, nrm.f64, m.f64, rho.f64, T.f64,
+                               phase.data(), has_flags ? flags.data() : nullptr, nullptr};
+  }
   cryo_host_particles_t view() const {
-    auto p = [](const auto& a, bool on) { return on ? const_cast<std::remove_const_t<std::remove_pointer_t<decltype(a.data())>>*>(a.data()) : nullptr; };
-    return cryo_host_particles_t{static_cast<int>(n), p(x, true), p(v, has_v), p(nrm, has_nrm), p(m, true),
-                                 p(rho, true), p(T, true), p(phase, true), p(flags, has_flags), nullptr};
+    auto f = [&](const FloatColumn& c) -> const float* {
+      if (!c.present) return nullptr;
+      if (!c.f64) return static_cast<const float*>(c.arr.data());
+      f32_copies.push_back(py::cast<F32>(c.arr));
+      return f32_copies.back().data();
+    };
+    return cryo_host_particles_t{static_cast<int>(n), f(x), f(v), f(nrm), f(m), f(rho), f(T), phase.data(),
+                                 has_flags ? flags.data() : nullptr, nullptr};
   }
 };
 
@@ -135,17 +172,18 @@ HostParticles host_particles_of(const py::dict& d) {
                           d.contains("normal") ? py::handle(d["normal"]) : py::handle(py::none()),
                           d.contains("flags") ? py::handle(d["flags"]) : py::handle(py::none()));
   const auto n = static_cast<std::size_t>(c.n);
+  const cryo_host_particles_t f = c.view();  // float columns
   HostParticles hp;
-  auto vecs = [n](std::vector<Vec3>& dst, const F32& a, bool on) {
+  auto vecs = [n](std::vector<Vec3>& dst, const float* a) {
     dst.assign(n, Vec3{0, 0, 0});
-    if (on && n) std::memcpy(dst.data(), a.data(), 12 * n);
+    if (a && n) std::memcpy(dst.data(), a, 12 * n);
   };
-  vecs(hp.x, c.x, true);
-  vecs(hp.v, c.v, c.has_v);
-  vecs(hp.nrm, c.nrm, c.has_nrm);
-  hp.m.assign(c.m.data(), c.m.data() + n);
-  hp.rho.assign(c.rho.data(), c.rho.data() + n);
-  hp.T.assign(c.T.data(), c.T.data() + n);
+  vecs(hp.x, f.x);
+  vecs(hp.v, f.v);
+  vecs(hp.nrm, f.nrm);
+  hp.m.assign(f.m, f.m + n);
+  hp.rho.assign(f.rho, f.rho + n);
+  hp.T.assign(f.T, f.T + n);
   hp.phase.assign(c.phase.data(), c.phase.data() + n);
   hp.flags = c.has_flags ? std::vector<std::uint8_t>(c.flags.data(), c.flags.data() + n) : std::vector<std::uint8_t>(n, 0);
   hp.id.resize(n);
@@ -461,7 +499,7 @@ PYBIND11_MODULE(CryoSPH, m) {
              py::object phase, const Triple& domain_lo, const Triple& domain_hi, py::object velocity,
              py::object normal, py::object flags) {
             const ParticleColumns cols(position, mass, density, temperature, phase, velocity, normal, flags);
-            const cryo_host_particles_t view = cols.view();
+            const cryo_host_columns_t view = cols.columns();
             py::gil_scoped_release nogil;
             s.set_particles(view, AABB{vec(domain_lo), vec(domain_hi)});
           },

@@ -322,6 +322,9 @@ class Solver {
   void set_particles(const HostParticles& particles, const AABB& domain);
   // the same from caller-owned arrays in the C ABI's layout (no host copy)
   void set_particles(const cryo_host_particles_t& particles, const AABB& domain);
+  // Columns of floats or doubles (cryo_set_particles_columns): doubles are
+  // rounded to float while they are copied into the transfer buffer.
+  void set_particles(const cryo_host_columns_t& particles, const AABB& domain);
   // on_device: generate the lattice on the GPU where the geometry has a
   // device form (the particles are the same as the host generator's)
   void build_tank(const Geometry& geometry, const FillSpec& fill, bool on_device = true);

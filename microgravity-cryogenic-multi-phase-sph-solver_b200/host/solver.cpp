@@ -164,6 +164,12 @@ void Solver::set_particles(const cryo_host_particles_t& p, const AABB& domain) {
   check(cryo_set_particles(ctx_, &p, lo, hi));
 }
 
+void Solver::set_particles(const cryo_host_columns_t& p, const AABB& domain) {
+  float lo[3], hi[3];
+  domain_floats(domain, lo, hi);
+  check(cryo_set_particles_columns(ctx_, &p, lo, hi));
+}
+
 void Solver::download(cryo_host_particles_out_t& out) const { check(cryo_download(ctx_, &out)); }
 
 // Solver::build_tank (sph_solver.cu:430-437)

@@ -259,6 +259,16 @@ def test_particles_round_trip_through_the_soa_transfers(cuda_device):
     q = solver.particles()
     assert not q["velocity"].any() and not q["normal"].any() and not q["flags"].any()
     assert np.array_equal(q["id"], np.arange(n))
+    # float64 columns (NumPy's default; converted on several host threads)
+    # arrive rounded exactly as astype(float32) rounds them
+    f64 = {k: np.asarray(p[k], np.float64) * (1.0 + 1e-9) for k in ("position", "mass", "density", "temperature")}
+    v64 = rng.standard_normal((n, 3))
+    solver.set_particles(f64["position"], f64["mass"], f64["density"], f64["temperature"], p["phase"],
+                         domain_lo=(-0.03, -0.03, -0.03), domain_hi=(0.03, 0.03, 0.03), velocity=v64)
+    q = solver.particles()
+    for k, a in f64.items():
+        assert np.array_equal(q[k], a.astype(np.float32)), k
+    assert np.array_equal(q["velocity"], v64.astype(np.float32))
 
 
 def test_diagnostics_requested_without_blocking_equal_the_blocking_ones(cuda_device):
