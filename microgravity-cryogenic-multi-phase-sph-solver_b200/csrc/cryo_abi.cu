@@ -196,7 +196,7 @@ void cryo_ctx::grid_build(int src) {
 
 // Radix sort of keys_a, cell table, reorder gather into the other set and
 // (with lists on) the neighbour / phase lists of the new order.
-void cryo_ctx::sort_and_gather(int src, int list_mode) {
+void cryo_ctx::sort_and_gather(int src, int list_mode, bool reset_maxima) {
   const int G = grid_blocks();
   const int tiles = (capacity + RS_TILE - 1) / RS_TILE;
   const uint32_t* kin = keys_a;
@@ -218,7 +218,7 @@ void cryo_ctx::sort_and_gather(int src, int list_mode) {
   const int GC = std::max(1, std::min((P.num_cells + 1 + kBlock - 1) / kBlock, sm_count * 16));
   LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
   if (P.use_lists) CK(cudaMemsetAsync(cell_fluid, 0, (size_t)P.num_cells, stream));
-  LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce());
+  LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce(), reset_maxima ? 1 : 0);
   if (P.use_lists) {
     LAUNCH(k_build_lists, G, kBlock, P, view(1 - src), reduce(), list_mode);
     lists_built = true;
@@ -308,9 +308,10 @@ void cryo_ctx::enqueue_step(int s, const StepTape* tape) {
     tape_sums = tape->sums;
     tape_n = tape->n;
   }
-  LAUNCH(k_begin_step, 1, 1, P, view(s), BEGIN_STEP);
-  LAUNCH(k_kick_drift_keys, G, kBlock, P, view(s), keys_a);
-  sort_and_gather(s, LISTS_PHASE);
+  // the step size, the frame and the kick-drift in one launch; the maxima
+  // are reset by the gather
+  LAUNCH(k_begin_kick_drift_keys, G, kBlock, P, view(s), keys_a);
+  sort_and_gather(s, LISTS_PHASE, true);
   const int d = 1 - s;
   const View V = view(d);
   slab_point(SLAB_SORTED, d);
@@ -319,6 +320,11 @@ void cryo_ctx::enqueue_step(int s, const StepTape* tape) {
     LAUNCH(k_adj_copy4, G, kBlock, V.vT, tape->vT1, tape->m1, V.mrps, dyn);
     LAUNCH(k_adj_copy4, G, kBlock, V.ns4, tape->ns1, nullptr, nullptr, dyn);
     CK(cudaMemcpyAsync(tape->dyn1, dyn, sizeof(DynState), cudaMemcpyDeviceToDevice, stream));
+  }
+  if (!P.cfg_phase_change && !(P.shift_strength > 0.0f) && !slab_group) {
+    // nothing runs between the closing kick and the end of the step
+    LAUNCH(k_kick_saturation, G, kBlock, P, V, reduce());
+    return;
   }
   LAUNCH(k_kick, G, kBlock, P, V, (P.cfg_phase_change ? KICK_SOURCES : 0) | KICK_HEAT);
   slab_point(SLAB_HALO, d);

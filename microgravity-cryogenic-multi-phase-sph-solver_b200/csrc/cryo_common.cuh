@@ -582,6 +582,27 @@ __device__ inline void block_sum(double (&v)[NV], double* sh) {
   }
   __syncthreads();
 }
+// kick_drift (sph_solver.cu:20-34)
+__device__ inline void kick_drift_one(const Params& P, const View& V, int i, float dt, int continuity, int tvf,
+                                      float4& xp) {
+  const float half = 0.5f * dt;
+  float4 vT = V.vT[i];
+  const V3 v = xyz(vT) + xyz(V.a4[i]) * half;
+  V.vT[i] = f4(v, vT.w);
+  float4 vt4 = V.vt[i];
+  const V3 vt = tvf ? v + xyz(V.ab4[i]) * half : v;
+  V.vt[i] = f4(vt, vt4.w);
+  const V3 x = xyz(xp) + vt * dt;
+  xp.x = x.x;
+  xp.y = x.y;
+  xp.z = x.z;
+  V.xp[i] = xp;
+  if (continuity) {
+    float* mr = reinterpret_cast<float*>(V.mrps + i);
+    mr[1] += V.ab4[i].w * dt;
+  }
+}
+
 // atomicMax on non-negative floats through their (order-preserving) bits.
 __device__ inline void atomic_max_pos(float* addr, float v) {
   if (v > 0.0f) atomicMax(reinterpret_cast<int*>(addr), __float_as_int(v));

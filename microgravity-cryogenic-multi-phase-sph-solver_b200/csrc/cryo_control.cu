@@ -77,6 +77,40 @@ __global__ void k_begin_step(Params P, View V, int mode) {
   d->spacing_ratio = 1.0f;
 }
 
+// The start of Solver::step fused with its kick_drift and hash keys (the
+// step path, one launch instead of two): every block derives the step size
+// itself from the previous evaluation's maxima -- compute_dt over the same
+// scalars, so every block gets the same dt bit for bit -- and block 0 stores
+// it and moves the manoeuvre frame to the new time level.  The maxima are
+// reset later in the step (k_gather with reset_maxima), once no block of this
+// kernel can still read them; the frame is not read here.
+__global__ void __launch_bounds__(kBlock) k_begin_kick_drift_keys(Params P, View V, uint32_t* __restrict__ keys) {
+  __shared__ float sdt;
+  DynState* d = V.dyn;
+  if (threadIdx.x == 0) {
+    const float dt = compute_dt(P, *d);
+    sdt = dt;
+    if (blockIdx.x == 0) {
+      d->dt = dt;
+      if (d->fr.has_maneuver) {
+        V3 a, w, wd;
+        maneuver_evaluate(V, d->man_n, d->man_rot, d->time + (double)dt, a, w, wd);
+        apply_frame(d, a, w, wd, d->man_origin);
+      }
+    }
+  }
+  __syncthreads();
+  const float dt = sdt;
+  const int n = d->n;
+  const int continuity = P.density_mode == CRYO_DENSITY_CONTINUITY;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 xp = V.xp[i];
+    const int ph = ph_of(xp);
+    if (is_fluid(ph)) kick_drift_one(P, V, i, dt, continuity, P.tvf, xp);
+    keys[i] = ph == kDead ? (uint32_t)P.num_cells : (uint32_t)cell_index(P, xyz(xp));
+  }
+}
+
 // Solver::update_saturation (sph_solver.cu:586-607) with the phase inventory
 // (sph_solver.cu:137-145) as one FP64 reduction; with end_of_step the clock
 // advances (sph_solver.cu:530-532) and the relax damping is applied
@@ -132,6 +166,71 @@ __global__ void __launch_bounds__(kBlock) k_saturation(Params P, View V, Reduce 
     d->step += 1;
     d->last_dt = (double)d->dt;
   }
+}
+
+// The closing kick (sph_solver.cu:36-46, k_kick without phase-change
+// sources) fused with k_saturation's end of step, for steps where nothing runs
+// between them (no particle shifting, no phase change, one context per
+// tank): each thread kicks its particle and then adds it to the ullage sums
+// and damps it, in the chunk order k_saturation uses, so the sums and the
+// state equal the two launches' bit for bit.
+__global__ void __launch_bounds__(kBlock) k_kick_saturation(Params P, View V, Reduce R) {
+  __shared__ double sh[3 * kBlock / 32];
+  DynState* d = V.dyn;
+  const int n = d->n;
+  const int nch = num_chunks(n);
+  const float dt = d->dt;
+  const float half = 0.5f * dt;
+  const int thermal = d->thermal_on;
+  const bool closed = P.thermo_closed && P.has_vapor;
+  const bool damp = d->damp_after_step;
+  const float damping = d->damping;
+  for (int c = blockIdx.x; c < nch; c += gridDim.x) {
+    const int i = c * kChunk + threadIdx.x;
+    double s[3] = {0.0, 0.0, 0.0};
+    if (i < n) {
+      const int ph = ph_of(V.xp[i]);
+      if (is_fluid(ph)) {
+        float4 vT = V.vT[i];
+        const float4 a4 = V.a4[i];
+        V3 v = xyz(vT) + xyz(a4) * half;
+        float T = vT.w;
+        if (thermal) T += a4.w * dt;
+        if (closed) {
+          const double m = V.mrps[i].x;
+          if (ph == kLiquid) s[0] = m;
+          if (ph == kVapor) {
+            s[1] = m;
+            s[2] = m * T;
+          }
+        }
+        if (damp) {
+          v = v * damping;
+          const float4 vt = V.vt[i];
+          V.vt[i] = f4(xyz(vt) * damping, vt.w);
+        }
+        V.vT[i] = f4(v, T);
+      }
+    }
+    if (closed) publish_chunk<3>(R, c, s, sh);
+  }
+  const bool last = closed ? last_block(R.ticket) : (blockIdx.x == 0);
+  if (!last) return;
+  double m_liq = 0, m_vap = 0, mT_vap = 0;
+  if (closed) {
+    m_liq = block_sum_partials(R, 0, nch);
+    m_vap = block_sum_partials(R, 1, nch);
+    mT_vap = block_sum_partials(R, 2, nch);
+  }
+  if (threadIdx.x != 0) return;
+  if (thermal && d->heat_inv_norm > 0.0f) d->heat_input += (double)P.heat_power * (double)dt;
+  d->sat_sum[0] = m_liq;
+  d->sat_sum[1] = m_vap;
+  d->sat_sum[2] = mT_vap;
+  saturation_update(P, d, closed, m_liq, m_vap, mT_vap);
+  d->time += (double)d->dt;
+  d->step += 1;
+  d->last_dt = (double)d->dt;
 }
 
 // Heat-weight normalisation on its own (sph_solver.cu:466-472), for

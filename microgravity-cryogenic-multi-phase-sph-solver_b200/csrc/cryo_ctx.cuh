@@ -511,7 +511,7 @@ struct cryo_ctx {
 
   // ------------------------------------------------------ step pieces
   void grid_build(int src);               // keys of current positions, sort, cells, gather, lists
-  void sort_and_gather(int src, int list_mode);  // after keys_a holds the keys
+  void sort_and_gather(int src, int list_mode, bool reset_maxima = false);  // after keys_a holds the keys
   void evaluate_rates(int s, bool maxima_reset, bool density_done, bool tape = false);
   void enqueue_step(int s, const StepTape* tape = nullptr);
   void launch_step();

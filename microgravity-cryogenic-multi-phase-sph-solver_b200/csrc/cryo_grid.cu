@@ -190,9 +190,18 @@ __global__ void k_cells(Params P, const uint32_t* __restrict__ keys, DynState* d
 // into the chunk offsets of the ordered phase index lists (partials rows 0
 // and 1) and their lengths.
 __global__ void __launch_bounds__(kBlock) k_gather(Params P, View src, View dst, const uint32_t* __restrict__ perm,
-                                                   Reduce R) {
+                                                   Reduce R, int reset_maxima) {
   __shared__ double sh[2 * kBlock / 32];
   DynState* dyn = src.dyn;
+  // the step's maxima start over for the force pass to come (the step size
+  // was taken from them by the launch before the sort)
+  if (reset_maxima && blockIdx.x == 0 && threadIdx.x == 0) {
+    dyn->v_max = 0.0f;
+    dyn->a_max = 0.0f;
+    dyn->Tv_max = 0.0f;
+    dyn->nu_t_max = 0.0f;
+    dyn->spacing_ratio = 1.0f;
+  }
   const int na = dyn->n_alive;
   const int nch = num_chunks(na);
   int own_lo, own_hi;

@@ -167,7 +167,7 @@ __global__ void k_rs_scan(uint32_t* hist, const DynState* dyn);
 __global__ void k_rs_downsweep(const uint32_t* kin, const uint32_t* vin, uint32_t* kout, uint32_t* vout, int shift,
                                int bits, const DynState* dyn, const uint32_t* hist);
 __global__ void k_cells(Params P, const uint32_t* keys, DynState* dyn, int* cell_begin);
-__global__ void k_gather(Params P, View src, View dst, const uint32_t* perm, Reduce R);
+__global__ void k_gather(Params P, View src, View dst, const uint32_t* perm, Reduce R, int reset_maxima);
 enum { LISTS_ONLY = 0, LISTS_PHASE = 1 };
 __global__ void k_build_lists(Params P, View V, Reduce R, int mode);
 __global__ void k_nbr_count(Params P, View V, int stored, int* counts);
@@ -287,6 +287,8 @@ __device__ inline void saturation_update(const Params& P, DynState* d, bool clos
   }
 }
 __global__ void k_saturation(Params P, View V, Reduce R, int end_of_step);
+__global__ void k_begin_kick_drift_keys(Params P, View V, uint32_t* keys);
+__global__ void k_kick_saturation(Params P, View V, Reduce R);
 __global__ void k_diagnostics(Params P, View V, Reduce R, double* out);
 
 // Packed per-particle telemetry record (telemetry.hpp:28-31).
