@@ -215,8 +215,7 @@ void cryo_ctx::sort_and_gather(int src, int list_mode, bool reset_maxima) {
   }
   sorted_keys = kin;
   sorted_perm = vin;
-  const int GC = std::max(1, std::min((P.num_cells + 1 + kBlock - 1) / kBlock, sm_count * 16));
-  LAUNCH(k_cells, GC, kBlock, P, kin, dyn, cell_begin);
+  LAUNCH(k_cells, G, kBlock, P, kin, dyn, cell_begin);
   if (P.use_lists) CK(cudaMemsetAsync(cell_fluid, 0, (size_t)P.num_cells, stream));
   LAUNCH(k_gather, G, kBlock, P, view(src), view(1 - src), vin, reduce(), reset_maxima ? 1 : 0);
   if (P.use_lists) {

@@ -165,21 +165,40 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_downsweep(const uint32_t* __r
 
 // Dense cell table: cell_begin[c] = first sorted index with key >= c, for
 // c in [0, num_cells]; cell_begin[num_cells] = number of live particles.
+// One pass over the sorted keys (clamped to num_cells: dead particles carry
+// that sentinel) instead of a binary search per cell: position i (0..n, with
+// key[-1] = -1 and key[n] = num_cells) writes i to every cell in
+// (key[i-1], key[i]], so each cell receives its lower bound exactly once.
+// A run longer than 8 cells (the empty cells of padding layers or around a
+// tank) is written by the whole warp together.
 __global__ void k_cells(Params P, const uint32_t* __restrict__ keys, DynState* dyn, int* __restrict__ cell_begin) {
-  // cell_begin[c] = first sorted index whose key is >= c (lower_bound), one
-  // thread per cell, so long runs of empty cells (the padding layers) cost no
-  // more than occupied ones; cell_begin[num_cells] = the live count.
   const int n = dyn->n;
   const int nc = P.num_cells;
-  for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= nc; c += gridDim.x * blockDim.x) {
-    int lo = 0, hi = n;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if ((int)min(__ldg(keys + mid), (uint32_t)nc) < c) lo = mid + 1;
-      else hi = mid;
+  const int lane = threadIdx.x & 31;
+  // whole warps walk 32 positions at a time (a warp-uniform loop), so every
+  // lane takes part in the ballots
+  const int warps = (gridDim.x * blockDim.x) >> 5;
+  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w * 32 <= n; w += warps) {
+    const int i = w * 32 + lane;
+    int lo = 0, hi = -1;  // cells lo..hi get i
+    if (i <= n) {
+      lo = (i == 0 ? -1 : (int)min(__ldg(keys + i - 1), (uint32_t)nc)) + 1;
+      hi = i == n ? nc : (int)min(__ldg(keys + i), (uint32_t)nc);
     }
-    cell_begin[c] = lo;
-    if (c == nc) dyn->n_alive = lo;
+    const int len = hi - lo + 1;
+    if (len > 0 && len <= 8) {
+      for (int c = lo; c <= hi; ++c) cell_begin[c] = i;
+      if (hi == nc) dyn->n_alive = i;
+    }
+    unsigned longs = __ballot_sync(0xffffffffu, len > 8);
+    while (longs) {
+      const int src = __ffs(longs) - 1;
+      longs &= longs - 1u;
+      const int rl = __shfl_sync(0xffffffffu, lo, src), rh = __shfl_sync(0xffffffffu, hi, src);
+      const int ri = __shfl_sync(0xffffffffu, i, src);
+      for (int c = rl + lane; c <= rh; c += 32) cell_begin[c] = ri;
+      if (lane == src && rh == nc) dyn->n_alive = ri;
+    }
   }
 }
 
