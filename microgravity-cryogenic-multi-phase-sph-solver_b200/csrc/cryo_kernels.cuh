@@ -247,7 +247,6 @@ constexpr int forces_min_blocks(int what) {
 
 // integrator + phase change (cryo_phase.cu)
 __global__ void k_kick_drift(Params P, View V, int continuity, int tvf);
-__global__ void k_kick_drift_keys(Params P, View V, uint32_t* keys);
 enum { KICK_SOURCES = 1, KICK_HEAT = 2 };
 __global__ void k_kick(Params P, View V, int flags);
 __global__ void k_pc_sources(Params P, View V);

@@ -18,20 +18,6 @@ __global__ void __launch_bounds__(kBlock) k_kick_drift(Params P, View V, int con
   }
 }
 
-// kick_drift fused with the hash keys of the new positions (spatial_hash.cu:61-68).
-__global__ void __launch_bounds__(kBlock) k_kick_drift_keys(Params P, View V, uint32_t* __restrict__ keys) {
-  const DynState* dyn = V.dyn;
-  const int n = dyn->n;
-  const float dt = dyn->dt;
-  const int continuity = P.density_mode == CRYO_DENSITY_CONTINUITY;
-  PARTICLE_LOOP(i, n) {
-    float4 xp = V.xp[i];
-    const int ph = ph_of(xp);
-    if (is_fluid(ph)) kick_drift_one(P, V, i, dt, continuity, P.tvf, xp);
-    keys[i] = ph == kDead ? (uint32_t)P.num_cells : (uint32_t)cell_index(P, xyz(xp));
-  }
-}
-
 // phase_change_sources (phase_change.cu:77-137) for particle i.
 __device__ inline void pc_source_one(const Params& P, const View& V, int i, float T_sat, float dt, float4 xp) {
   const int ph = ph_of(xp);
