@@ -474,6 +474,43 @@ __device__ inline void for_each_nbr(const Params& P, const View& V, int i, V3 xi
   }
 }
 
+// for_each_nbr for passes with little work per neighbour: the loop takes
+// each loaded quad of indices whole (its four entries at fixed positions, no
+// shifting), with one reload test per four neighbours; the next neighbour's
+// position is in flight while the current one is processed, as in
+// for_each_nbr, and the order and the r2 bits are the same.
+template <class F>
+__device__ inline void for_each_nbr_quads(const Params& P, const View& V, int i, V3 xi, F&& f) {
+  const int c = P.use_lists ? __ldg(V.nbr_cnt + i) : kMaxNbr + 1;
+  if (c <= kMaxNbr) {
+    const int4* __restrict__ base = reinterpret_cast<const int4*>(V.nbr + (size_t)i * kNbrChunk);
+    const size_t cstride = (size_t)V.capacity * (kNbrChunk / 4);
+    auto quad = [&](int q) { return __ldg(base + (size_t)(q >> 1) * cstride + (q & 1)); };
+    int4 cur = c > 0 ? quad(0) : make_int4(0, 0, 0, 0);
+    int4 nxt = c > 4 ? quad(1) : make_int4(0, 0, 0, 0);
+    float4 xn = c > 0 ? __ldg(V.xp + cur.x) : make_float4(0, 0, 0, 0);
+    for (int k0 = 0; k0 < c; k0 += 4) {
+      const int js[4] = {cur.x, cur.y, cur.z, cur.w};
+      const int next0 = nxt.x;  // the first entry of the next quad
+      cur = nxt;
+      if (k0 + 8 < c) nxt = quad((k0 >> 2) + 2);
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        if (k0 + u < c) {
+          const int j = js[u];
+          const float4 xj = xn;
+          if (k0 + u + 1 < c) xn = __ldg(V.xp + (u < 3 ? js[u + 1] : next0));
+          const V3 rij = xi - xyz(xj);
+          const float r2 = norm2(rij);
+          f(j, xj, rij, r2);
+        }
+      }
+    }
+  } else {
+    for_each_neighbor(P, V.cell_begin, V.xp, xi, f);
+  }
+}
+
 // for_each_nbr that also brings each neighbour's record of `A` (one float4
 // per particle) along with its position, one neighbour ahead, so that load
 // is in flight while the previous neighbour is processed: f(j, xj, rij, r2, aj).

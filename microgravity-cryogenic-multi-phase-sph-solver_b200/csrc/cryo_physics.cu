@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kBlock) k_density(Params P, View V, int fuse_e
     }
     const V3 xi = xyz(xpi);
     float sum = 0.0f, r2min = P.support2;
-    for_each_nbr(P, V, i, xi, [&](int j, float4, V3, float r2) {
+    for_each_nbr_quads(P, V, i, xi, [&](int j, float4, V3, float r2) {
       sum += kernel_W(P, sqrtf(r2));
       if (j != i && r2 < r2min) r2min = r2;
     });
