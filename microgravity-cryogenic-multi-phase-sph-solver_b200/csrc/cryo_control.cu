@@ -268,48 +268,53 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
   __shared__ float shmax[2][kBlock / 32];
   DynState* d = V.dyn;
   const int n = d->n;
-  const int nch = num_chunks(n);
+  // chunks of kDiagPer * kChunk particles: each thread adds its kDiagPer
+  // particles first, so a block reduction covers four times the particles
+  constexpr int kDiagPer = 4;
+  const int nch = (n + kDiagPer * kChunk - 1) / (kDiagPer * kChunk);
   const int own_lo = d->own_lo, own_hi = d->own_hi, n_sorted = d->n_sorted;
   for (int c = blockIdx.x; c < nch; c += gridDim.x) {
-    const int i = c * kChunk + threadIdx.x;
     double s[23];
 #pragma unroll
     for (int k = 0; k < 23; ++k) s[k] = 0.0;
     float vmax = 0.0f, tmax = 0.0f;
-    if (i < n && owned(own_lo, own_hi, n_sorted, i)) {
-      const float4 xp = V.xp[i];
-      const int ph = ph_of(xp);
-      const float4 vT = V.vT[i];
-      const double m = V.mrps[i].x;
-      if (ph == kLiquid || ph == kVapor) {
-        // per-phase slots chosen by selects, not by a run-time index, so the
-        // 23 sums stay in registers (an indexed store would put them in
-        // local memory)
-        const bool liq = ph == kLiquid;
-        const double ke = 0.5 * m * (double)norm2(xyz(vT));
-        const double H = m * (double)specific_enthalpy(P, ph, vT.w);
-        const double mT = m * vT.w;
-        s[0] = liq ? 1.0 : 0.0;
-        s[1] = liq ? 0.0 : 1.0;
-        s[3] = liq ? m : 0.0;
-        s[4] = liq ? 0.0 : m;
-        s[5] = liq ? ke : 0.0;
-        s[6] = liq ? 0.0 : ke;
-        s[7] = liq ? H : 0.0;
-        s[8] = liq ? 0.0 : H;
-        s[9] = liq ? mT : 0.0;
-        s[10] = liq ? 0.0 : mT;
-        const float4 fw = V.fw[i], mw = V.mw[i];
-        s[17] = fw.x; s[18] = fw.y; s[19] = fw.z;
-        s[20] = mw.x; s[21] = mw.y; s[22] = mw.z;
-        vmax = norm(xyz(vT));
-        if (ph == kLiquid) {
-          s[11] = m * xp.x; s[12] = m * xp.y; s[13] = m * xp.z;
-          s[14] = m * vT.x; s[15] = m * vT.y; s[16] = m * vT.z;
-          tmax = vT.w;
+    for (int u = 0; u < kDiagPer; ++u) {
+      const int i = (c * kDiagPer + u) * kChunk + threadIdx.x;
+      if (i < n && owned(own_lo, own_hi, n_sorted, i)) {
+        const float4 xp = V.xp[i];
+        const int ph = ph_of(xp);
+        const float4 vT = V.vT[i];
+        const double m = V.mrps[i].x;
+        if (ph == kLiquid || ph == kVapor) {
+          // per-phase slots chosen by selects, not by a run-time index, so the
+          // 23 sums stay in registers (an indexed store would put them in
+          // local memory)
+          const bool liq = ph == kLiquid;
+          const double ke = 0.5 * m * (double)norm2(xyz(vT));
+          const double H = m * (double)specific_enthalpy(P, ph, vT.w);
+          const double mT = m * vT.w;
+          s[0] += liq ? 1.0 : 0.0;
+          s[1] += liq ? 0.0 : 1.0;
+          s[3] += liq ? m : 0.0;
+          s[4] += liq ? 0.0 : m;
+          s[5] += liq ? ke : 0.0;
+          s[6] += liq ? 0.0 : ke;
+          s[7] += liq ? H : 0.0;
+          s[8] += liq ? 0.0 : H;
+          s[9] += liq ? mT : 0.0;
+          s[10] += liq ? 0.0 : mT;
+          const float4 fw = V.fw[i], mw = V.mw[i];
+          s[17] += fw.x; s[18] += fw.y; s[19] += fw.z;
+          s[20] += mw.x; s[21] += mw.y; s[22] += mw.z;
+          vmax = fmaxf(vmax, norm(xyz(vT)));
+          if (ph == kLiquid) {
+            s[11] += m * xp.x; s[12] += m * xp.y; s[13] += m * xp.z;
+            s[14] += m * vT.x; s[15] += m * vT.y; s[16] += m * vT.z;
+            tmax = fmaxf(tmax, vT.w);
+          }
+        } else if (ph == kWall) {
+          s[2] += 1.0;
         }
-      } else if (ph == kWall) {
-        s[2] = 1.0;
       }
     }
     publish_chunk<23>(R, c, s, sh);
