@@ -598,27 +598,6 @@ __device__ inline float warp_max(float v) {
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
   return v;
 }
-// Block sum of NV doubles per thread; result valid in thread 0.  `sh` must
-// hold NV * (blockDim/32) doubles.
-template <int NV>
-__device__ inline void block_sum(double (&v)[NV], double* sh) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < NV; ++k) sh[k * nw + warp] = v[k];
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int k = 0; k < NV; ++k) {
-      double s = 0;
-      for (int w = 0; w < nw; ++w) s += sh[k * nw + w];
-      v[k] = s;
-    }
-  }
-  __syncthreads();
-}
 // kick_drift (sph_solver.cu:20-34)
 __device__ inline void kick_drift_one(const Params& P, const View& V, int i, float dt, int continuity, int tvf,
                                       float4& xp) {

@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kBlock) k_heat_norm(Params P, View V, Reduce R
 //   11-13 m x (L), 14-16 m v (L), 17-19 sum fw (fluid), 20-22 sum mw (fluid),
 //   23 max fluid speed, 24 max liquid T, 25-43 the scalar state (clock,
 //   counters, ullage, frame)
-__global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce R, double* __restrict__ out) {
+__global__ void __launch_bounds__(kBlock, 2) k_diagnostics(Params P, View V, Reduce R, double* __restrict__ out) {
   __shared__ double sh[23 * kBlock / 32];
   __shared__ float shmax[2][kBlock / 32];
   DynState* d = V.dyn;
@@ -278,13 +278,27 @@ __global__ void __launch_bounds__(kBlock) k_diagnostics(Params P, View V, Reduce
 #pragma unroll
     for (int k = 0; k < 23; ++k) s[k] = 0.0;
     float vmax = 0.0f, tmax = 0.0f;
+    // the records of all kDiagPer particles are requested before any of them
+    // is added, so the thread waits on one round trip instead of kDiagPer
+    float4 xpu[kDiagPer], vTu[kDiagPer];
+    float massu[kDiagPer];
+    bool oku[kDiagPer];
+#pragma unroll
     for (int u = 0; u < kDiagPer; ++u) {
       const int i = (c * kDiagPer + u) * kChunk + threadIdx.x;
-      if (i < n && owned(own_lo, own_hi, n_sorted, i)) {
-        const float4 xp = V.xp[i];
+      oku[u] = i < n && owned(own_lo, own_hi, n_sorted, i);
+      xpu[u] = oku[u] ? V.xp[i] : make_float4(0, 0, 0, 0);
+      vTu[u] = oku[u] ? V.vT[i] : make_float4(0, 0, 0, 0);
+      massu[u] = oku[u] ? V.mrps[i].x : 0.0f;
+    }
+#pragma unroll
+    for (int u = 0; u < kDiagPer; ++u) {
+      const int i = (c * kDiagPer + u) * kChunk + threadIdx.x;
+      if (oku[u]) {
+        const float4 xp = xpu[u];
         const int ph = ph_of(xp);
-        const float4 vT = V.vT[i];
-        const double m = V.mrps[i].x;
+        const float4 vT = vTu[u];
+        const double m = massu[u];
         if (ph == kLiquid || ph == kVapor) {
           // per-phase slots chosen by selects, not by a run-time index, so the
           // 23 sums stay in registers (an indexed store would put them in

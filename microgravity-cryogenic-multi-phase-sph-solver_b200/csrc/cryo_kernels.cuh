@@ -150,13 +150,28 @@ __device__ inline double block_exclusive_scan(const Reduce& R, int v, int nchunk
   __syncthreads();
   return t;
 }
-// Writes the block sums of NV values for chunk c.
+// Writes the block sums of NV values (one per thread each) for chunk c:
+// every warp reduces its lanes, then lane k of warp 0 adds value k's warp
+// sums in warp order (from 0.0, one after another) and stores it, so the
+// values are finished side by side rather than one after another by one
+// thread; each value's additions are the same either way.  `sh` must hold
+// NV * (blockDim / 32) doubles; every thread of the block must call it.
 template <int NV>
 __device__ inline void publish_chunk(const Reduce& R, int c, double (&v)[NV], double* sh) {
-  block_sum<NV>(v, sh);
-  if (threadIdx.x == 0)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-    for (int k = 0; k < NV; ++k) R.partials[(size_t)k * R.max_chunks + c] = v[k];
+  for (int k = 0; k < NV; ++k) v[k] = warp_sum(v[k]);
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < NV; ++k) sh[k * nw + warp] = v[k];
+  __syncthreads();
+  if (warp == 0)
+    for (int k = lane; k < NV; k += 32) {
+      double s = 0;
+      for (int w = 0; w < nw; ++w) s += sh[k * nw + w];
+      R.partials[(size_t)k * R.max_chunks + c] = s;
+    }
+  __syncthreads();  // sh is free again
 }
 __device__ inline int num_chunks(int n) { return (n + kChunk - 1) / kChunk; }
 
