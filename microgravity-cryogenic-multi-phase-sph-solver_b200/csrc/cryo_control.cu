@@ -263,6 +263,9 @@ __global__ void __launch_bounds__(kBlock) k_heat_norm(Params P, View V, Reduce R
 //   11-13 m x (L), 14-16 m v (L), 17-19 sum fw (fluid), 20-22 sum mw (fluid),
 //   23 max fluid speed, 24 max liquid T, 25-43 the scalar state (clock,
 //   counters, ullage, frame)
+// Two resident blocks per SM (at most 128 registers): a thread holds its four
+// particles' records at once, and the 199 chunk blocks of a 200k-particle
+// tank still run in one wave over the 148 SMs.
 __global__ void __launch_bounds__(kBlock, 2) k_diagnostics(Params P, View V, Reduce R, double* __restrict__ out) {
   __shared__ double sh[23 * kBlock / 32];
   __shared__ float shmax[2][kBlock / 32];
